@@ -1,0 +1,361 @@
+"""Benchmark: symbolic LU factorization throughput on the B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload nd3d|plain2d|circuit|bundled]
+
+A step is one full symbolic factorization (fill pattern of L and U, per-line
+counts, supernode partition) of the workload matrix.  The default workload is
+the 80^3 7-point stencil in geometric nested-dissection order with a seeded
+10% of one-sided drops (n = 512,000), the single-GPU configuration the
+headline metric is quoted on.  Inputs are seeded synthetic matrices.
+
+Printed (rank 0, one JSON line):
+  value  -- nnz(L+U)/s over all ranks, matrix resident in HBM, pattern kept on
+            the device, CUDA events on the launching stream, max over ranks;
+  e2e    -- the same metric through the public API from pinned host buffers:
+            upload (H2D + graph build), factorization, and download of every
+            result array including the pattern, all inside the timed region;
+  roofline, cpu_baseline, clocks, gpu_launches as documented in the keys.
+
+Multi-GPU (torchrun): every rank factorizes its own copy of the workload (the
+units are independent factorizations; no data-path collective), so per-GPU
+work is fixed: weak scaling.
+
+--impl reference times the CPU restatement of the reference algorithm (the
+reference has no CPU path of its own) on a bounded, evenly strided sample of
+the workload's sources, with all host threads, in the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["nd3d", "plain2d", "circuit", "bundled"], default="nd3d")
+    ap.add_argument("--side", type=int, default=80, help="grid side of the nd3d workload")
+    ap.add_argument("--reuse", type=int, default=0, help="reuse traversals along s-1 -> s chains")
+    ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--lanes", type=int, default=0)
+    ap.add_argument("--ctas-per-sm", type=int, default=0)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(args):
+    from gsofa_b200 import matgen
+    if args.workload == "nd3d":
+        g = matgen.config_nd3d(args.side)
+        cfg = {"workload": f"grid3d_{args.side}^3_7pt_nd_drop0.1", "n": g.n, "nnz": g.nnz,
+               "ordering": "geometric nested dissection", "seed": matgen.SEEDS["nd3d"]}
+    elif args.workload == "plain2d":
+        g = matgen.config_plain2d()
+        cfg = {"workload": "grid2d_64x64_5pt_natural", "n": g.n, "nnz": g.nnz, "ordering": "natural"}
+    elif args.workload == "circuit":
+        g = matgen.config_circuit()
+        cfg = {"workload": "powerlaw_659033_rcm", "n": g.n, "nnz": g.nnz, "ordering": "random+RCM",
+               "seed": matgen.SEEDS["circuit"]}
+    else:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from tests.common import bundled
+        g = bundled()
+        cfg = {"workload": "superlu_dump_11948", "n": g.n, "nnz": g.nnz}
+    return g, cfg
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for i, nm in enumerate(names):
+                if len(s) > 5 + i and s[5 + i].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.samples)}
+
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_per_launch(cfg_name):
+    """DRAM bytes per factorization launch from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        e = d.get(cfg_name)
+        return None if e is None else float(e["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
+def cpu_sample(g, budget_s, step_hint=None):
+    """Times the oracle (all host threads) on every k-th source of both passes.
+    Returns (nnz_per_s, cores, description, k)."""
+    import oracle
+    n = g.n
+    cores = os.cpu_count() or 1
+
+    def run(k):
+        src = np.arange(n - 1, -1, -k, dtype=np.int32)   # includes the heaviest line
+        t0 = time.perf_counter()
+        c0, _, _, _ = oracle.counts(g.beg, g.end, g.adj, 0, nthreads=0, sources=src)
+        c1, _, _, _ = oracle.counts(g.beg, g.end, g.adj, 1, nthreads=0, sources=src)
+        dt = time.perf_counter() - t0
+        nnz = int(c0[src].sum() + c1[src].sum() + src.shape[0])
+        return nnz, dt, src.shape[0]
+
+    k = step_hint or max(1, n // 64)
+    nnz, dt, ns = run(k)
+    while dt < budget_s / 4 and k > 1:
+        k = max(1, int(k * max(dt, 1e-3) / (budget_s / 2)) if dt > 0 else k // 8)
+        k = max(1, min(k, n))
+        nnz, dt, ns = run(k)
+        if dt >= budget_s / 4:
+            break
+    return nnz / dt, cores, f"every {k}-th line of both passes ({ns} of {n} sources), {dt:.2f} s", k
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    g, cfg = workload(args)
+    per_step = max(args.cpu_seconds / max(args.steps, 1), 1.0)
+    # one calibration + warm-up runs
+    rate, cores, desc, k = cpu_sample(g, per_step)
+    for _ in range(max(args.warmup - 1, 0)):
+        cpu_sample(g, per_step, step_hint=k)
+    rates = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r, cores, desc, _ = cpu_sample(g, per_step, step_hint=k)
+        rates.append(r)
+    wall = time.perf_counter() - t0
+    value = statistics.mean(rates)
+    line = {
+        "metric": "nnz(L+U)/s", "value": value, "unit": "nnz/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * wall / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded generator)", "impl": "reference",
+        "config": dict(cfg, sample=desc),
+        "cpu_baseline": {"value": value, "unit": "nnz/s", "cores": cores, "kind": "port",
+                         "sample": desc},
+        "e2e": {"value": value, "unit": "nnz/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    import gsofa_b200
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    g, cfg = workload(args)
+    ctx = gsofa_b200.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    m = ctx.upload(g)
+    params = gsofa_b200.Params.default(want_pattern=1, flags=gsofa_b200.FLAG_NO_DOWNLOAD,
+                                       reuse=args.reuse, block_size=args.block,
+                                       threads_per_source=args.lanes, ctas_per_sm=args.ctas_per_sm)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    res = None
+    for _ in range(max(args.warmup, 0)):
+        res = ctx.symbfact(m, params)
+    if res is None:
+        res = ctx.symbfact(m, params)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- device-resident timed region ------------------------------------
+    kernel_ms = []
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(args.steps):
+            if i:
+                flush.fill_(i & 0xff)      # evict L2 between steps
+            r = ctx.symbfact(m, params)
+            kernel_ms.append(r.kernel_ms)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    t_ms = e0.elapsed_time(e1)
+    t_max = t_ms
+    if world > 1:
+        tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    nnz_lu = res.nnz_lu
+    value = world * args.steps * nnz_lu / (t_max / 1000.0)
+    facts = world * args.steps / (t_max / 1000.0)
+
+    # ---- end-to-end through the public API ----------------------------------
+    e2e = None
+    if not args.no_e2e:
+        pb = torch.from_numpy(g.beg).pin_memory()
+        pe = torch.from_numpy(g.end).pin_memory()
+        pa = torch.from_numpy(g.adj).pin_memory()
+        pe2e = gsofa_b200.Params.default(want_pattern=1, reuse=args.reuse, block_size=args.block,
+                                         threads_per_source=args.lanes, ctas_per_sm=args.ctas_per_sm)
+        out = None
+        for _ in range(1):   # warm the host-side allocations
+            mm = ctx.upload(pb.numpy(), pe.numpy(), pa.numpy())
+            out = ctx.symbfact(mm, pe2e)
+            mm.free()
+        k2 = max(1, min(args.steps, 3))
+        barrier()
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for i in range(k2):
+            if i:
+                flush.fill_(i & 0xff)
+            mm = ctx.upload(pb.numpy(), pe.numpy(), pa.numpy())
+            out = ctx.symbfact(mm, pe2e)
+            mm.free()
+        f1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        te = f0.elapsed_time(f1)
+        if world > 1:
+            tt = torch.tensor([te], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            te = float(tt.item())
+        assert out.nnz_lu == nnz_lu and out.fill_count == res.fill_count
+        h2d = (2 * g.n + g.nnz) * 4
+        d2h = 4 * (out.nnz_u + out.nnz_l) + 2 * 8 * (g.n + 1) + 3 * 4 * g.n + 4 * out.n_supernodes
+        e2e = {"value": world * k2 * nnz_lu / (te / 1000.0), "unit": "nnz/s", "steps": k2,
+               "ms_per_step": te / k2, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+    # ---- roofline of the factorization kernel --------------------------------
+    peak, peak_kind = hbm_peak()
+    kms = statistics.mean(kernel_ms)
+    n = g.n
+    b_alg = 8 * res.x_total + 8 * res.e_insp + 4 * nnz_lu + 8 * n
+    achieved = b_alg / (kms / 1000.0) / 1e9
+    traffic = traffic_per_launch(cfg["workload"])
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+            "algorithmic_bytes": int(b_alg), "kernel_ms": kms, "x_total": res.x_total,
+            "e_insp": res.e_insp, "edges_inspected": res.edges_inspected,
+            "work_ratio": res.edges_inspected / max(res.e_insp, 1)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, cores, desc, _ = cpu_sample(g, args.cpu_seconds)
+        cpu = {"value": rate, "unit": "nnz/s", "cores": cores, "kind": "port", "sample": desc}
+
+    if rank == 0:
+        line = {
+            "metric": "nnz(L+U)/s", "value": value, "unit": "nnz/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded generator)",
+            "config": dict(cfg, nnz_lu=int(nnz_lu), fill_count=int(res.fill_count),
+                           supernodes=int(res.n_supernodes), pattern="on device",
+                           reuse=args.reuse, l2="flushed between steps (256 MiB write)",
+                           parallelism=f"independent factorization per rank x{world}"),
+            "factorizations_per_s": facts,
+            "e2e": e2e,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "gpu_launches": args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,350 @@
+"""gsofa_b200 -- B200-native symbolic LU factorization (gSoFa's fill traversal).
+
+Python face of ``libgsofa.so`` (C ABI in ``include/gsofa.h``).  It mirrors the
+reference's interface for this path:
+
+* :func:`symbfact_min_id` -- the reference's host entry
+  ``symbfact_min_id(args, argv, myrank, fill_count, time)``
+  (without_space_optimization/symbfact.cuh:991) with the same argv contract;
+  it returns ``(fill_count, time_ms)`` and raises :class:`GsofaError` where the
+  reference would call ``exit()``.
+* :class:`Context` -- device context with device-resident matrices,
+  :meth:`Context.symbfact` for one matrix and :meth:`Context.symbfact_batch`
+  for many matrices in one persistent launch.
+
+All computation runs in the CUDA library; there is no CPU fallback.  Loading
+fails loudly when ``libgsofa.so`` has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import os
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from .matgen import Graph
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgsofa.so")
+
+OK = 0
+STATUS_NAMES = {
+    0: "ok", 1: "invalid input", 2: "out of memory", 3: "queue or pattern pool overflow",
+    4: "device wait timed out", 5: "CUDA error", 6: "input file error",
+    7: "unsupported device or size",
+}
+
+FLAG_NO_DOWNLOAD = 0x1
+FLAG_DEVICE_TIMING = 0x2
+
+
+class GsofaError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = int(status)
+        msg = STATUS_NAMES.get(self.status, f"status {status}")
+        super().__init__(f"{what}: {msg}" if what else msg)
+
+
+class Params(ctypes.Structure):
+    """gsofa_params; zero fields mean 'choose automatically'."""
+
+    _fields_ = [
+        ("src_chunk", ctypes.c_int32),
+        ("block_size", ctypes.c_int32),
+        ("threads_per_source", ctypes.c_int32),
+        ("ctas_per_sm", ctypes.c_int32),
+        ("queue_capacity", ctypes.c_int64),
+        ("pool_capacity", ctypes.c_int64),
+        ("max_supernode_size", ctypes.c_int32),
+        ("want_pattern", ctypes.c_int32),
+        ("reuse", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
+        ("part_count", ctypes.c_int32),
+        ("part_index", ctypes.c_int32),
+    ]
+
+    @classmethod
+    def default(cls, **kw) -> "Params":
+        p = cls()
+        lib().gsofa_default_params(ctypes.byref(p))
+        for k, v in kw.items():
+            if not hasattr(p, k):
+                raise TypeError(f"unknown parameter {k!r}")
+            setattr(p, k, int(v))
+        return p
+
+
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+
+
+class _CResult(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int32),
+        ("n_supernodes", ctypes.c_int32),
+        ("fill_count", ctypes.c_uint64),
+        ("nnz_lu", ctypes.c_uint64),
+        ("nnz_u", ctypes.c_uint64),
+        ("nnz_l", ctypes.c_uint64),
+        ("edges_inspected", ctypes.c_uint64),
+        ("sources", ctypes.c_uint64),
+        ("x_total", ctypes.c_uint64),
+        ("e_insp", ctypes.c_uint64),
+        ("kernel_ms", ctypes.c_double),
+        ("u_row_count", _i32p),
+        ("l_col_count", _i32p),
+        ("l_row_count", _i32p),
+        ("sn_start", _i32p),
+        ("u_ptr", _i64p),
+        ("u_idx", _i32p),
+        ("l_ptr", _i64p),
+        ("l_idx", _i32p),
+        ("internal", ctypes.c_void_p),
+    ]
+
+
+@dataclasses.dataclass
+class Result:
+    """One factorization: counts, supernodes and (optionally) the pattern.
+
+    ``u_ptr/u_idx``: U by rows (sorted columns > s of row s).
+    ``l_ptr/l_idx``: L by columns (sorted rows > j of column j).
+    """
+
+    n: int
+    fill_count: int
+    nnz_lu: int
+    nnz_u: int
+    nnz_l: int
+    n_supernodes: int
+    edges_inspected: int
+    sources: int
+    x_total: int
+    e_insp: int
+    kernel_ms: float
+    u_row_count: Optional[np.ndarray] = None
+    l_col_count: Optional[np.ndarray] = None
+    l_row_count: Optional[np.ndarray] = None
+    sn_start: Optional[np.ndarray] = None
+    u_ptr: Optional[np.ndarray] = None
+    u_idx: Optional[np.ndarray] = None
+    l_ptr: Optional[np.ndarray] = None
+    l_idx: Optional[np.ndarray] = None
+
+
+_lib = None
+
+
+def lib():
+    """Loads libgsofa.so; raises when it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing; build it with `python -m gsofa_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    L.gsofa_status_str.argtypes = [ctypes.c_int]
+    L.gsofa_status_str.restype = ctypes.c_char_p
+    L.gsofa_abi_version.restype = ctypes.c_int
+    L.gsofa_default_params.argtypes = [ctypes.POINTER(Params)]
+    L.gsofa_default_params.restype = None
+    L.gsofa_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_size_t]
+    L.gsofa_create.restype = ctypes.c_int
+    L.gsofa_destroy.argtypes = [vp]
+    L.gsofa_destroy.restype = None
+    L.gsofa_set_stream.argtypes = [vp, vp]
+    L.gsofa_set_stream.restype = ctypes.c_int
+    L.gsofa_read_text.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                  _i32p, _i64p, ctypes.POINTER(_i32p), ctypes.POINTER(_i32p),
+                                  ctypes.POINTER(_i32p)]
+    L.gsofa_read_text.restype = ctypes.c_int
+    L.gsofa_free.argtypes = [vp]
+    L.gsofa_free.restype = None
+    L.gsofa_upload.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, _i32p, _i32p, _i32p,
+                               ctypes.POINTER(vp)]
+    L.gsofa_upload.restype = ctypes.c_int
+    L.gsofa_matrix_free.argtypes = [vp]
+    L.gsofa_matrix_free.restype = None
+    L.gsofa_matrix_n.argtypes = [vp]
+    L.gsofa_matrix_n.restype = ctypes.c_int32
+    L.gsofa_symbfact.argtypes = [vp, vp, ctypes.POINTER(Params), ctypes.POINTER(_CResult)]
+    L.gsofa_symbfact.restype = ctypes.c_int
+    L.gsofa_symbfact_batch.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.POINTER(Params),
+                                       ctypes.POINTER(_CResult)]
+    L.gsofa_symbfact_batch.restype = ctypes.c_int
+    L.gsofa_result_free.argtypes = [ctypes.POINTER(_CResult)]
+    L.gsofa_result_free.restype = None
+    L.gsofa_predict_scratch_bytes.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(Params)]
+    L.gsofa_predict_scratch_bytes.restype = ctypes.c_size_t
+    L.gsofa_symbfact_min_id.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double)]
+    L.gsofa_symbfact_min_id.restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def _check(status: int, what: str = "") -> None:
+    if status != OK:
+        raise GsofaError(status, what)
+
+
+def _arr(ptr, count: int, dtype) -> Optional[np.ndarray]:
+    if not ptr or count < 0:
+        return None
+    if count == 0:
+        return np.zeros(0, dtype)
+    return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dtype, copy=True)
+
+
+def _convert(r: _CResult) -> Result:
+    n = int(r.n)
+    out = Result(n=n, fill_count=int(r.fill_count), nnz_lu=int(r.nnz_lu), nnz_u=int(r.nnz_u),
+                 nnz_l=int(r.nnz_l), n_supernodes=int(r.n_supernodes),
+                 edges_inspected=int(r.edges_inspected), sources=int(r.sources),
+                 x_total=int(r.x_total), e_insp=int(r.e_insp), kernel_ms=float(r.kernel_ms))
+    out.u_row_count = _arr(r.u_row_count, n, np.int32)
+    out.l_col_count = _arr(r.l_col_count, n, np.int32)
+    out.l_row_count = _arr(r.l_row_count, n, np.int32)
+    out.sn_start = _arr(r.sn_start, int(r.n_supernodes), np.int32)
+    out.u_ptr = _arr(r.u_ptr, n + 1, np.int64)
+    out.l_ptr = _arr(r.l_ptr, n + 1, np.int64)
+    out.u_idx = _arr(r.u_idx, int(r.nnz_u), np.int32)
+    out.l_idx = _arr(r.l_idx, int(r.nnz_l), np.int32)
+    return out
+
+
+class Matrix:
+    """A device-resident matrix (G and its transpose) owned by a Context."""
+
+    def __init__(self, ctx: "Context", handle: ctypes.c_void_p, n: int, nnz: int):
+        self._ctx = ctx
+        self._h = handle
+        self.n = n
+        self.nnz = nnz
+
+    def free(self) -> None:
+        if self._h:
+            lib().gsofa_matrix_free(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        if not self._h:
+            raise GsofaError(1, "matrix already freed")
+        return self._h
+
+
+class Context:
+    """A device context: stream, scratch pools and uploaded matrices."""
+
+    def __init__(self, device: int = 0, mem_budget_bytes: int = 0):
+        h = ctypes.c_void_p()
+        _check(lib().gsofa_create(ctypes.byref(h), int(device), int(mem_budget_bytes)), "gsofa_create")
+        self._h = h
+        self._mats: List[Matrix] = []
+
+    def set_stream(self, cuda_stream: int) -> None:
+        """Issue work on this cudaStream_t handle (0: the context's own)."""
+        _check(lib().gsofa_set_stream(self._h, ctypes.c_void_p(int(cuda_stream) or None)), "gsofa_set_stream")
+
+    def close(self) -> None:
+        if self._h:
+            for m in self._mats:
+                m._h = None
+            lib().gsofa_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, beg, end=None, adj=None) -> Matrix:
+        """Uploads a matrix given as a Graph or as (beg, end, adj) int32 arrays."""
+        if isinstance(beg, Graph):
+            g = beg
+            beg, end, adj = g.beg, g.end, g.adj
+        beg = np.ascontiguousarray(beg, dtype=np.int32)
+        end = np.ascontiguousarray(end, dtype=np.int32)
+        adj = np.ascontiguousarray(adj, dtype=np.int32)
+        if beg.shape != end.shape:
+            raise GsofaError(1, "beg and end differ in length")
+        h = ctypes.c_void_p()
+        _check(lib().gsofa_upload(self._h, beg.shape[0], adj.shape[0], beg.ctypes.data_as(_i32p),
+                                  end.ctypes.data_as(_i32p), adj.ctypes.data_as(_i32p),
+                                  ctypes.byref(h)), "gsofa_upload")
+        m = Matrix(self, h, int(beg.shape[0]), int(adj.shape[0]))
+        self._mats.append(m)
+        return m
+
+    def symbfact(self, m: Matrix, params: Optional[Params] = None, **kw) -> Result:
+        p = params if params is not None else Params.default(**kw)
+        r = _CResult()
+        _check(lib().gsofa_symbfact(self._h, m.handle, ctypes.byref(p), ctypes.byref(r)), "gsofa_symbfact")
+        try:
+            return _convert(r)
+        finally:
+            lib().gsofa_result_free(ctypes.byref(r))
+
+    def symbfact_batch(self, mats: Sequence[Matrix], params: Optional[Params] = None, **kw) -> List[Result]:
+        p = params if params is not None else Params.default(**kw)
+        k = len(mats)
+        hs = (ctypes.c_void_p * k)(*[m.handle for m in mats])
+        rs = (_CResult * k)()
+        _check(lib().gsofa_symbfact_batch(self._h, k, hs, ctypes.byref(p), rs), "gsofa_symbfact_batch")
+        try:
+            return [_convert(rs[i]) for i in range(k)]
+        finally:
+            for i in range(k):
+                lib().gsofa_result_free(ctypes.byref(rs[i]))
+
+    def predict_scratch_bytes(self, n: int, nnz: int, params: Optional[Params] = None) -> int:
+        p = params if params is not None else Params.default()
+        return int(lib().gsofa_predict_scratch_bytes(self._h, int(n), int(nnz), ctypes.byref(p)))
+
+
+def read_text(beg_file: str, end_file: str, csr_file: str) -> Graph:
+    """Reads the reference's colbeg/colend/csr text files through the library."""
+    n = ctypes.c_int32()
+    nnz = ctypes.c_int64()
+    b, e, a = _i32p(), _i32p(), _i32p()
+    _check(lib().gsofa_read_text(beg_file.encode(), end_file.encode(), csr_file.encode(),
+                                 ctypes.byref(n), ctypes.byref(nnz), ctypes.byref(b), ctypes.byref(e),
+                                 ctypes.byref(a)), "gsofa_read_text")
+    try:
+        g = Graph(int(n.value), _arr(b, n.value, np.int32), _arr(e, n.value, np.int32),
+                  _arr(a, nnz.value, np.int32), os.path.basename(csr_file))
+    finally:
+        for p in (b, e, a):
+            lib().gsofa_free(ctypes.cast(p, ctypes.c_void_p))
+    return g
+
+
+def symbfact_min_id(argv: Sequence[str], myrank: int = 0):
+    """The reference entry point: returns (fill_count, time_ms) for argv
+    ``[prog, colbeg, colend, csr, N_GPU, (mem_GB, (max_supernode_size, GPUs_per_node))]``."""
+    enc = [str(a).encode() for a in argv]
+    arr = (ctypes.c_char_p * len(enc))(*enc)
+    fc = ctypes.c_uint64()
+    t = ctypes.c_double()
+    _check(lib().gsofa_symbfact_min_id(len(enc), arr, int(myrank), ctypes.byref(fc), ctypes.byref(t)),
+           "symbfact_min_id")
+    return int(fc.value), float(t.value)
+
+
+def exported_symbols() -> List[str]:
+    """Names of the C ABI entry points declared in include/gsofa.h."""
+    return ["gsofa_symbfact_min_id", "gsofa_status_str", "gsofa_abi_version", "gsofa_default_params",
+            "gsofa_create", "gsofa_destroy", "gsofa_set_stream", "gsofa_read_text", "gsofa_free", "gsofa_upload",
+            "gsofa_matrix_free", "gsofa_matrix_n", "gsofa_symbfact", "gsofa_symbfact_batch",
+            "gsofa_result_free", "gsofa_predict_scratch_bytes"]

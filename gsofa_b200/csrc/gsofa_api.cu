@@ -1,0 +1,832 @@
+// gsofa_api.cu -- host side of the B200 symbolic factorization (C ABI).
+//
+// Replaces the reference's host orchestration symbfact_min_id
+// (without_space_optimization/symbfact.cuh:991-1391,
+//  with_space_optimization/symbfact.cuh:1553-2583): file reading, device
+// selection, scratch sizing, the launch and the result report.  Unlike the
+// reference, nothing here exits the process; every failure is a status code.
+#include "../../include/gsofa.h"
+#include "gsofa_device.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace gsofa::dev;
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Small helpers
+
+struct CudaFail {
+    cudaError_t e;
+};
+
+#define GS_CUDA(x)                                                     \
+    do {                                                               \
+        cudaError_t _e = (x);                                          \
+        if (_e != cudaSuccess) throw CudaFail{_e};                     \
+    } while (0)
+
+thread_local char g_last_error[256];
+
+gsofa_status fail_cuda(cudaError_t e)
+{
+    std::snprintf(g_last_error, sizeof(g_last_error), "%s", cudaGetErrorString(e));
+    cudaGetLastError();
+    return (e == cudaErrorMemoryAllocation) ? GSOFA_ERR_OOM : GSOFA_ERR_CUDA;
+}
+
+// Grow-only device buffer owned by a context.
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct gsofa_ctx {
+    int device = 0;
+    int sm_count = 0;
+    size_t smem_optin = 0;
+    size_t budget = 0;
+    size_t held = 0;          // bytes of grow-only scratch currently held
+    cudaStream_t stream = nullptr;      // stream all work is issued on
+    cudaStream_t own_stream = nullptr;  // the context's own stream
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // job scratch
+    DevBuf queue, cnt, nxt, poff, gptr, lrow, snind, snlist, tiles, misc, pool, out, mats, ranges;
+    // upload staging
+    DevBuf st_beg, st_end, st_adj, st_tmp;
+    std::vector<gsofa_matrix *> matrices;
+
+    void *grow(DevBuf &b, size_t bytes)
+    {
+        bytes = std::max<size_t>(bytes, 256);
+        if (b.bytes >= bytes) return b.p;
+        if (b.p) {
+            GS_CUDA(cudaFree(b.p));
+            held -= b.bytes;
+            b.p = nullptr;
+            b.bytes = 0;
+        }
+        if (held + bytes > budget) throw CudaFail{cudaErrorMemoryAllocation};
+        GS_CUDA(cudaMalloc(&b.p, bytes));
+        b.bytes = bytes;
+        held += bytes;
+        return b.p;
+    }
+    void release(DevBuf &b)
+    {
+        if (b.p) {
+            cudaFree(b.p);
+            held -= b.bytes;
+        }
+        b.p = nullptr;
+        b.bytes = 0;
+    }
+};
+
+struct gsofa_matrix {
+    gsofa_ctx *ctx = nullptr;
+    int32_t n = 0;
+    int64_t nnz_in = 0;
+    int64_t nnz_g = 0;            // distinct off-diagonal entries kept
+    int32_t *d_gptr = nullptr, *d_gadj = nullptr;
+    int32_t *d_tptr = nullptr, *d_tadj = nullptr;
+    int32_t *d_orig_up = nullptr, *d_orig_lo = nullptr, *d_rawdeg = nullptr;
+    uint64_t orig_up = 0, orig_lo = 0;
+    int64_t last_pattern_total = -1;  // pool size the last run needed
+};
+
+namespace {
+
+struct ResultInternal {
+    // nothing yet; reserved for device-side views
+};
+
+int pick_block(int32_t max_n)
+{
+    if (max_n <= 8192) return 256;
+    return 512;
+}
+
+template <int BLOCK>
+void *factor_fn()
+{
+    return (void *)factor_kernel<BLOCK>;
+}
+
+void *factor_kernel_for(int block)
+{
+    switch (block) {
+    case 128: return factor_fn<128>();
+    case 256: return factor_fn<256>();
+    case 512: return factor_fn<512>();
+    case 1024: return factor_fn<1024>();
+    default: return nullptr;
+    }
+}
+
+void resolve_params(const gsofa_params *in, gsofa_params *p)
+{
+    gsofa_default_params(p);
+    if (in) *p = *in;
+}
+
+// Copies a device array [off, off+count) of T into a fresh malloc'd host array.
+template <class T>
+T *download(cudaStream_t st, const T *d, int64_t off, int64_t count)
+{
+    T *h = (T *)std::malloc((size_t)std::max<int64_t>(count, 1) * sizeof(T));
+    if (!h) throw std::bad_alloc();
+    if (count > 0)
+        GS_CUDA(cudaMemcpyAsync(h, d + off, (size_t)count * sizeof(T), cudaMemcpyDeviceToHost, st));
+    return h;
+}
+
+void free_result_arrays(gsofa_result *r)
+{
+    std::free(r->u_row_count);
+    std::free(r->l_col_count);
+    std::free(r->l_row_count);
+    std::free(r->sn_start);
+    std::free(r->u_ptr);
+    std::free(r->u_idx);
+    std::free(r->l_ptr);
+    std::free(r->l_idx);
+    r->u_row_count = r->l_col_count = r->l_row_count = r->sn_start = nullptr;
+    r->u_ptr = r->l_ptr = nullptr;
+    r->u_idx = r->l_idx = nullptr;
+}
+
+// The factorization of `count` matrices in one cooperative launch.
+gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
+                     const gsofa_params *pin, gsofa_result *out)
+{
+    gsofa_params p;
+    resolve_params(pin, &p);
+    if (count <= 0 || !mats || !out) return GSOFA_ERR_INVALID_INPUT;
+    for (int i = 0; i < count; i++) {
+        if (!mats[i] || mats[i]->ctx != ctx) return GSOFA_ERR_INVALID_INPUT;
+        std::memset(&out[i], 0, sizeof(gsofa_result));
+        out[i].n = mats[i]->n;
+    }
+    const int part_count = p.part_count > 1 ? p.part_count : 1;
+    const int part_index = p.part_count > 1 ? p.part_index : 0;
+    if (part_index < 0 || part_index >= part_count) return GSOFA_ERR_INVALID_INPUT;
+    const bool want_pattern = p.want_pattern != 0 && part_count == 1;
+    const int reuse = (p.reuse > 0 && part_count == 1) ? 1 : 0;
+
+    // line space and per-matrix descriptors
+    std::vector<MatDesc> md(count);
+    int64_t L = 0;
+    int32_t max_n = 1;
+    for (int i = 0; i < count; i++) {
+        md[i].n = mats[i]->n;
+        md[i].pad = 0;
+        md[i].line_base = L;
+        md[i].g[0] = PassGraph{mats[i]->d_gptr, mats[i]->d_gadj};
+        md[i].g[1] = PassGraph{mats[i]->d_tptr, mats[i]->d_tadj};
+        md[i].rawdeg = mats[i]->d_rawdeg;
+        L += mats[i]->n;
+        max_n = std::max(max_n, mats[i]->n);
+    }
+    if (L == 0) return GSOFA_OK;
+
+    // parameters
+    int block = p.block_size ? p.block_size : pick_block(max_n);
+    void *kfn = factor_kernel_for(block);
+    if (!kfn) return GSOFA_ERR_INVALID_INPUT;
+    int lanes = p.threads_per_source ? p.threads_per_source : 8;
+    if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) return GSOFA_ERR_INVALID_INPUT;
+    int chunk = p.src_chunk > 0 ? p.src_chunk : (reuse ? 32 : 1);
+
+    const int32_t bitmap_words = (max_n + 31) / 32;
+    const size_t smem = ((size_t)bitmap_words * 4 + 15) / 16 * 16;
+    if (smem + sizeof(SharedState) + 1024 > ctx->smem_optin) return GSOFA_ERR_UNSUPPORTED;
+    GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0;
+    GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, block, smem));
+    if (occ <= 0) return GSOFA_ERR_UNSUPPORTED;
+    int per_sm = p.ctas_per_sm > 0 ? std::min(p.ctas_per_sm, occ) : occ;
+    const int grid = per_sm * ctx->sm_count;
+
+    // work ranges: biggest matrices first
+    std::vector<int> order(count);
+    for (int i = 0; i < count; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return mats[x]->n > mats[y]->n; });
+    std::vector<Range> ranges;
+    int64_t npieces = 0;
+    for (int i : order) {
+        const int32_t n = mats[i]->n;
+        if (n <= part_index) continue;
+        Range r{};
+        r.mat = i;
+        r.chunk = chunk;
+        r.stride = part_count;
+        r.offset = part_index;
+        r.nj = (n - part_index + part_count - 1) / part_count;
+        r.piece_base = npieces;
+        r.npieces = 2 * (((int64_t)r.nj + chunk - 1) / chunk);
+        npieces += r.npieces;
+        ranges.push_back(r);
+    }
+
+    const int64_t qcap = std::max<int64_t>(p.queue_capacity, max_n);
+    const int64_t ntiles = (L + TILE - 1) / TILE;
+
+    // pool sizing: the last run's exact need, else a share of the budget
+    int64_t pool_cap = 0;
+    if (want_pattern) {
+        if (p.pool_capacity > 0) {
+            pool_cap = p.pool_capacity;
+        } else {
+            int64_t known = 0;
+            bool all_known = true;
+            for (int i = 0; i < count; i++) {
+                if (mats[i]->last_pattern_total < 0) all_known = false;
+                else known += mats[i]->last_pattern_total;
+            }
+            if (all_known) {
+                pool_cap = std::max<int64_t>(known, 1);
+            } else {
+                size_t freeb = ctx->budget > ctx->held ? ctx->budget - ctx->held : 0;
+                pool_cap = std::max<int64_t>((int64_t)(freeb / 4 / (2 * sizeof(int32_t))), 1 << 20);
+                pool_cap = std::min<int64_t>(pool_cap, (int64_t)1 << 31);
+            }
+        }
+    }
+
+    for (int attempt = 0; attempt < 2; attempt++) {
+        // scratch
+        int32_t *d_queue = (int32_t *)ctx->grow(ctx->queue, (size_t)grid * qcap * sizeof(int32_t));
+        int32_t *d_cnt = (int32_t *)ctx->grow(ctx->cnt, (size_t)2 * L * sizeof(int32_t));
+        uint8_t *d_nxt = (uint8_t *)ctx->grow(ctx->nxt, (size_t)2 * L);
+        int64_t *d_poff = (int64_t *)ctx->grow(ctx->poff, (size_t)2 * L * sizeof(int64_t));
+        int64_t *d_gptr = (int64_t *)ctx->grow(ctx->gptr, (size_t)2 * (L + 1) * sizeof(int64_t));
+        int32_t *d_lrow = (int32_t *)ctx->grow(ctx->lrow, (size_t)L * sizeof(int32_t));
+        uint8_t *d_snind = (uint8_t *)ctx->grow(ctx->snind, (size_t)L);
+        int32_t *d_sn = (int32_t *)ctx->grow(ctx->snlist, (size_t)L * sizeof(int32_t));
+        int64_t *d_tiles = (int64_t *)ctx->grow(ctx->tiles, (size_t)4 * ntiles * sizeof(int64_t));
+        // misc: piece counter, pool tail, counters[4], status
+        char *d_misc = (char *)ctx->grow(ctx->misc, 256);
+        unsigned long long *d_piece = (unsigned long long *)d_misc;
+        unsigned long long *d_tail = (unsigned long long *)(d_misc + 8);
+        unsigned long long *d_counters = (unsigned long long *)(d_misc + 16);
+        uint32_t *d_status = (uint32_t *)(d_misc + 64);
+        int32_t *d_pool = nullptr, *d_out = nullptr;
+        if (want_pattern) {
+            d_pool = (int32_t *)ctx->grow(ctx->pool, (size_t)pool_cap * sizeof(int32_t));
+            d_out = (int32_t *)ctx->grow(ctx->out, (size_t)pool_cap * sizeof(int32_t));
+        }
+        MatDesc *d_mats = (MatDesc *)ctx->grow(ctx->mats, md.size() * sizeof(MatDesc));
+        Range *d_ranges = (Range *)ctx->grow(ctx->ranges, std::max<size_t>(ranges.size(), 1) * sizeof(Range));
+
+        cudaStream_t st = ctx->stream;
+        GS_CUDA(cudaMemcpyAsync(d_mats, md.data(), md.size() * sizeof(MatDesc), cudaMemcpyHostToDevice, st));
+        if (!ranges.empty())
+            GS_CUDA(cudaMemcpyAsync(d_ranges, ranges.data(), ranges.size() * sizeof(Range),
+                                    cudaMemcpyHostToDevice, st));
+        GS_CUDA(cudaMemsetAsync(d_misc, 0, 256, st));
+        GS_CUDA(cudaMemsetAsync(d_lrow, 0, (size_t)L * sizeof(int32_t), st));
+        if (part_count > 1) {
+            GS_CUDA(cudaMemsetAsync(d_cnt, 0, (size_t)2 * L * sizeof(int32_t), st));
+            GS_CUDA(cudaMemsetAsync(d_nxt, 0, (size_t)2 * L, st));
+        }
+
+        JobArgs a{};
+        a.mats = d_mats;
+        a.nmats = count;
+        a.nranges = (int32_t)ranges.size();
+        a.ranges = d_ranges;
+        a.npieces = npieces;
+        a.piece_counter = d_piece;
+        a.queue = d_queue;
+        a.qcap = qcap;
+        a.bitmap_words = bitmap_words;
+        a.lanes = lanes;
+        a.reuse = reuse;
+        a.want_pattern = want_pattern ? 1 : 0;
+        a.max_sn = p.max_supernode_size;
+        a.L = L;
+        a.cnt = d_cnt;
+        a.nxt = d_nxt;
+        a.poff = d_poff;
+        a.pool = d_pool;
+        a.pool_cap = pool_cap;
+        a.pool_tail = d_tail;
+        a.gptr = d_gptr;
+        a.out = d_out;
+        a.lrow = d_lrow;
+        a.snind = d_snind;
+        a.sn_list = d_sn;
+        a.ntiles = ntiles;
+        a.tile_sum = d_tiles;
+        a.tile_last = d_tiles + 2 * ntiles;
+        a.tile_sn = d_tiles + 3 * ntiles;
+        a.counters = d_counters;
+        a.status = d_status;
+
+        void *args[] = {&a};
+        GS_CUDA(cudaEventRecord(ctx->ev0, st));
+        GS_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(block), args, smem, st));
+        GS_CUDA(cudaEventRecord(ctx->ev1, st));
+
+        unsigned long long h_misc[9];
+        GS_CUDA(cudaMemcpyAsync(h_misc, d_misc, 72, cudaMemcpyDeviceToHost, st));
+        int64_t tot[2];
+        GS_CUDA(cudaMemcpyAsync(&tot[0], d_gptr + L, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        GS_CUDA(cudaMemcpyAsync(&tot[1], d_gptr + (L + 1) + L, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        GS_CUDA(cudaStreamSynchronize(st));
+        float ms = 0.f;
+        GS_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        const uint32_t status = (uint32_t)(h_misc[8] & 0xffffffffu);
+        const unsigned long long edges = h_misc[2], nsrc = h_misc[3], nsn = h_misc[4];
+        const unsigned long long xtot = h_misc[5], einsp = h_misc[6];
+
+        if (status & ERR_QUEUE_OVERFLOW) return GSOFA_ERR_QUEUE_OVERFLOW;
+        if (want_pattern && (status & ERR_POOL_OVERFLOW)) {
+            if (attempt == 0) {
+                pool_cap = std::max<int64_t>(tot[0] + tot[1], 1);
+                continue;   // rerun with the exact pool the counts ask for
+            }
+            return GSOFA_ERR_QUEUE_OVERFLOW;
+        }
+
+        // per-matrix results
+        std::vector<int64_t> gp0(count + 1), gp1(count + 1);
+        std::vector<int32_t> snl;
+        const bool download_lines = !(p.flags & GSOFA_FLAG_NO_DOWNLOAD);
+        for (int i = 0; i < count; i++) {
+            int64_t lb = md[i].line_base, n = md[i].n;
+            int64_t v[4];
+            GS_CUDA(cudaMemcpyAsync(&v[0], d_gptr + lb, 8, cudaMemcpyDeviceToHost, st));
+            GS_CUDA(cudaMemcpyAsync(&v[1], d_gptr + lb + n, 8, cudaMemcpyDeviceToHost, st));
+            GS_CUDA(cudaMemcpyAsync(&v[2], d_gptr + (L + 1) + lb, 8, cudaMemcpyDeviceToHost, st));
+            GS_CUDA(cudaMemcpyAsync(&v[3], d_gptr + (L + 1) + lb + n, 8, cudaMemcpyDeviceToHost, st));
+            GS_CUDA(cudaStreamSynchronize(st));
+            gsofa_result &r = out[i];
+            r.nnz_u = (uint64_t)(v[1] - v[0]);
+            r.nnz_l = (uint64_t)(v[3] - v[2]);
+            r.nnz_lu = r.nnz_u + r.nnz_l + (uint64_t)n;
+            r.kernel_ms = ms;
+            r.edges_inspected = edges;
+            r.sources = nsrc;
+            r.x_total = xtot;
+            r.e_insp = einsp;
+            if (part_count == 1) {
+                r.fill_count = r.nnz_u - mats[i]->orig_up + r.nnz_l - mats[i]->orig_lo;
+                const_cast<gsofa_matrix *>(mats[i])->last_pattern_total = (int64_t)(r.nnz_u + r.nnz_l);
+            }
+            if (download_lines) {
+                r.u_row_count = download(st, d_cnt, lb, n);
+                r.l_col_count = download(st, d_cnt, L + lb, n);
+                r.l_row_count = download(st, d_lrow, lb, n);
+            }
+            if (want_pattern && download_lines) {
+                r.u_ptr = download(st, d_gptr, lb, n + 1);
+                r.l_ptr = download(st, d_gptr, (L + 1) + lb, n + 1);
+                r.u_idx = download(st, d_out, v[0], v[1] - v[0]);
+                r.l_idx = download(st, d_out, tot[0] + v[2], v[3] - v[2]);
+            }
+        }
+        if (download_lines || true) {
+            snl.resize((size_t)nsn);
+            if (nsn) GS_CUDA(cudaMemcpyAsync(snl.data(), d_sn, nsn * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        }
+        GS_CUDA(cudaStreamSynchronize(st));
+        for (int i = 0; i < count; i++) {
+            gsofa_result &r = out[i];
+            const int64_t lb = md[i].line_base, n = md[i].n;
+            auto b = std::lower_bound(snl.begin(), snl.end(), (int32_t)lb);
+            auto e = std::lower_bound(snl.begin(), snl.end(), (int32_t)(lb + n));
+            r.n_supernodes = (int32_t)(e - b);
+            if (download_lines) {
+                r.sn_start = (int32_t *)std::malloc(std::max<size_t>((size_t)(e - b), 1) * sizeof(int32_t));
+                if (!r.sn_start) throw std::bad_alloc();
+                for (auto it = b; it != e; ++it) r.sn_start[it - b] = *it - (int32_t)lb;
+            }
+            if (want_pattern && download_lines) {
+                const int64_t u0 = r.u_ptr[0], l0 = r.l_ptr[0];
+                for (int64_t s = 0; s <= n; s++) { r.u_ptr[s] -= u0; r.l_ptr[s] -= l0; }
+            }
+            if (part_count > 1) {
+                // fills of the processed lines: subtract their original entries
+                std::vector<int32_t> ou((size_t)n), ol((size_t)n);
+                GS_CUDA(cudaMemcpy(ou.data(), mats[i]->d_orig_up, n * 4, cudaMemcpyDeviceToHost));
+                GS_CUDA(cudaMemcpy(ol.data(), mats[i]->d_orig_lo, n * 4, cudaMemcpyDeviceToHost));
+                uint64_t o = 0;
+                for (int64_t s = part_index; s < n; s += part_count) o += (uint64_t)ou[s] + (uint64_t)ol[s];
+                r.fill_count = r.nnz_u + r.nnz_l - o;
+            }
+        }
+        return GSOFA_OK;
+    }
+    return GSOFA_ERR_QUEUE_OVERFLOW;
+}
+
+}  // namespace
+
+// ============================================================================
+// C ABI
+
+extern "C" {
+
+const char *gsofa_status_str(gsofa_status s)
+{
+    switch (s) {
+    case GSOFA_OK: return "ok";
+    case GSOFA_ERR_INVALID_INPUT: return "invalid input";
+    case GSOFA_ERR_OOM: return "out of memory";
+    case GSOFA_ERR_QUEUE_OVERFLOW: return "queue or pattern pool overflow";
+    case GSOFA_ERR_TIMEOUT: return "device wait timed out";
+    case GSOFA_ERR_CUDA: return "CUDA error";
+    case GSOFA_ERR_IO: return "input file error";
+    case GSOFA_ERR_UNSUPPORTED: return "unsupported device or size";
+    }
+    return "unknown status";
+}
+
+int gsofa_abi_version(void) { return GSOFA_ABI_VERSION; }
+
+void gsofa_default_params(gsofa_params *p)
+{
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->want_pattern = 1;
+    p->reuse = 0;
+    p->part_count = 1;
+}
+
+gsofa_status gsofa_create(gsofa_ctx **out, int device, size_t mem_budget_bytes)
+{
+    if (!out) return GSOFA_ERR_INVALID_INPUT;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return GSOFA_ERR_UNSUPPORTED;
+    }
+    if (device < 0 || device >= ndev) return GSOFA_ERR_INVALID_INPUT;
+    gsofa_ctx *c = new (std::nothrow) gsofa_ctx();
+    if (!c) return GSOFA_ERR_OOM;
+    try {
+        c->device = device;
+        GS_CUDA(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        GS_CUDA(cudaGetDeviceProperties(&prop, device));
+        if (prop.major < 10 || !prop.cooperativeLaunch) {
+            delete c;
+            return GSOFA_ERR_UNSUPPORTED;
+        }
+        c->sm_count = prop.multiProcessorCount;
+        c->smem_optin = prop.sharedMemPerBlockOptin;
+        size_t fr = 0, tot = 0;
+        GS_CUDA(cudaMemGetInfo(&fr, &tot));
+        c->budget = mem_budget_bytes ? mem_budget_bytes : (size_t)(0.9 * (double)fr);
+        GS_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+        c->stream = c->own_stream;
+        GS_CUDA(cudaEventCreate(&c->ev0));
+        GS_CUDA(cudaEventCreate(&c->ev1));
+    } catch (CudaFail &f) {
+        gsofa_destroy(c);
+        return fail_cuda(f.e);
+    }
+    *out = c;
+    return GSOFA_OK;
+}
+
+void gsofa_matrix_free(gsofa_matrix *m)
+{
+    if (!m) return;
+    gsofa_ctx *c = m->ctx;
+    if (c) {
+        cudaSetDevice(c->device);
+        auto &v = c->matrices;
+        v.erase(std::remove(v.begin(), v.end(), m), v.end());
+    }
+    cudaFree(m->d_gptr);
+    cudaFree(m->d_gadj);
+    cudaFree(m->d_tptr);
+    cudaFree(m->d_tadj);
+    cudaFree(m->d_orig_up);
+    cudaFree(m->d_orig_lo);
+    cudaFree(m->d_rawdeg);
+    delete m;
+}
+
+void gsofa_destroy(gsofa_ctx *c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    while (!c->matrices.empty()) gsofa_matrix_free(c->matrices.back());
+    DevBuf *bufs[] = {&c->queue, &c->cnt, &c->nxt, &c->poff, &c->gptr, &c->lrow, &c->snind,
+                      &c->snlist, &c->tiles, &c->misc, &c->pool, &c->out, &c->mats, &c->ranges,
+                      &c->st_beg, &c->st_end, &c->st_adj, &c->st_tmp};
+    for (DevBuf *b : bufs) c->release(*b);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+}
+
+gsofa_status gsofa_set_stream(gsofa_ctx *c, void *cuda_stream)
+{
+    if (!c) return GSOFA_ERR_INVALID_INPUT;
+    c->stream = cuda_stream ? (cudaStream_t)cuda_stream : c->own_stream;
+    return GSOFA_OK;
+}
+
+void gsofa_free(void *p) { std::free(p); }
+
+int32_t gsofa_matrix_n(const gsofa_matrix *m) { return m ? m->n : -1; }
+
+gsofa_status gsofa_read_text(const char *beg_file, const char *end_file, const char *csr_file,
+                             int32_t *n_out, int64_t *nnz_out, int32_t **beg_out,
+                             int32_t **end_out, int32_t **adj_out)
+{
+    if (!beg_file || !end_file || !csr_file || !n_out || !nnz_out || !beg_out || !end_out || !adj_out)
+        return GSOFA_ERR_INVALID_INPUT;
+    *beg_out = *end_out = *adj_out = nullptr;
+    FILE *f = std::fopen(csr_file, "r");
+    if (!f) return GSOFA_ERR_IO;
+    long long nnz = -1, n = -1;
+    if (std::fscanf(f, "%lld", &nnz) != 1 || std::fscanf(f, "%lld", &n) != 1 || nnz < 0 || n < 0 ||
+        n > INT32_MAX || nnz > INT32_MAX) {
+        std::fclose(f);
+        return GSOFA_ERR_IO;
+    }
+    int32_t *adj = (int32_t *)std::malloc((size_t)std::max<long long>(nnz, 1) * 4);
+    int32_t *beg = (int32_t *)std::malloc((size_t)std::max<long long>(n, 1) * 4);
+    int32_t *end = (int32_t *)std::malloc((size_t)std::max<long long>(n, 1) * 4);
+    if (!adj || !beg || !end) {
+        std::fclose(f);
+        std::free(adj); std::free(beg); std::free(end);
+        return GSOFA_ERR_OOM;
+    }
+    auto read_ints = [](FILE *fp, int32_t *dst, long long cnt) -> bool {
+        for (long long i = 0; i < cnt; i++) {
+            long long x;
+            if (std::fscanf(fp, "%lld", &x) != 1 || x < INT32_MIN || x > INT32_MAX) return false;
+            dst[i] = (int32_t)x;
+        }
+        return true;
+    };
+    bool ok = read_ints(f, adj, nnz);
+    std::fclose(f);
+    if (ok) {
+        FILE *fb = std::fopen(beg_file, "r");
+        ok = fb && read_ints(fb, beg, n);
+        if (fb) std::fclose(fb);
+    }
+    if (ok) {
+        FILE *fe = std::fopen(end_file, "r");
+        ok = fe && read_ints(fe, end, n);
+        if (fe) std::fclose(fe);
+    }
+    if (!ok) {
+        std::free(adj); std::free(beg); std::free(end);
+        return GSOFA_ERR_IO;
+    }
+    *n_out = (int32_t)n;
+    *nnz_out = nnz;
+    *beg_out = beg;
+    *end_out = end;
+    *adj_out = adj;
+    return GSOFA_OK;
+}
+
+gsofa_status gsofa_upload(gsofa_ctx *c, int32_t n, int64_t nnz, const int32_t *beg,
+                          const int32_t *end, const int32_t *adj, gsofa_matrix **out)
+{
+    if (!c || !out || n < 0 || nnz < 0 || nnz > INT32_MAX) return GSOFA_ERR_INVALID_INPUT;
+    if ((n > 0 && (!beg || !end)) || (nnz > 0 && !adj)) return GSOFA_ERR_INVALID_INPUT;
+    *out = nullptr;
+    gsofa_matrix *m = new (std::nothrow) gsofa_matrix();
+    if (!m) return GSOFA_ERR_OOM;
+    m->ctx = c;
+    m->n = n;
+    m->nnz_in = nnz;
+    try {
+        GS_CUDA(cudaSetDevice(c->device));
+        cudaStream_t st = c->stream;
+        const size_t nb = (size_t)std::max<int32_t>(n, 1) * 4;
+        int32_t *d_beg = (int32_t *)c->grow(c->st_beg, nb);
+        int32_t *d_end = (int32_t *)c->grow(c->st_end, nb);
+        int32_t *d_adj = (int32_t *)c->grow(c->st_adj, (size_t)std::max<int64_t>(nnz, 1) * 4);
+        // tmp: deg[n] | indeg[n+1] | tcursor[n+1] | tile sums | counts | status
+        const int64_t scan_tiles = ((int64_t)n + 1 + 255) / 256 + 1;
+        const size_t ints_bytes = ((size_t)(3 * ((int64_t)n + 1)) * 4 + 15) / 16 * 16;
+        const size_t tmp_bytes = ints_bytes + (size_t)(2 * scan_tiles) * 8 + 64;
+        char *tmp = (char *)c->grow(c->st_tmp, tmp_bytes);
+        int32_t *d_deg = (int32_t *)tmp;
+        int32_t *d_indeg = d_deg + (n + 1);
+        int32_t *d_tcur = d_indeg + (n + 1);
+        int64_t *d_tsum = (int64_t *)(tmp + ints_bytes);
+        unsigned long long *d_counts = (unsigned long long *)(d_tsum + 2 * scan_tiles);
+        uint32_t *d_status = (uint32_t *)(d_counts + 4);
+
+        GS_CUDA(cudaMalloc(&m->d_gptr, (size_t)(n + 1) * 4));
+        GS_CUDA(cudaMalloc(&m->d_tptr, (size_t)(n + 1) * 4));
+        GS_CUDA(cudaMalloc(&m->d_orig_up, nb));
+        GS_CUDA(cudaMalloc(&m->d_orig_lo, nb));
+        GS_CUDA(cudaMalloc(&m->d_rawdeg, nb));
+        c->matrices.push_back(m);
+
+        if (n > 0) {
+            GS_CUDA(cudaMemcpyAsync(d_beg, beg, (size_t)n * 4, cudaMemcpyHostToDevice, st));
+            GS_CUDA(cudaMemcpyAsync(d_end, end, (size_t)n * 4, cudaMemcpyHostToDevice, st));
+        }
+        if (nnz > 0) GS_CUDA(cudaMemcpyAsync(d_adj, adj, (size_t)nnz * 4, cudaMemcpyHostToDevice, st));
+        GS_CUDA(cudaMemsetAsync(d_indeg, 0, (size_t)(n + 1) * 4, st));
+        GS_CUDA(cudaMemsetAsync(d_counts, 0, 64, st));
+        GS_CUDA(cudaMemsetAsync(m->d_orig_lo, 0, nb, st));
+        GS_CUDA(cudaMemsetAsync(d_deg, 0, (size_t)(n + 1) * 4, st));
+
+        UploadArgs u{};
+        u.n = n;
+        u.nnz = nnz;
+        u.beg = d_beg;
+        u.end = d_end;
+        u.adj = d_adj;
+        u.deg = d_deg;
+        u.indeg = d_indeg;
+        u.orig_up = m->d_orig_up;
+        u.orig_lo = m->d_orig_lo;
+        u.rawdeg = m->d_rawdeg;
+        u.counts = d_counts;
+        u.status = d_status;
+        const int ub = 256;
+        const int ugrid = (int)std::min<int64_t>(std::max<int64_t>(((int64_t)n * 32 + ub - 1) / ub, 1),
+                                                 (int64_t)c->sm_count * 16);
+        if (n > 0) {
+            upload_count_kernel<<<ugrid, ub, 0, st>>>(u);
+            GS_CUDA(cudaGetLastError());
+        }
+        // G offsets (from deg) and G^T offsets (from indeg)
+        int64_t tot[2] = {0, 0};
+        const int64_t ntl = ((int64_t)n + 255) / 256;
+        int32_t *scan_in[2] = {d_deg, d_indeg};
+        int32_t *scan_out[2] = {m->d_gptr, m->d_tptr};
+        for (int k = 0; k < 2; k++) {
+            int64_t *ts = d_tsum + k * scan_tiles;
+            int64_t *dt = (int64_t *)(d_counts + 2 + k);
+            if (ntl > 0) scan_tiles_kernel<256><<<(unsigned)ntl, 256, 0, st>>>(scan_in[k], n, ts);
+            scan_partials_kernel<256><<<1, 256, 0, st>>>(ts, ntl, dt);
+            scan_apply_kernel<256><<<(unsigned)std::max<int64_t>(ntl, 1), 256, 0, st>>>(scan_in[k], n, ts,
+                                                                                       scan_out[k], dt);
+            GS_CUDA(cudaGetLastError());
+        }
+        unsigned long long hc[5];
+        GS_CUDA(cudaMemcpyAsync(hc, d_counts, 5 * 8, cudaMemcpyDeviceToHost, st));
+        GS_CUDA(cudaStreamSynchronize(st));
+        uint32_t status = (uint32_t)(hc[4] & 0xffffffffu);
+        tot[0] = (int64_t)hc[2];
+        tot[1] = (int64_t)hc[3];
+        if (status & 1u) {
+            gsofa_matrix_free(m);
+            return GSOFA_ERR_INVALID_INPUT;
+        }
+        m->orig_up = hc[0];
+        m->orig_lo = hc[1];
+        m->nnz_g = tot[0];
+        GS_CUDA(cudaMalloc(&m->d_gadj, (size_t)std::max<int64_t>(tot[0], 1) * 4));
+        GS_CUDA(cudaMalloc(&m->d_tadj, (size_t)std::max<int64_t>(tot[1], 1) * 4));
+        GS_CUDA(cudaMemcpyAsync(d_tcur, m->d_tptr, (size_t)(n + 1) * 4, cudaMemcpyDeviceToDevice, st));
+        if (n > 0) {
+            upload_fill_kernel<<<ugrid, ub, 0, st>>>(u, m->d_gptr, m->d_gadj, d_tcur, m->d_tadj);
+            GS_CUDA(cudaGetLastError());
+        }
+        GS_CUDA(cudaStreamSynchronize(st));
+    } catch (CudaFail &f) {
+        gsofa_matrix_free(m);
+        return fail_cuda(f.e);
+    }
+    *out = m;
+    return GSOFA_OK;
+}
+
+gsofa_status gsofa_symbfact(gsofa_ctx *c, const gsofa_matrix *m, const gsofa_params *params,
+                            gsofa_result *out)
+{
+    return gsofa_symbfact_batch(c, 1, &m, params, out);
+}
+
+gsofa_status gsofa_symbfact_batch(gsofa_ctx *c, int count, const gsofa_matrix *const *mats,
+                                  const gsofa_params *params, gsofa_result *out)
+{
+    if (!c) return GSOFA_ERR_INVALID_INPUT;
+    try {
+        GS_CUDA(cudaSetDevice(c->device));
+        gsofa_status s = run_job(c, count, mats, params, out);
+        if (s != GSOFA_OK && out)
+            for (int i = 0; i < count; i++) free_result_arrays(&out[i]);
+        return s;
+    } catch (CudaFail &f) {
+        if (out)
+            for (int i = 0; i < count; i++) free_result_arrays(&out[i]);
+        return fail_cuda(f.e);
+    } catch (std::bad_alloc &) {
+        if (out)
+            for (int i = 0; i < count; i++) free_result_arrays(&out[i]);
+        return GSOFA_ERR_OOM;
+    }
+}
+
+void gsofa_result_free(gsofa_result *r)
+{
+    if (!r) return;
+    free_result_arrays(r);
+    delete (ResultInternal *)r->internal;
+    r->internal = nullptr;
+}
+
+size_t gsofa_predict_scratch_bytes(const gsofa_ctx *c, int32_t n, int64_t nnz,
+                                   const gsofa_params *params)
+{
+    if (!c || n < 0) return 0;
+    gsofa_params p;
+    resolve_params(params, &p);
+    const int block = p.block_size ? p.block_size : pick_block(std::max(n, 1));
+    const size_t smem = ((size_t)(n + 31) / 32 * 4 + 15) / 16 * 16;
+    int per_sm = p.ctas_per_sm > 0 ? p.ctas_per_sm : std::max(1, (int)(200 * 1024 / std::max<size_t>(smem, 1)));
+    per_sm = std::min(per_sm, 2048 / block);
+    const size_t grid = (size_t)per_sm * c->sm_count;
+    const size_t qcap = (size_t)std::max<int64_t>(p.queue_capacity, n);
+    const size_t L = (size_t)n;
+    size_t b = grid * qcap * 4;                 // frontier queues
+    b += L * (2 * 4 + 2 + 2 * 8 + 4 + 1 + 4);   // cnt, nxt, poff, lrow, snind, sn list
+    b += 2 * (L + 1) * 8;                       // gptr
+    b += (size_t)(n + 1) * 8 + (size_t)nnz * 8; // G and G^T
+    return b;
+}
+
+// ---------------------------------------------------------------------------
+// Reference-compatible entry (argv contract of symbfact_min_id).
+
+gsofa_status gsofa_symbfact_min_id(int argc, char **argv, int myrank, uint64_t *fill_count,
+                                   double *time_ms)
+{
+    if (!argv || argc < 5 || argc > 8 || argc == 7) return GSOFA_ERR_INVALID_INPUT;
+    const int nparts = std::atoi(argv[4]);
+    if (nparts <= 0) return GSOFA_ERR_INVALID_INPUT;
+    double mem_gb = argc >= 6 ? std::atof(argv[5]) : 0.0;
+    int max_sn = argc >= 8 ? std::atoi(argv[6]) : 0;
+    int gpus_per_node = argc >= 8 ? std::atoi(argv[7]) : 1;
+    if (gpus_per_node <= 0 || mem_gb < 0) return GSOFA_ERR_INVALID_INPUT;
+    int32_t n = 0;
+    int64_t nnz = 0;
+    int32_t *beg = nullptr, *end = nullptr, *adj = nullptr;
+    gsofa_status s = gsofa_read_text(argv[1], argv[2], argv[3], &n, &nnz, &beg, &end, &adj);
+    if (s != GSOFA_OK) return s;
+    gsofa_ctx *c = nullptr;
+    // the reference's budget counts the traversal state only; ours adds the
+    // queues, so it is a floor rather than a cap
+    s = gsofa_create(&c, myrank % gpus_per_node, 0);
+    gsofa_matrix *m = nullptr;
+    if (s == GSOFA_OK) s = gsofa_upload(c, n, nnz, beg, end, adj, &m);
+    std::free(beg);
+    std::free(end);
+    std::free(adj);
+    uint64_t total = 0;
+    double tmax = 0.0, tmin = 1e300, tsum = 0.0;
+    for (int g = 0; s == GSOFA_OK && g < nparts; g++) {
+        gsofa_params p;
+        gsofa_default_params(&p);
+        p.want_pattern = 0;
+        p.max_supernode_size = max_sn;
+        p.part_count = nparts;
+        p.part_index = g;
+        gsofa_result r;
+        s = gsofa_symbfact(c, m, &p, &r);
+        if (s == GSOFA_OK) {
+            total += r.fill_count;
+            tmax = std::max(tmax, r.kernel_ms);
+            tmin = std::min(tmin, r.kernel_ms);
+            tsum += r.kernel_ms;
+            gsofa_result_free(&r);
+        }
+    }
+    if (s == GSOFA_OK) {
+        std::printf("Total Number of fill-ins detected: %llu\n", (unsigned long long)total);
+        std::printf("\tSlowest virtual GPU takes: %.4f ms\n", tmax);
+        std::printf("\tFastest virtual GPU takes: %.4f ms\n", nparts ? tmin : 0.0);
+        if (fill_count) *fill_count = total;
+        if (time_ms) *time_ms = tsum;
+    }
+    gsofa_destroy(c);
+    return s;
+}
+
+}  // extern "C"

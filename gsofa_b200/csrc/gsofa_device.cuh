@@ -1,0 +1,738 @@
+// gsofa_device.cuh -- device code of the B200 symbolic factorization.
+//
+// Layout of one factorization job in HBM (all matrices of a batch share it):
+//   per matrix  : n, line_base, G = (ptr[n+1], adj[]) and G^T = (ptr, adj),
+//                 compact int32 CSR without diagonal entries;
+//   per line l  : cnt[2][L] int32   -- |hi(s)| of pass 0 (U row) / 1 (L column)
+//                 nxt[2][L] uint8   -- s+1 in hi(s)
+//                 poff[2][L] int64  -- where the sorted hi(s) list sits in pool
+//                 gptr[2][L+1] int64-- CSR offsets after compaction
+//                 lrow[L] int32     -- |L row s| (histogram of the L columns)
+//                 snind[L] uint8    -- line starts a supernode
+//   pool / out  : int32 pattern entries (traversal writes pool, compaction
+//                 writes out in line order);
+//   per CTA     : frontier queue of qcap int32 (every vertex enters at most
+//                 once per source, so qcap >= n never overflows).
+// The per-source visited set is an n-bit bitmap in shared memory.
+#pragma once
+
+#include <cooperative_groups.h>
+#include <stdint.h>
+
+namespace gsofa {
+namespace dev {
+
+namespace cg = cooperative_groups;
+
+struct PassGraph {
+    const int32_t *ptr;  // [n+1]
+    const int32_t *adj;  // [ptr[n]]
+};
+
+struct MatDesc {
+    int32_t n;
+    int32_t pad;
+    int64_t line_base;   // first line of this matrix in the job's line space
+    PassGraph g[2];      // 0: G, 1: G^T
+    const int32_t *rawdeg; // [n] input degree of every line (work counters)
+};
+
+// The sources of one matrix, s = offset + stride * j for j in [0, nj), cut
+// into pieces of `chunk` consecutive j.  Piece k of a range covers pass k & 1
+// and chunk k >> 1 counted from the top (the highest sources, which carry the
+// largest traversals, are handed out first).
+struct Range {
+    int32_t mat;
+    int32_t chunk;
+    int32_t nj;
+    int32_t stride;
+    int32_t offset;
+    int32_t pad;
+    int64_t piece_base;  // first global piece index of this range
+    int64_t npieces;     // 2 * ceil(nj / chunk)
+};
+
+// Error bits reported through JobArgs::status.
+enum : uint32_t {
+    ERR_POOL_OVERFLOW = 1u,
+    ERR_QUEUE_OVERFLOW = 2u,
+};
+
+struct JobArgs {
+    const MatDesc *mats;
+    int32_t nmats;
+    int32_t nranges;
+    const Range *ranges;
+    int64_t npieces;
+    unsigned long long *piece_counter; // dynamic fetch of work pieces
+    int32_t *queue;            // gridDim.x * qcap
+    int64_t qcap;
+    int32_t bitmap_words;      // shared-memory bitmap size (>= max n / 32)
+    int32_t lanes;             // lanes per frontier vertex (4..32, power of 2)
+    int32_t reuse;
+    int32_t want_pattern;
+    int32_t max_sn;
+    int64_t L;                 // total lines
+    int32_t *cnt;              // [2][L]
+    uint8_t *nxt;              // [2][L]
+    int64_t *poff;             // [2][L]
+    int32_t *pool;
+    int64_t pool_cap;
+    unsigned long long *pool_tail;
+    int64_t *gptr;             // [2][L+1]
+    int32_t *out;              // pool_cap entries
+    int32_t *lrow;             // [L]
+    uint8_t *snind;            // [L]
+    int32_t *sn_list;          // [L]
+    int64_t ntiles;
+    int64_t *tile_sum;         // [2][ntiles] then exclusive prefix (in place)
+    int64_t *tile_last;        // [ntiles] last supernode-run start, then prefix max
+    int64_t *tile_sn;          // [ntiles] then exclusive prefix
+    unsigned long long *counters; // [0] edges inspected, [1] sources, [2] sn total,
+                                  // [3] pass-G expansions, [4] pass-G input degrees
+    uint32_t *status;
+};
+
+constexpr int TILE = 2048;     // lines per tile in the post-traversal phases
+
+__device__ __forceinline__ int64_t warp_incl_scan(int64_t x)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+
+// Exclusive scan over the block; *total receives the block sum.  Uses
+// s_warp[32]; contains two __syncthreads and a trailing one.
+template <int BLOCK>
+__device__ __forceinline__ int64_t block_excl_scan(int64_t v, int64_t *total,
+                                                   int64_t *s_warp)
+{
+    constexpr int NW = BLOCK / 32;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int64_t x = warp_incl_scan(v);
+    if (lane == 31) s_warp[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int64_t w = lane < NW ? s_warp[lane] : 0;
+        w = warp_incl_scan(w);
+        if (lane < NW) s_warp[lane] = w;
+    }
+    __syncthreads();
+    int64_t pre = wid ? s_warp[wid - 1] : 0;
+    *total = s_warp[NW - 1];
+    __syncthreads();
+    return pre + x - v;
+}
+
+template <int BLOCK>
+__device__ __forceinline__ int64_t block_sum(int64_t v, int64_t *s_warp)
+{
+    int64_t t;
+    block_excl_scan<BLOCK>(v, &t, s_warp);
+    return t;
+}
+
+// Exclusive max-scan over the block (identity -1); *total receives the
+// block maximum.
+template <int BLOCK>
+__device__ __forceinline__ int64_t block_excl_max(int64_t v, int64_t *total,
+                                                  int64_t *s_warp)
+{
+    constexpr int NW = BLOCK / 32;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int64_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x = max(x, y);
+    }
+    int64_t ex = __shfl_up_sync(0xffffffffu, x, 1);
+    if (lane == 0) ex = -1;
+    if (lane == 31) s_warp[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int64_t w = lane < NW ? s_warp[lane] : -1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int64_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w = max(w, y);
+        }
+        if (lane < NW) s_warp[lane] = w;
+    }
+    __syncthreads();
+    int64_t pre = wid ? s_warp[wid - 1] : -1;
+    *total = s_warp[NW - 1];
+    __syncthreads();
+    return max(pre, ex);
+}
+
+// Bit test-and-set in the shared-memory bitmap; true when this call set it.
+__device__ __forceinline__ bool test_and_set(uint32_t *bm, int32_t m)
+{
+    const uint32_t bit = 1u << (m & 31);
+    uint32_t *w = bm + (m >> 5);
+    if (*reinterpret_cast<volatile uint32_t *>(w) & bit) return false;
+    return !(atomicOr(w, bit) & bit);
+}
+
+// Appends m to the CTA's frontier queue; one shared atomic per coalesced
+// group of lanes (warp-aggregated enqueue).
+__device__ __forceinline__ void enqueue(int32_t *q, int64_t qcap, int *s_qtail,
+                                        uint32_t *status, int32_t m)
+{
+    cg::coalesced_group g = cg::coalesced_threads();
+    int base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(s_qtail, (int)g.size());
+    base = g.shfl(base, 0);
+    const int64_t pos = (int64_t)base + g.thread_rank();
+    if (pos < qcap) q[pos] = m;
+    else atomicOr(status, 2u);  // ERR_QUEUE_OVERFLOW; cannot happen with qcap >= n
+}
+
+struct SharedState {
+    long long piece;
+    int flag;
+    int qtail;
+    int qnext;
+    int chain_lo;     // lowest vertex set in the bitmap since the last clear
+    int chain_hi;     // highest vertex set since the last clear
+    int64_t pool_base;
+    int64_t warp[32];
+};
+
+// Clears the bitmap words covering vertices [lo, hi].
+template <int BLOCK>
+__device__ __forceinline__ void clear_range(uint32_t *bm, int lo, int hi)
+{
+    if (hi < lo) return;
+    for (int w = (lo >> 5) + threadIdx.x; w <= (hi >> 5); w += BLOCK) bm[w] = 0u;
+}
+
+// One source s of one pass: seeds from adj(s), expands the frontier level by
+// level through vertices < s, then counts (and optionally writes) hi(s).
+// With `reuse`, the bitmap still holds the finished traversal of s-1, which is
+// valid because s-1 in adj(s) implies X(s-1) u {s-1} is inside X(s) and
+// hi(s-1) minus (s-1, s] is inside hi(s).
+template <int BLOCK>
+__device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
+                               int64_t line, int pass, int32_t s, uint32_t *bm,
+                               int32_t *q, SharedState &sh, int &t_lo, int &t_hi,
+                               unsigned long long &edges, const int32_t *rawdeg,
+                               unsigned long long &xcnt, unsigned long long &einsp)
+{
+    const int tid = threadIdx.x;
+    const int lanes = a.lanes;
+    const int lane_in_group = tid & (lanes - 1);
+    const int lane = tid & 31;
+    const unsigned gmask = (lanes == 32) ? 0xffffffffu
+                                         : (((1u << lanes) - 1u) << (lane & ~(lanes - 1)));
+
+    if (tid == 0) { sh.qtail = 0; }
+    // source bit
+    if (tid == 0 && test_and_set(bm, s)) { t_lo = min(t_lo, s); t_hi = max(t_hi, s); }
+    __syncthreads();
+
+    // seeding: every neighbour of s is structure of line s
+    const int32_t b0 = g.ptr[s], e0 = g.ptr[s + 1];
+    if (tid == 0) {
+        edges += (unsigned long long)(e0 - b0);
+        if (pass == 0) einsp += (unsigned long long)rawdeg[s];
+    }
+    for (int32_t k = b0 + tid; k < e0; k += BLOCK) {
+        int32_t m = g.adj[k];
+        if (test_and_set(bm, m)) {
+            t_lo = min(t_lo, m); t_hi = max(t_hi, m);
+            if (m < s) enqueue(q, a.qcap, &sh.qtail, a.status, m);
+        }
+    }
+
+    // level-synchronous expansion restricted to vertices < s
+    int lo = 0;
+    for (;;) {
+        __syncthreads();
+        const int hi = sh.qtail;
+        if (tid == 0) sh.qnext = lo;
+        __syncthreads();
+        if (hi == lo) break;
+        for (;;) {
+            int it = 0;
+            if (lane_in_group == 0) it = atomicAdd(&sh.qnext, 1);
+            it = __shfl_sync(gmask, it, 0, lanes);
+            if (it >= hi) break;
+            const int32_t v = q[it];
+            const int32_t b = g.ptr[v], e = g.ptr[v + 1];
+            if (lane_in_group == 0) {
+                edges += (unsigned long long)(e - b);
+                if (pass == 0) { xcnt++; einsp += (unsigned long long)rawdeg[v]; }
+            }
+            for (int32_t k = b + lane_in_group; k < e; k += lanes) {
+                const int32_t m = g.adj[k];
+                if (test_and_set(bm, m)) {
+                    t_lo = min(t_lo, m); t_hi = max(t_hi, m);
+                    if (m < s) enqueue(q, a.qcap, &sh.qtail, a.status, m);
+                }
+            }
+        }
+        lo = hi;
+    }
+
+    // fold the per-thread touched range into the chain range
+    {
+        int64_t vmax, vneg;
+        block_excl_max<BLOCK>((int64_t)t_hi, &vmax, sh.warp);
+        block_excl_max<BLOCK>(-(int64_t)t_lo, &vneg, sh.warp);
+        if (tid == 0) {
+            sh.chain_hi = max(sh.chain_hi, (int)vmax);
+            sh.chain_lo = min(sh.chain_lo, (int)(-vneg));
+        }
+        __syncthreads();
+    }
+    const int chain_hi = sh.chain_hi;
+
+    // hi(s) = set bits in (s, chain_hi]
+    const int w0 = (s + 1) >> 5;
+    const int w1 = (chain_hi > s) ? (chain_hi >> 5) : (w0 - 1);
+    int64_t count = 0;
+    for (int w = w0 + tid; w <= w1; w += BLOCK) {
+        uint32_t x = bm[w];
+        if (w == w0) x &= ~0u << ((s + 1) & 31);
+        count += __popc(x);
+    }
+    const int64_t total = block_sum<BLOCK>(count, sh.warp);
+
+    const int64_t slot = (int64_t)pass * a.L + line;
+    if (tid == 0) {
+        a.cnt[slot] = (int32_t)total;
+        a.nxt[slot] = (uint8_t)((s + 1 < n) && ((bm[(s + 1) >> 5] >> ((s + 1) & 31)) & 1u));
+    }
+    if (a.want_pattern) {
+        if (tid == 0) {
+            unsigned long long off = atomicAdd(a.pool_tail, (unsigned long long)total);
+            if ((int64_t)off + total > a.pool_cap) {
+                atomicOr(a.status, ERR_POOL_OVERFLOW);
+                sh.pool_base = -1;
+            } else {
+                sh.pool_base = (int64_t)off;
+            }
+            a.poff[slot] = sh.pool_base;
+        }
+        __syncthreads();
+        const int64_t base = sh.pool_base;
+        if (base >= 0 && total > 0) {
+            int64_t run = base;
+            // tiles of BLOCK words, block-wide scan for sorted output
+            for (int wt = w0; wt <= w1; wt += BLOCK) {
+                const int w = wt + tid;
+                uint32_t x = 0u;
+                if (w <= w1) {
+                    x = bm[w];
+                    if (w == w0 && ((s + 1) & 31)) x &= ~0u << ((s + 1) & 31);
+                }
+                int64_t tot;
+                int64_t pos = run + block_excl_scan<BLOCK>((int64_t)__popc(x), &tot, sh.warp);
+                while (x) {
+                    const int bit = __ffs(x) - 1;
+                    x &= x - 1u;
+                    a.pool[pos++] = (w << 5) + bit;
+                }
+                run += tot;
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// The persistent cooperative factorization kernel.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
+{
+    extern __shared__ __align__(16) uint32_t bm[];
+    __shared__ SharedState sh;
+    cg::grid_group grid = cg::this_grid();
+    const int tid = threadIdx.x;
+
+    // ---- phase 1: traversals ------------------------------------------------
+    for (int w = tid; w < a.bitmap_words; w += BLOCK) bm[w] = 0u;
+    if (tid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
+    int32_t *q = a.queue + (int64_t)blockIdx.x * a.qcap;
+    unsigned long long edges = 0, nsrc = 0, xcnt = 0, einsp = 0;
+    __syncthreads();
+    for (;;) {
+        if (tid == 0) sh.piece = (long long)atomicAdd(a.piece_counter, 1ull);
+        __syncthreads();
+        const int64_t pc = sh.piece;
+        if (pc >= a.npieces) break;
+        int r = 0;
+        {
+            int hi = a.nranges - 1;
+            while (r < hi) {
+                const int mid = (r + hi + 1) >> 1;
+                if (a.ranges[mid].piece_base <= pc) r = mid; else hi = mid - 1;
+            }
+        }
+        const Range rg = a.ranges[r];
+        const int64_t k = pc - rg.piece_base;
+        const int pass = (int)(k & 1);
+        const int64_t c = k >> 1;
+        const int64_t j1 = (int64_t)rg.nj - c * rg.chunk;
+        const int64_t j0 = max((int64_t)0, j1 - rg.chunk);
+        const MatDesc md = a.mats[rg.mat];
+        const PassGraph g = md.g[pass];
+        int prev = -2;
+        for (int64_t j = j0; j < j1; j++) {
+            const int32_t s = rg.offset + (int32_t)j * rg.stride;
+            int reuse = 0;
+            if (a.reuse && prev == s - 1) {
+                if (tid == 0) sh.flag = 0;
+                __syncthreads();
+                for (int32_t k = g.ptr[s] + tid; k < g.ptr[s + 1]; k += BLOCK)
+                    if (g.adj[k] == s - 1) sh.flag = 1;
+                __syncthreads();
+                reuse = sh.flag;
+            }
+            if (!reuse) {
+                const int clo = sh.chain_lo, chi = sh.chain_hi;
+                clear_range<BLOCK>(bm, clo, chi);
+                __syncthreads();
+                if (tid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
+            }
+            int t_lo = INT32_MAX, t_hi = -1;
+            process_source<BLOCK>(a, g, md.n, md.line_base + s, pass, s, bm, q,
+                                  sh, t_lo, t_hi, edges, md.rawdeg, xcnt, einsp);
+            prev = s;
+            nsrc++;
+        }
+        // the next item starts from an empty bitmap
+        {
+            const int clo = sh.chain_lo, chi = sh.chain_hi;
+            clear_range<BLOCK>(bm, clo, chi);
+            __syncthreads();
+            if (tid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
+            __syncthreads();
+        }
+    }
+    {
+        const int64_t e = block_sum<BLOCK>((int64_t)edges, sh.warp);
+        const int64_t x = block_sum<BLOCK>((int64_t)xcnt, sh.warp);
+        const int64_t ei = block_sum<BLOCK>((int64_t)einsp, sh.warp);
+        if (tid == 0) {
+            atomicAdd(&a.counters[0], (unsigned long long)e);
+            atomicAdd(&a.counters[1], nsrc);
+            atomicAdd(&a.counters[3], (unsigned long long)x);
+            atomicAdd(&a.counters[4], (unsigned long long)ei);
+        }
+    }
+    grid.sync();
+
+    const int64_t L = a.L;
+    const int64_t ntiles = a.ntiles;
+
+    // line -> matrix lookup (matrices are stored in line order)
+    auto mat_of = [&](int64_t l) -> int {
+        int lo = 0, hi = a.nmats - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (a.mats[mid].line_base <= l) lo = mid; else hi = mid - 1;
+        }
+        return lo;
+    };
+    // supernode run boundary before line l (SURVEY a11 definition)
+    auto sn_flag = [&](int64_t l) -> bool {
+        const MatDesc &md = a.mats[mat_of(l)];
+        const int64_t s = l - md.line_base;
+        if (s == 0) return true;
+        const bool linked = a.nxt[L + l - 1] && a.nxt[l - 1] && (a.cnt[l] == a.cnt[l - 1] - 1);
+        return !linked;
+    };
+
+    // ---- phase 2: tile partial sums ------------------------------------------
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        int64_t s0 = 0, s1 = 0, last = -1;
+        for (int64_t l = t * TILE + tid; l < min(L, (t + 1) * TILE); l += BLOCK) {
+            s0 += a.cnt[l];
+            s1 += a.cnt[L + l];
+            if (sn_flag(l)) last = max(last, l);
+        }
+        int64_t t0 = block_sum<BLOCK>(s0, sh.warp);
+        int64_t t1 = block_sum<BLOCK>(s1, sh.warp);
+        int64_t tl;
+        block_excl_max<BLOCK>(last, &tl, sh.warp);
+        if (tid == 0) {
+            a.tile_sum[t] = t0;
+            a.tile_sum[ntiles + t] = t1;
+            a.tile_last[t] = tl;
+        }
+    }
+    grid.sync();
+
+    // ---- phase 3: block 0 scans the tile partials -----------------------------
+    if (blockIdx.x == 0) {
+        int64_t c0 = 0, c1 = 0, cm = -1;
+        for (int64_t base = 0; base < ntiles; base += BLOCK) {
+            const int64_t t = base + tid;
+            const int64_t v0 = t < ntiles ? a.tile_sum[t] : 0;
+            const int64_t v1 = t < ntiles ? a.tile_sum[ntiles + t] : 0;
+            const int64_t vm = t < ntiles ? a.tile_last[t] : -1;
+            int64_t tot0, tot1, totm;
+            const int64_t e0 = block_excl_scan<BLOCK>(v0, &tot0, sh.warp);
+            const int64_t e1 = block_excl_scan<BLOCK>(v1, &tot1, sh.warp);
+            const int64_t em = block_excl_max<BLOCK>(vm, &totm, sh.warp);
+            if (t < ntiles) {
+                a.tile_sum[t] = c0 + e0;
+                a.tile_sum[ntiles + t] = c1 + e1;
+                a.tile_last[t] = max(cm, em);
+            }
+            c0 += tot0; c1 += tot1; cm = max(cm, totm);
+        }
+        if (tid == 0) {
+            a.gptr[L] = c0;                  // pass 0 total
+            a.gptr[(L + 1) + L] = c1;        // pass 1 total
+        }
+    }
+    grid.sync();
+
+    // ---- phase 4: CSR offsets and supernode starts per tile -------------------
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        int64_t c0 = a.tile_sum[t], c1 = a.tile_sum[ntiles + t], carry = a.tile_last[t];
+        int64_t nsn = 0;
+        for (int64_t base = t * TILE; base < min(L, (t + 1) * TILE); base += BLOCK) {
+            const int64_t l = base + tid;
+            const bool in = l < min(L, (t + 1) * TILE);
+            int64_t v0 = in ? a.cnt[l] : 0;
+            int64_t v1 = in ? a.cnt[L + l] : 0;
+            bool f = in && sn_flag(l);
+            int64_t tot0, tot1;
+            int64_t e0 = block_excl_scan<BLOCK>(v0, &tot0, sh.warp);
+            int64_t e1 = block_excl_scan<BLOCK>(v1, &tot1, sh.warp);
+            int64_t sub_last;
+            int64_t rs = block_excl_max<BLOCK>(f ? l : -1, &sub_last, sh.warp);
+            rs = max(max(rs, f ? l : (int64_t)-1), carry);
+            bool start = false;
+            if (in) {
+                a.gptr[l] = c0 + e0;
+                a.gptr[(L + 1) + l] = c1 + e1;
+                start = f || (a.max_sn > 0 && ((l - rs) % a.max_sn) == 0);
+                a.snind[l] = start ? 1 : 0;
+            }
+            const int64_t ns = block_sum<BLOCK>(start ? 1 : 0, sh.warp);
+            carry = max(carry, sub_last);   // run start carried to the next sub-tile
+            c0 += tot0; c1 += tot1; nsn += ns;
+        }
+        if (tid == 0) a.tile_sn[t] = nsn;
+    }
+    grid.sync();
+
+    // ---- phase 5: block 0 scans the supernode tile counts ---------------------
+    if (blockIdx.x == 0) {
+        int64_t c = 0;
+        for (int64_t base = 0; base < ntiles; base += BLOCK) {
+            const int64_t t = base + tid;
+            int64_t v = t < ntiles ? a.tile_sn[t] : 0;
+            int64_t tot;
+            int64_t e = block_excl_scan<BLOCK>(v, &tot, sh.warp);
+            if (t < ntiles) a.tile_sn[t] = c + e;
+            c += tot;
+        }
+        if (tid == 0) a.counters[2] = (unsigned long long)c;
+    }
+    grid.sync();
+
+    // ---- phase 6: supernode list, pattern compaction, L row histogram ---------
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        int64_t c = a.tile_sn[t];
+        for (int64_t base = t * TILE; base < min(L, (t + 1) * TILE); base += BLOCK) {
+            const int64_t l = base + tid;
+            const bool in = l < min(L, (t + 1) * TILE);
+            int64_t v = (in && a.snind[l]) ? 1 : 0;
+            int64_t tot;
+            int64_t e = block_excl_scan<BLOCK>(v, &tot, sh.warp);
+            if (v) a.sn_list[c + e] = (int32_t)l;
+            c += tot;
+        }
+    }
+    if (a.want_pattern && (*a.status & ERR_POOL_OVERFLOW) == 0) {
+        const int warps = (gridDim.x * BLOCK) >> 5;
+        const int gw = (blockIdx.x * BLOCK + tid) >> 5;
+        const int lane = tid & 31;
+        const int64_t tot0 = a.gptr[L];
+        for (int64_t pl = gw; pl < 2 * L; pl += warps) {
+            const int pass = pl >= L;
+            const int64_t l = pass ? pl - L : pl;
+            const int32_t c = a.cnt[pl];
+            if (c == 0) continue;
+            const int64_t src = a.poff[pl];
+            const int64_t dst = (pass ? tot0 : 0) + a.gptr[pass * (L + 1) + l];
+            int64_t lb = 0;
+            if (pass) lb = a.mats[mat_of(l)].line_base;
+            for (int32_t k = lane; k < c; k += 32) {
+                const int32_t m = a.pool[src + k];
+                a.out[dst + k] = m;
+                if (pass) atomicAdd(&a.lrow[lb + m], 1);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Upload kernels: validation, diagonal removal, distinct-entry counts, G^T.
+
+struct UploadArgs {
+    int32_t n;
+    int64_t nnz;
+    const int32_t *beg, *end, *adj;  // staged input
+    int32_t *deg;                    // [n]   distinct off-diagonal entries per line
+    int32_t *indeg;                  // [n+1] entries per transposed line
+    int32_t *orig_up;                // [n]   distinct entries > v in line v
+    int32_t *orig_lo;                // [n]   distinct lines u > j holding j
+    int32_t *rawdeg;                 // [n]   end[v] - beg[v]
+    unsigned long long *counts;      // [0] distinct upper, [1] distinct lower
+    uint32_t *status;                // bit 0: invalid input
+};
+
+// True when adj[k] is the first occurrence of its value in line [b, k].
+__device__ __forceinline__ bool first_in_line(const int32_t *adj, int32_t b, int32_t k,
+                                              bool sorted)
+{
+    const int32_t m = adj[k];
+    if (sorted) return (k == b) || (adj[k - 1] != m);
+    for (int32_t j = b; j < k; j++)
+        if (adj[j] == m) return false;
+    return true;
+}
+
+// One warp per line.  Checks the range and the ids, counts kept entries and
+// transposed entries, and the distinct off-diagonal entries above/below.
+__global__ void upload_count_kernel(UploadArgs u)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned long long up = 0, lo = 0;
+    for (int64_t v = gw; v < u.n; v += nw) {
+        const int32_t b = u.beg[v], e = u.end[v];
+        if (b < 0 || e < b || (int64_t)e > u.nnz) {
+            if (lane == 0) {
+                atomicOr(u.status, 1u);
+                u.deg[v] = 0; u.orig_up[v] = 0; u.rawdeg[v] = 0;
+            }
+            continue;
+        }
+        if (lane == 0) u.rawdeg[v] = e - b;
+        // sorted lists allow a linear duplicate test
+        bool sorted = true;
+        for (int32_t k = b + lane; k + 1 < e; k += 32)
+            if (u.adj[k] > u.adj[k + 1]) sorted = false;
+        sorted = __all_sync(0xffffffffu, sorted);
+        int kept = 0, kup = 0;
+        for (int32_t k = b + lane; k < e; k += 32) {
+            const int32_t m = u.adj[k];
+            if (m < 0 || m >= u.n) { atomicOr(u.status, 1u); continue; }
+            if (m == (int32_t)v) continue;
+            if (!first_in_line(u.adj, b, k, sorted)) continue;
+            kept++;
+            atomicAdd(&u.indeg[m], 1);
+            if (m > v) { up++; kup++; }
+            else { lo++; atomicAdd(&u.orig_lo[m], 1); }
+        }
+        for (int o = 16; o; o >>= 1) {
+            kept += __shfl_xor_sync(0xffffffffu, kept, o);
+            kup += __shfl_xor_sync(0xffffffffu, kup, o);
+        }
+        if (lane == 0) { u.deg[v] = kept; u.orig_up[v] = kup; }
+    }
+    for (int o = 16; o; o >>= 1) {
+        up += __shfl_xor_sync(0xffffffffu, up, o);
+        lo += __shfl_xor_sync(0xffffffffu, lo, o);
+    }
+    if (lane == 0) {
+        if (up) atomicAdd(&u.counts[0], up);
+        if (lo) atomicAdd(&u.counts[1], lo);
+    }
+}
+
+// One warp per line: copies the kept entries (order preserved) into G and
+// scatters them into G^T through per-line cursors.
+__global__ void upload_fill_kernel(UploadArgs u, const int32_t *gptr, int32_t *gadj,
+                                   int32_t *tcursor, int32_t *tadj)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t v = gw; v < u.n; v += nw) {
+        const int32_t b = u.beg[v], e = u.end[v];
+        if (b < 0 || e < b || (int64_t)e > u.nnz) continue;
+        bool sorted = true;
+        for (int32_t k = b + lane; k + 1 < e; k += 32)
+            if (u.adj[k] > u.adj[k + 1]) sorted = false;
+        sorted = __all_sync(0xffffffffu, sorted);
+        int32_t out = gptr[v];
+        for (int32_t k0 = b; k0 < e; k0 += 32) {
+            const int32_t k = k0 + lane;
+            int32_t m = -1;
+            bool keep = false;
+            if (k < e) {
+                m = u.adj[k];
+                keep = (m >= 0 && m < u.n && m != (int32_t)v) &&
+                       first_in_line(u.adj, b, k, sorted);
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, keep);
+            if (keep) {
+                gadj[out + __popc(bal & ((1u << lane) - 1u))] = m;
+                const int32_t p = atomicAdd(&tcursor[m], 1);
+                tadj[p] = (int32_t)v;
+            }
+            out += __popc(bal);
+        }
+    }
+}
+
+// Exclusive scan of int32 counts into int32 offsets: three kernels.
+template <int BLOCK>
+__global__ void scan_tiles_kernel(const int32_t *in, int64_t n, int64_t *tile_sums)
+{
+    __shared__ int64_t warp[32];
+    const int64_t t = blockIdx.x;
+    const int64_t i = t * BLOCK + threadIdx.x;
+    int64_t v = i < n ? in[i] : 0;
+    int64_t s = block_sum<BLOCK>(v, warp);
+    if (threadIdx.x == 0) tile_sums[t] = s;
+}
+
+template <int BLOCK>
+__global__ void scan_partials_kernel(int64_t *tile_sums, int64_t ntiles, int64_t *total)
+{
+    __shared__ int64_t warp[32];
+    int64_t c = 0;
+    for (int64_t base = 0; base < ntiles; base += BLOCK) {
+        const int64_t t = base + threadIdx.x;
+        int64_t v = t < ntiles ? tile_sums[t] : 0;
+        int64_t tot;
+        int64_t e = block_excl_scan<BLOCK>(v, &tot, warp);
+        if (t < ntiles) tile_sums[t] = c + e;
+        c += tot;
+    }
+    if (threadIdx.x == 0) *total = c;
+}
+
+template <int BLOCK>
+__global__ void scan_apply_kernel(const int32_t *in, int64_t n, const int64_t *tile_sums,
+                                  int32_t *out, const int64_t *total)
+{
+    __shared__ int64_t warp[32];
+    const int64_t t = blockIdx.x;
+    const int64_t i = t * BLOCK + threadIdx.x;
+    int64_t v = i < n ? in[i] : 0;
+    int64_t tot;
+    int64_t e = block_excl_scan<BLOCK>(v, &tot, warp);
+    if (i < n) out[i] = (int32_t)(tile_sums[t] + e);
+    if (i == 0) out[n] = (int32_t)*total;
+}
+
+}  // namespace dev
+}  // namespace gsofa

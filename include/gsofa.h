@@ -1,0 +1,182 @@
+/*
+ * gsofa.h -- C ABI of the B200-native gSoFa symbolic LU factorization.
+ *
+ * The reference exposes one host entry point,
+ *     void symbfact_min_id(int args, char **argv, int myrank,
+ *                          ull_t &fill_count, double &time)
+ * (without_space_optimization/symbfact.cuh:991 and
+ *  with_space_optimization/symbfact.cuh:1553), called from
+ * without_space_optimization/main.cu:31.  It reads the colbeg/colend/csr text
+ * files named in argv, runs the multi-source fill traversal on the GPU, and
+ * reports the total fill count and the time; every error calls exit().
+ *
+ * This header replaces it with:
+ *   - gsofa_symbfact_min_id(): the same argv contract, returning a status;
+ *   - a structured API (context, device-resident matrix, parameters, result)
+ *     that also returns the L+U pattern, per-line counts and the supernode
+ *     partition, for one matrix or a batch of matrices in one launch.
+ *
+ * Conventions:
+ *   - every function returns a gsofa_status and never exits the process;
+ *   - input arrays are caller-owned host memory and are copied;
+ *   - result arrays are library-owned host memory, valid until
+ *     gsofa_result_free();
+ *   - a context is used by one host thread at a time.
+ *
+ * Matrix convention: n lines; line v owns adj[beg[v] .. end[v]) (the
+ * reference's colbeg/colend/csr triple).  Ranges may sit anywhere inside adj,
+ * in any order; lists may be unsorted and may contain the diagonal or
+ * duplicates.  The pattern computed is that of the LU factors of the matrix
+ * whose row v holds the entries of line v:
+ *   U by rows:    u_idx[u_ptr[s] .. u_ptr[s+1])  = sorted { j > s : (s,j) in L+U }
+ *   L by columns: l_idx[l_ptr[j] .. l_ptr[j+1])  = sorted { i > j : (i,j) in L+U }
+ * (entries are original nonzeros plus fill; the diagonal is implicit).
+ */
+#ifndef GSOFA_H
+#define GSOFA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GSOFA_ABI_VERSION 1
+
+typedef enum gsofa_status {
+    GSOFA_OK = 0,
+    GSOFA_ERR_INVALID_INPUT = 1, /* bad sizes, ranges or ids; bad argv     */
+    GSOFA_ERR_OOM = 2,           /* device or host allocation failed       */
+    GSOFA_ERR_QUEUE_OVERFLOW = 3,/* a frontier queue or the pattern pool
+                                    ran out of room (retried internally)    */
+    GSOFA_ERR_TIMEOUT = 4,       /* a bounded device-side wait gave up     */
+    GSOFA_ERR_CUDA = 5,          /* a CUDA runtime call failed             */
+    GSOFA_ERR_IO = 6,            /* an input file could not be read        */
+    GSOFA_ERR_UNSUPPORTED = 7    /* no usable GPU or too large for it      */
+} gsofa_status;
+
+typedef struct gsofa_ctx gsofa_ctx;       /* device, stream, scratch pools */
+typedef struct gsofa_matrix gsofa_matrix; /* device-resident G and G^T     */
+
+/* Tuning and output parameters; zero means "choose automatically". */
+typedef struct gsofa_params {
+    int32_t src_chunk;          /* consecutive sources per work item          */
+    int32_t block_size;         /* threads per CTA: 128, 256, 512 or 1024     */
+    int32_t threads_per_source; /* lanes expanding one frontier vertex:
+                                   4, 8, 16 or 32                             */
+    int32_t ctas_per_sm;        /* resident CTAs per SM                       */
+    int64_t queue_capacity;     /* frontier entries per CTA (>= n, else n)    */
+    int64_t pool_capacity;      /* pattern entries kept on the device         */
+    int32_t max_supernode_size; /* 0 or negative: unbounded                   */
+    int32_t want_pattern;       /* 1: return u/l index arrays                 */
+    int32_t reuse;              /* 1: reuse traversal state along a chain of
+                                   sources s-1 -> s when s-1 is in adj(s);
+                                   0: every source starts from scratch;
+                                   -1: choose automatically (default 0)       */
+    int32_t flags;              /* GSOFA_FLAG_* bits                          */
+    int32_t part_count;         /* >1: process only the sources s with        */
+    int32_t part_index;         /*     s % part_count == part_index (the
+                                   reference's interleaved virtual-GPU
+                                   partition, symbfact.cuh:1093); per-line
+                                   outputs of other lines are zero            */
+} gsofa_params;
+
+#define GSOFA_FLAG_NO_DOWNLOAD 0x1 /* keep per-line arrays on the device only */
+#define GSOFA_FLAG_DEVICE_TIMING 0x2 /* record the traversal kernel time       */
+
+typedef struct gsofa_result {
+    int32_t n;
+    int32_t n_supernodes;
+    uint64_t fill_count;     /* new nonzeros (original entries excluded);
+                                with part_count > 1: of the processed lines */
+    uint64_t nnz_lu;         /* |struct(A) u fill u diag|                  */
+    uint64_t nnz_u;          /* strictly upper entries                      */
+    uint64_t nnz_l;          /* strictly lower entries                      */
+    uint64_t edges_inspected;/* adjacency entries the traversal read        */
+    uint64_t sources;        /* traversals run (both passes)                */
+    uint64_t x_total;        /* pass-G vertices expanded: sum |X(s)| when
+                                every source starts from scratch          */
+    uint64_t e_insp;         /* pass-G input-degree sum over the sources and
+                                the vertices expanded, sum deg(s) + sum over
+                                X(s) of deg(v) (input degrees, diagonal and
+                                duplicates included)                      */
+    double kernel_ms;        /* factorization kernel time on the device     */
+    /* per-line arrays (host, library-owned; NULL with NO_DOWNLOAD) */
+    int32_t *u_row_count;    /* [n] |U row s|                               */
+    int32_t *l_col_count;    /* [n] |L column j|                            */
+    int32_t *l_row_count;    /* [n] |L row s|                               */
+    int32_t *sn_start;       /* [n_supernodes] first line of each supernode */
+    /* pattern (host, library-owned; NULL unless want_pattern) */
+    int64_t *u_ptr;          /* [n+1] */
+    int32_t *u_idx;          /* [nnz_u] */
+    int64_t *l_ptr;          /* [n+1] */
+    int32_t *l_idx;          /* [nnz_l] */
+    void *internal;
+} gsofa_result;
+
+/* ---- reference-compatible entry ------------------------------------------
+ * Replaces symbfact_min_id (without_space_optimization/symbfact.cuh:991;
+ * with_space_optimization/symbfact.cuh:1553).  argv as the reference's CLI:
+ *   argv[1] colbeg file, argv[2] colend file, argv[3] csr file,
+ *   argv[4] N_GPU (source partitions, run back to back),
+ *   optional argv[5] memory budget in GB, argv[6] max_supernode_size,
+ *   argv[7] GPUs per node.
+ * The device is myrank % GPUs-per-node.  *fill_count receives the TOTAL over
+ * all partitions; *time_ms the factorization time.  Returns a status. */
+gsofa_status gsofa_symbfact_min_id(int argc, char **argv, int myrank,
+                                   uint64_t *fill_count, double *time_ms);
+
+/* ---- structured API ------------------------------------------------------ */
+const char *gsofa_status_str(gsofa_status s);
+int gsofa_abi_version(void);
+void gsofa_default_params(gsofa_params *p);
+
+/* Context on `device`; mem_budget_bytes bounds the device memory it may hold
+ * (0: 90% of the free memory at creation). */
+gsofa_status gsofa_create(gsofa_ctx **ctx, int device, size_t mem_budget_bytes);
+void gsofa_destroy(gsofa_ctx *ctx);
+
+/* Makes ctx issue its work on `cuda_stream` (a cudaStream_t of ctx's device;
+ * NULL restores the context's own stream).  Calls still return only after
+ * their work has finished. */
+gsofa_status gsofa_set_stream(gsofa_ctx *ctx, void *cuda_stream);
+
+/* Reads the reference's text files (csr: "nnz n" then nnz ids; colbeg and
+ * colend: n ids each; without_space_optimization/symbfact.cuh:1022-1071) into
+ * malloc'd arrays the caller frees with gsofa_free(). */
+gsofa_status gsofa_read_text(const char *beg_file, const char *end_file,
+                             const char *csr_file, int32_t *n, int64_t *nnz,
+                             int32_t **beg, int32_t **end, int32_t **adj);
+void gsofa_free(void *p);
+
+/* Copies the caller's host arrays to the device, validates them (every range
+ * inside [0, nnz), every id inside [0, n)) and builds the compact graph and its
+ * transpose.  The matrix belongs to ctx. */
+gsofa_status gsofa_upload(gsofa_ctx *ctx, int32_t n, int64_t nnz,
+                          const int32_t *beg, const int32_t *end,
+                          const int32_t *adj, gsofa_matrix **out);
+void gsofa_matrix_free(gsofa_matrix *m);
+int32_t gsofa_matrix_n(const gsofa_matrix *m);
+
+/* Symbolic factorization of one matrix (params may be NULL). */
+gsofa_status gsofa_symbfact(gsofa_ctx *ctx, const gsofa_matrix *m,
+                            const gsofa_params *params, gsofa_result *out);
+
+/* `count` matrices in one persistent launch; out[i] belongs to mats[i]. */
+gsofa_status gsofa_symbfact_batch(gsofa_ctx *ctx, int count,
+                                  const gsofa_matrix *const *mats,
+                                  const gsofa_params *params,
+                                  gsofa_result *out);
+
+void gsofa_result_free(gsofa_result *r);
+
+/* Device scratch bytes a factorization of an n-line, nnz-entry matrix needs
+ * with these parameters, excluding the pattern pool (admission control). */
+size_t gsofa_predict_scratch_bytes(const gsofa_ctx *ctx, int32_t n, int64_t nnz,
+                                   const gsofa_params *params);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GSOFA_H */

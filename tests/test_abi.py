@@ -1,0 +1,81 @@
+"""The C ABI library loads and exports what include/gsofa.h declares; the
+host-only entry points behave (no GPU needed)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import gsofa_b200
+from tests.common import bundled
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    names = set()
+    for f in os.listdir(os.path.join(ROOT, "include")):
+        if f.endswith(".h"):
+            src = open(os.path.join(ROOT, "include", f)).read()
+            src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+            names |= set(re.findall(r"\b(gsofa_\w+)\s*\(", src))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    L = ctypes.CDLL(gsofa_b200.LIB_PATH)
+    declared = _declared()
+    assert declared, "no declarations found"
+    missing = [n for n in sorted(declared) if not hasattr(L, n)]
+    assert not missing, missing
+    assert set(gsofa_b200.exported_symbols()) <= declared
+
+
+def test_abi_version_and_status_strings():
+    L = gsofa_b200.lib()
+    assert L.gsofa_abi_version() == 1
+    for s in range(8):
+        assert L.gsofa_status_str(s)
+    p = gsofa_b200.Params.default()
+    assert p.want_pattern == 1 and p.part_count == 1 and p.reuse == 0
+
+
+def test_params_layout_matches_header():
+    # the ctypes mirror must have the C struct's size: 4*i32, 2*i64, 6*i32
+    assert ctypes.sizeof(gsofa_b200.Params) == 4 * 4 + 2 * 8 + 6 * 4
+    assert ctypes.sizeof(gsofa_b200._CResult) == 2 * 4 + 8 * 8 + 8 + 9 * 8
+
+
+def test_read_text_matches_fixture(tmp_path):
+    g = bundled()
+    (tmp_path / "b.dat").write_text(" ".join(map(str, g.beg.tolist())) + "\n")
+    (tmp_path / "e.dat").write_text(" ".join(map(str, g.end.tolist())) + "\n")
+    (tmp_path / "c.dat").write_text(f"{g.nnz}\n{g.n}\n" + "\n".join(map(str, g.adj.tolist())) + "\n")
+    r = gsofa_b200.read_text(str(tmp_path / "b.dat"), str(tmp_path / "e.dat"), str(tmp_path / "c.dat"))
+    assert r.n == g.n and np.array_equal(r.beg, g.beg) and np.array_equal(r.end, g.end)
+    assert np.array_equal(r.adj, g.adj)
+
+
+def test_read_text_errors(tmp_path):
+    with pytest.raises(gsofa_b200.GsofaError) as e:
+        gsofa_b200.read_text(str(tmp_path / "nope"), str(tmp_path / "nope"), str(tmp_path / "nope"))
+    assert e.value.status == 6
+    (tmp_path / "c.dat").write_text("10\n5\n1 2 3\n")  # truncated
+    (tmp_path / "b.dat").write_text("0 0 0 0 0")
+    with pytest.raises(gsofa_b200.GsofaError):
+        gsofa_b200.read_text(str(tmp_path / "b.dat"), str(tmp_path / "b.dat"), str(tmp_path / "c.dat"))
+
+
+def test_bad_argv_is_a_status_not_an_exit():
+    with pytest.raises(gsofa_b200.GsofaError) as e:
+        gsofa_b200.symbfact_min_id(["gsofa", "a", "b"])
+    assert e.value.status == 1
+
+
+def test_cli_usage():
+    cli = os.path.join(ROOT, "gsofa_b200", "gsofa")
+    assert os.path.exists(cli)
+    r = subprocess.run([cli], capture_output=True, text=True)
+    assert r.returncode == 2 and "usage" in r.stderr

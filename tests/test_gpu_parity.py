@@ -1,0 +1,159 @@
+"""GPU parity: the CUDA library (through its C ABI) against the CPU oracle,
+bit for bit -- pattern, per-line counts, supernodes, fill totals."""
+import numpy as np
+import pytest
+
+import gsofa_b200
+import oracle
+from gsofa_b200 import matgen
+from tests.common import assert_same, bundled, expected, random_graph
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = gsofa_b200.Context(0)
+    yield c
+    c.close()
+
+
+def _oracle(g, max_sn=0, pattern=True):
+    return oracle.symbfact(g.beg, g.end, g.adj, want_pattern=pattern, max_supernode_size=max_sn)
+
+
+def test_bundled_matrix(ctx):
+    g = bundled()
+    m = ctx.upload(g)
+    exp = expected()["bundled_11948"]
+    for max_sn in (0, 4):
+        ref = _oracle(g, max_sn)
+        r = ctx.symbfact(m, max_supernode_size=max_sn)
+        assert r.fill_count == exp["fill_count"] and r.nnz_lu == exp["nnz_lu"]
+        assert_same(r, ref, where=f"bundled max_sn={max_sn}")
+
+
+def test_grid2d_natural_golden(ctx):
+    g = matgen.config_plain2d()
+    r = ctx.symbfact(ctx.upload(g))
+    exp = expected()["grid2d_64x64_natural"]
+    assert r.fill_count == exp["fill_count"] and r.nnz_lu == exp["nnz_lu"]
+    assert_same(r, _oracle(g), where="grid2d 64")
+
+
+@pytest.mark.parametrize("side", [6, 13, 20])
+def test_grid3d_nd(ctx, side):
+    g = matgen.grid3d(side, ordering="nd", drop_frac=0.1, seed=side)
+    assert_same(ctx.symbfact(ctx.upload(g)), _oracle(g), where=f"grid3d {side}")
+
+
+@pytest.mark.parametrize("n", [500, 3000])
+def test_powerlaw(ctx, n):
+    g = matgen.powerlaw(n, seed=n)
+    assert_same(ctx.symbfact(ctx.upload(g)), _oracle(g), where=f"powerlaw {n}")
+
+
+@pytest.mark.parametrize("seed", range(10))
+def test_random_free_form_layout(ctx, seed):
+    rng = np.random.default_rng(100 + seed)
+    n = int(rng.integers(1, 400))
+    g = random_graph(n, float(rng.choice([0.003, 0.01, 0.03, 0.1])), seed)
+    assert_same(ctx.symbfact(ctx.upload(g)), _oracle(g), where=f"random {seed}")
+
+
+def test_empty_and_tiny(ctx):
+    for n in (1, 2, 33):
+        g = matgen.Graph(n, np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(0, np.int32))
+        r = ctx.symbfact(ctx.upload(g))
+        assert r.fill_count == 0 and r.nnz_lu == n
+        assert_same(r, _oracle(g), where=f"empty {n}")
+
+
+@pytest.mark.parametrize("block,lanes,reuse,chunk,per_sm", [
+    (128, 4, 0, 1, 0), (256, 8, 1, 7, 1), (512, 16, 1, 32, 0), (1024, 32, 0, 3, 0),
+    (256, 32, 1, 1, 2), (512, 8, 1, 200, 0)])
+def test_parameters_do_not_change_results(ctx, block, lanes, reuse, chunk, per_sm):
+    g = matgen.grid3d(14, ordering="nd", drop_frac=0.1, seed=5)
+    ref = _oracle(g, 8)
+    r = ctx.symbfact(ctx.upload(g), block_size=block, threads_per_source=lanes, reuse=reuse,
+                     src_chunk=chunk, ctas_per_sm=per_sm, max_supernode_size=8)
+    assert_same(r, ref, where=f"params {block},{lanes},{reuse},{chunk},{per_sm}")
+
+
+def test_counts_only_and_pool_retry(ctx):
+    g = matgen.powerlaw(2000, seed=9)
+    ref = _oracle(g)
+    m = ctx.upload(g)
+    r = ctx.symbfact(m, want_pattern=0)
+    assert_same(r, ref, pattern=False, where="counts only")
+    assert r.u_idx is None
+    # a pool far too small: the library reruns with the exact size
+    r = ctx.symbfact(m, pool_capacity=16)
+    assert_same(r, ref, where="pool retry")
+
+
+def test_partitions_sum_to_total(ctx):
+    g = bundled()
+    m = ctx.upload(g)
+    for parts in (6, 264):
+        tot = sum(ctx.symbfact(m, part_count=parts, part_index=i, want_pattern=0).fill_count
+                  for i in range(parts))
+        assert tot == expected()["bundled_11948"]["fill_count"]
+
+
+def test_invalid_inputs_are_statuses(ctx):
+    g = random_graph(50, 0.05, 3)
+    bad = g.adj.copy()
+    bad[len(bad) // 2] = 50
+    with pytest.raises(gsofa_b200.GsofaError) as e:
+        ctx.upload(g.beg, g.end, bad)
+    assert e.value.status == 1
+    beg = g.beg.copy()
+    beg[7] = len(g.adj) + 5
+    with pytest.raises(gsofa_b200.GsofaError):
+        ctx.upload(beg, g.end, g.adj)
+    # the context stays usable
+    assert_same(ctx.symbfact(ctx.upload(g)), _oracle(g), where="after errors")
+
+
+def test_reference_argv_entry(tmp_path):
+    g = bundled()
+    (tmp_path / "b.dat").write_text(" ".join(map(str, g.beg.tolist())))
+    (tmp_path / "e.dat").write_text(" ".join(map(str, g.end.tolist())))
+    (tmp_path / "c.dat").write_text(f"{g.nnz} {g.n}\n" + " ".join(map(str, g.adj.tolist())))
+    files = [str(tmp_path / f) for f in ("b.dat", "e.dat", "c.dat")]
+    want = expected()["bundled_11948"]["fill_count"]
+    for argv in (["gsofa", *files, "1"], ["gsofa", *files, "6", "1"],
+                 ["gsofa", *files, "264", "5", "128", "1"]):
+        fills, ms = gsofa_b200.symbfact_min_id(argv)
+        assert fills == want and ms > 0
+
+
+def test_batch_matches_one_by_one(ctx):
+    gs = [matgen.grid2d(17), matgen.grid3d(9, seed=1), matgen.powerlaw(700, seed=2),
+          random_graph(90, 0.04, 5), bundled(), random_graph(1, 0.0, 1)]
+    ms = [ctx.upload(g) for g in gs]
+    rs = ctx.symbfact_batch(ms, max_supernode_size=16)
+    for g, r in zip(gs, rs):
+        assert_same(r, _oracle(g, 16), where=f"batch {g.name}")
+
+
+def test_exhaustive_n4_in_one_batch(ctx):
+    import itertools
+    pairs = [(i, j) for i in range(4) for j in range(4) if i != j]
+    gs, ms = [], []
+    for mask in range(0, 1 << len(pairs), 3):   # every third pattern: 1,366 matrices
+        rows = [[] for _ in range(4)]
+        for b, (i, j) in enumerate(pairs):
+            if mask >> b & 1:
+                rows[i].append(j)
+        ptr = np.zeros(5, np.int64)
+        ptr[1:] = np.cumsum([len(r) for r in rows])
+        g = matgen.Graph.from_csr(ptr, np.array([c for r in rows for c in r], np.int32))
+        gs.append(g)
+        ms.append(ctx.upload(g))
+    rs = ctx.symbfact_batch(ms)
+    for g, r in zip(gs, rs):
+        assert_same(r, _oracle(g), where="n4")
+    for m in ms:
+        m.free()
