@@ -177,6 +177,9 @@ def lib():
     L.gsofa_symbfact_batch.restype = ctypes.c_int
     L.gsofa_result_free.argtypes = [ctypes.POINTER(_CResult)]
     L.gsofa_result_free.restype = None
+    L.gsofa_result_fetch.argtypes = [vp, ctypes.POINTER(_CResult), _i32p, _i32p, _i32p, _i32p,
+                                     _i64p, _i32p, _i64p, _i32p]
+    L.gsofa_result_fetch.restype = ctypes.c_int
     L.gsofa_predict_scratch_bytes.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(Params)]
     L.gsofa_predict_scratch_bytes.restype = ctypes.c_size_t
     L.gsofa_symbfact_min_id.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.c_int,
@@ -296,6 +299,37 @@ class Context:
         finally:
             lib().gsofa_result_free(ctypes.byref(r))
 
+    def symbfact_into(self, m: Matrix, params: Params, out: dict) -> Result:
+        """Factorizes and copies every result array into caller-owned host
+        buffers (numpy arrays, e.g. views of page-locked memory) named like
+        the Result fields; returns the Result with those arrays (trimmed)."""
+        p = Params()
+        ctypes.pointer(p)[0] = params
+        p.flags |= FLAG_NO_DOWNLOAD
+        r = _CResult()
+        _check(lib().gsofa_symbfact(self._h, m.handle, ctypes.byref(p), ctypes.byref(r)), "gsofa_symbfact")
+        try:
+            res = _convert(r)
+            need = {"u_row_count": r.n, "l_col_count": r.n, "l_row_count": r.n,
+                    "sn_start": r.n_supernodes, "u_ptr": r.n + 1, "l_ptr": r.n + 1,
+                    "u_idx": r.nnz_u if p.want_pattern else 0, "l_idx": r.nnz_l if p.want_pattern else 0}
+            ptrs = {}
+            for k, cnt in need.items():
+                buf = out.get(k)
+                if buf is None or cnt == 0 or (k in ("u_ptr", "l_ptr", "u_idx", "l_idx") and not p.want_pattern):
+                    ptrs[k] = None
+                    continue
+                if buf.shape[0] < cnt:
+                    raise GsofaError(1, f"buffer {k} holds {buf.shape[0]} < {cnt}")
+                ptrs[k] = buf.ctypes.data_as(_i64p if k.endswith("ptr") else _i32p)
+                setattr(res, k, buf[:cnt])
+            _check(lib().gsofa_result_fetch(self._h, ctypes.byref(r), ptrs["u_row_count"], ptrs["l_col_count"],
+                                            ptrs["l_row_count"], ptrs["sn_start"], ptrs["u_ptr"], ptrs["u_idx"],
+                                            ptrs["l_ptr"], ptrs["l_idx"]), "gsofa_result_fetch")
+            return res
+        finally:
+            lib().gsofa_result_free(ctypes.byref(r))
+
     def symbfact_batch(self, mats: Sequence[Matrix], params: Optional[Params] = None, **kw) -> List[Result]:
         p = params if params is not None else Params.default(**kw)
         k = len(mats)
@@ -347,4 +381,4 @@ def exported_symbols() -> List[str]:
     return ["gsofa_symbfact_min_id", "gsofa_status_str", "gsofa_abi_version", "gsofa_default_params",
             "gsofa_create", "gsofa_destroy", "gsofa_set_stream", "gsofa_read_text", "gsofa_free", "gsofa_upload",
             "gsofa_matrix_free", "gsofa_matrix_n", "gsofa_symbfact", "gsofa_symbfact_batch",
-            "gsofa_result_free", "gsofa_predict_scratch_bytes"]
+            "gsofa_result_free", "gsofa_result_fetch", "gsofa_predict_scratch_bytes"]

@@ -68,6 +68,7 @@ struct gsofa_ctx {
     // upload staging
     DevBuf st_beg, st_end, st_adj, st_tmp;
     std::vector<gsofa_matrix *> matrices;
+    uint64_t job_id = 0;      // incremented by every factorization
 
     void *grow(DevBuf &b, size_t bytes)
     {
@@ -110,8 +111,13 @@ struct gsofa_matrix {
 
 namespace {
 
+// Where a result's arrays sit in the context's device buffers (for
+// gsofa_result_fetch); valid while ctx->job_id == job_id.
 struct ResultInternal {
-    // nothing yet; reserved for device-side views
+    uint64_t job_id;
+    int64_t L, line_base, n;
+    int64_t u0, l0;         // first index of the U rows / L columns in `out`
+    std::vector<int32_t> sn;  // supernode starts (relative)
 };
 
 int pick_block(int32_t max_n)
@@ -207,8 +213,9 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     int block = p.block_size ? p.block_size : pick_block(max_n);
     void *kfn = factor_kernel_for(block);
     if (!kfn) return GSOFA_ERR_INVALID_INPUT;
-    int lanes = p.threads_per_source ? p.threads_per_source : 8;
-    if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) return GSOFA_ERR_INVALID_INPUT;
+    int lanes = p.threads_per_source ? p.threads_per_source : 1;
+    if (lanes != 1 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
+        return GSOFA_ERR_INVALID_INPUT;
     int chunk = p.src_chunk > 0 ? p.src_chunk : (reuse ? 32 : 1);
 
     const int32_t bitmap_words = (max_n + 31) / 32;
@@ -268,6 +275,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         }
     }
 
+    ctx->job_id++;
     for (int attempt = 0; attempt < 2; attempt++) {
         // scratch
         int32_t *d_queue = (int32_t *)ctx->grow(ctx->queue, (size_t)grid * qcap * sizeof(int32_t));
@@ -377,6 +385,8 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
             GS_CUDA(cudaMemcpyAsync(&v[3], d_gptr + (L + 1) + lb + n, 8, cudaMemcpyDeviceToHost, st));
             GS_CUDA(cudaStreamSynchronize(st));
             gsofa_result &r = out[i];
+            gp0[i] = v[0];
+            gp1[i] = tot[0] + v[2];
             r.nnz_u = (uint64_t)(v[1] - v[0]);
             r.nnz_l = (uint64_t)(v[3] - v[2]);
             r.nnz_lu = r.nnz_u + r.nnz_l + (uint64_t)n;
@@ -416,6 +426,17 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
                 r.sn_start = (int32_t *)std::malloc(std::max<size_t>((size_t)(e - b), 1) * sizeof(int32_t));
                 if (!r.sn_start) throw std::bad_alloc();
                 for (auto it = b; it != e; ++it) r.sn_start[it - b] = *it - (int32_t)lb;
+            } else {
+                ResultInternal *ri = new ResultInternal();
+                ri->job_id = ctx->job_id;
+                ri->L = L;
+                ri->line_base = lb;
+                ri->n = n;
+                ri->u0 = gp0[i];
+                ri->l0 = gp1[i];
+                ri->sn.reserve((size_t)(e - b));
+                for (auto it = b; it != e; ++it) ri->sn.push_back(*it - (int32_t)lb);
+                r.internal = ri;
             }
             if (want_pattern && download_lines) {
                 const int64_t u0 = r.u_ptr[0], l0 = r.l_ptr[0];
@@ -750,6 +771,47 @@ void gsofa_result_free(gsofa_result *r)
     free_result_arrays(r);
     delete (ResultInternal *)r->internal;
     r->internal = nullptr;
+}
+
+gsofa_status gsofa_result_fetch(gsofa_ctx *c, const gsofa_result *r, int32_t *u_row_count,
+                                int32_t *l_col_count, int32_t *l_row_count, int32_t *sn_start,
+                                int64_t *u_ptr, int32_t *u_idx, int64_t *l_ptr, int32_t *l_idx)
+{
+    if (!c || !r || !r->internal) return GSOFA_ERR_INVALID_INPUT;
+    const ResultInternal *ri = (const ResultInternal *)r->internal;
+    if (ri->job_id != c->job_id) return GSOFA_ERR_INVALID_INPUT;
+    try {
+        GS_CUDA(cudaSetDevice(c->device));
+        cudaStream_t st = c->stream;
+        const int64_t L = ri->L, lb = ri->line_base, n = ri->n;
+        const int32_t *cnt = (const int32_t *)c->cnt.p;
+        const int64_t *gptr = (const int64_t *)c->gptr.p;
+        const int32_t *outb = (const int32_t *)c->out.p;
+        auto cp = [&](void *dst, const void *src, size_t bytes) {
+            if (dst && bytes) GS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+        };
+        cp(u_row_count, cnt + lb, (size_t)n * 4);
+        cp(l_col_count, cnt + L + lb, (size_t)n * 4);
+        cp(l_row_count, (const int32_t *)c->lrow.p + lb, (size_t)n * 4);
+        if ((u_ptr || u_idx || l_ptr || l_idx) && !outb) return GSOFA_ERR_INVALID_INPUT;
+        cp(u_ptr, gptr + lb, (size_t)(n + 1) * 8);
+        cp(l_ptr, gptr + (L + 1) + lb, (size_t)(n + 1) * 8);
+        cp(u_idx, outb + ri->u0, (size_t)r->nnz_u * 4);
+        cp(l_idx, outb + ri->l0, (size_t)r->nnz_l * 4);
+        GS_CUDA(cudaStreamSynchronize(st));
+        if (sn_start && !ri->sn.empty()) std::memcpy(sn_start, ri->sn.data(), ri->sn.size() * 4);
+        if (u_ptr) {
+            const int64_t b = u_ptr[0];
+            for (int64_t s = 0; s <= n; s++) u_ptr[s] -= b;
+        }
+        if (l_ptr) {
+            const int64_t b = l_ptr[0];
+            for (int64_t s = 0; s <= n; s++) l_ptr[s] -= b;
+        }
+    } catch (CudaFail &f) {
+        return fail_cuda(f.e);
+    }
+    return GSOFA_OK;
 }
 
 size_t gsofa_predict_scratch_bytes(const gsofa_ctx *c, int32_t n, int64_t nnz,

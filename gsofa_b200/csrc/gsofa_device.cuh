@@ -68,7 +68,8 @@ struct JobArgs {
     int32_t *queue;            // gridDim.x * qcap
     int64_t qcap;
     int32_t bitmap_words;      // shared-memory bitmap size (>= max n / 32)
-    int32_t lanes;             // lanes per frontier vertex (4..32, power of 2)
+    int32_t lanes;             // lanes per frontier vertex: 1 (thread per vertex,
+                               // warp for long rows) or 4..32
     int32_t reuse;
     int32_t want_pattern;
     int32_t max_sn;
@@ -94,6 +95,7 @@ struct JobArgs {
 };
 
 constexpr int TILE = 2048;     // lines per tile in the post-traversal phases
+constexpr int HEAVY_ROW = 32;  // rows longer than this are expanded by a whole warp
 
 __device__ __forceinline__ int64_t warp_incl_scan(int64_t x)
 {
@@ -231,6 +233,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
     const int lane = tid & 31;
     const unsigned gmask = (lanes == 32) ? 0xffffffffu
                                          : (((1u << lanes) - 1u) << (lane & ~(lanes - 1)));
+    (void)gmask;
 
     if (tid == 0) { sh.qtail = 0; }
     // source bit
@@ -259,6 +262,59 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         if (tid == 0) sh.qnext = lo;
         __syncthreads();
         if (hi == lo) break;
+        if (lanes == 1) {
+            // Thread-per-vertex expansion: a warp takes 32 queue items with one
+            // shared atomic, every lane loads its vertex's row bounds and up to
+            // eight adjacency ids before touching the bitmap (independent loads
+            // in flight hide the L2 latency).  Rows longer than HEAVY_ROW are
+            // expanded by the whole warp.
+            for (;;) {
+                int base = 0;
+                if (lane == 0) base = atomicAdd(&sh.qnext, 32);
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (base >= hi) break;
+                const int it = base + lane;
+                int32_t b = 0, e = 0;
+                if (it < hi) {
+                    const int32_t v = q[it];
+                    b = g.ptr[v];
+                    e = g.ptr[v + 1];
+                    edges += (unsigned long long)(e - b);
+                    if (pass == 0) { xcnt++; einsp += (unsigned long long)rawdeg[v]; }
+                }
+                unsigned heavy = __ballot_sync(0xffffffffu, e - b > HEAVY_ROW);
+                while (heavy) {
+                    const int src = __ffs(heavy) - 1;
+                    heavy &= heavy - 1u;
+                    const int32_t hb = __shfl_sync(0xffffffffu, b, src);
+                    const int32_t he = __shfl_sync(0xffffffffu, e, src);
+                    for (int32_t k = hb + lane; k < he; k += 32) {
+                        const int32_t m = g.adj[k];
+                        if (test_and_set(bm, m)) {
+                            t_lo = min(t_lo, m); t_hi = max(t_hi, m);
+                            if (m < s) enqueue(q, a.qcap, &sh.qtail, a.status, m);
+                        }
+                    }
+                }
+                if (e - b <= HEAVY_ROW) {
+                    for (int32_t k0 = b; k0 < e; k0 += 8) {
+                        int32_t buf[8];
+#pragma unroll
+                        for (int u = 0; u < 8; u++) buf[u] = (k0 + u < e) ? g.adj[k0 + u] : -1;
+#pragma unroll
+                        for (int u = 0; u < 8; u++) {
+                            const int32_t m = buf[u];
+                            if (m >= 0 && test_and_set(bm, m)) {
+                                t_lo = min(t_lo, m); t_hi = max(t_hi, m);
+                                if (m < s) enqueue(q, a.qcap, &sh.qtail, a.status, m);
+                            }
+                        }
+                    }
+                }
+            }
+            lo = hi;
+            continue;
+        }
         for (;;) {
             int it = 0;
             if (lane_in_group == 0) it = atomicAdd(&sh.qnext, 1);

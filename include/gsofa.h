@@ -64,7 +64,8 @@ typedef struct gsofa_params {
     int32_t src_chunk;          /* consecutive sources per work item          */
     int32_t block_size;         /* threads per CTA: 128, 256, 512 or 1024     */
     int32_t threads_per_source; /* lanes expanding one frontier vertex:
-                                   4, 8, 16 or 32                             */
+                                   1 (default: one thread per vertex, a warp
+                                   for rows longer than 32), 4, 8, 16 or 32   */
     int32_t ctas_per_sm;        /* resident CTAs per SM                       */
     int64_t queue_capacity;     /* frontier entries per CTA (>= n, else n)    */
     int64_t pool_capacity;      /* pattern entries kept on the device         */
@@ -170,6 +171,17 @@ gsofa_status gsofa_symbfact_batch(gsofa_ctx *ctx, int count,
                                   gsofa_result *out);
 
 void gsofa_result_free(gsofa_result *r);
+
+/* Copies the arrays of a result made with GSOFA_FLAG_NO_DOWNLOAD into
+ * caller-owned host buffers (page-locked buffers give full PCIe speed).  Any
+ * pointer may be NULL; sizes follow the result: n for the per-line counts,
+ * n_supernodes, n+1 for the offsets, nnz_u / nnz_l for the indices.  Valid
+ * until the next factorization on ctx (GSOFA_ERR_INVALID_INPUT after it). */
+gsofa_status gsofa_result_fetch(gsofa_ctx *ctx, const gsofa_result *r,
+                                int32_t *u_row_count, int32_t *l_col_count,
+                                int32_t *l_row_count, int32_t *sn_start,
+                                int64_t *u_ptr, int32_t *u_idx,
+                                int64_t *l_ptr, int32_t *l_idx);
 
 /* Device scratch bytes a factorization of an n-line, nnz-entry matrix needs
  * with these parameters, excluding the pattern pool (admission control). */

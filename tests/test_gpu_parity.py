@@ -71,7 +71,7 @@ def test_empty_and_tiny(ctx):
 
 @pytest.mark.parametrize("block,lanes,reuse,chunk,per_sm", [
     (128, 4, 0, 1, 0), (256, 8, 1, 7, 1), (512, 16, 1, 32, 0), (1024, 32, 0, 3, 0),
-    (256, 32, 1, 1, 2), (512, 8, 1, 200, 0)])
+    (256, 32, 1, 1, 2), (512, 8, 1, 200, 0), (128, 1, 0, 1, 0), (1024, 1, 1, 16, 1)])
 def test_parameters_do_not_change_results(ctx, block, lanes, reuse, chunk, per_sm):
     g = matgen.grid3d(14, ordering="nd", drop_frac=0.1, seed=5)
     ref = _oracle(g, 8)
@@ -157,3 +157,33 @@ def test_exhaustive_n4_in_one_batch(ctx):
         assert_same(r, _oracle(g), where="n4")
     for m in ms:
         m.free()
+
+
+def test_fetch_into_caller_buffers(ctx):
+    g = matgen.grid3d(11, ordering="nd", drop_frac=0.1, seed=3)
+    ref = _oracle(g, 6)
+    m = ctx.upload(g)
+    n = g.n
+    big = 4 * int(ref["u_idx"].shape[0] + 10)
+    bufs = {"u_row_count": np.zeros(n, np.int32), "l_col_count": np.zeros(n, np.int32),
+            "l_row_count": np.zeros(n, np.int32), "sn_start": np.zeros(n, np.int32),
+            "u_ptr": np.zeros(n + 1, np.int64), "l_ptr": np.zeros(n + 1, np.int64),
+            "u_idx": np.zeros(big, np.int32), "l_idx": np.zeros(big, np.int32)}
+    r = ctx.symbfact_into(m, gsofa_b200.Params.default(max_supernode_size=6), bufs)
+    assert_same(r, ref, where="fetch")
+    # a stale result cannot be fetched after the next factorization
+    p = gsofa_b200.Params.default(flags=gsofa_b200.FLAG_NO_DOWNLOAD)
+    r1 = gsofa_b200._CResult()
+    L = gsofa_b200.lib()
+    assert L.gsofa_symbfact(ctx._h, m.handle, p, r1) == 0
+    r2 = gsofa_b200._CResult()
+    assert L.gsofa_symbfact(ctx._h, m.handle, p, r2) == 0
+    z = np.zeros(n, np.int32)
+    i32 = gsofa_b200._i32p
+    assert L.gsofa_result_fetch(ctx._h, r1, z.ctypes.data_as(i32), None, None, None, None, None,
+                                None, None) == 1
+    assert L.gsofa_result_fetch(ctx._h, r2, z.ctypes.data_as(i32), None, None, None, None, None,
+                                None, None) == 0
+    assert np.array_equal(z, ref["u_row_count"])
+    L.gsofa_result_free(r1)
+    L.gsofa_result_free(r2)
