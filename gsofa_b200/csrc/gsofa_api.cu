@@ -191,7 +191,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     const int part_index = p.part_count > 1 ? p.part_index : 0;
     if (part_index < 0 || part_index >= part_count) return GSOFA_ERR_INVALID_INPUT;
     const bool want_pattern = p.want_pattern != 0 && part_count == 1;
-    const int reuse = (p.reuse > 0 && part_count == 1) ? 1 : 0;
+    const int reuse = (p.reuse != 0 && part_count == 1) ? 1 : 0;   // -1 (auto): on
 
     // line space and per-matrix descriptors
     std::vector<MatDesc> md(count);
@@ -218,9 +218,14 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         return GSOFA_ERR_INVALID_INPUT;
     int chunk = p.src_chunk > 0 ? p.src_chunk : (reuse ? 32 : 1);
 
-    const int32_t bitmap_words = (max_n + 31) / 32;
-    const size_t smem = ((size_t)bitmap_words * 4 + 15) / 16 * 16;
-    if (smem + sizeof(SharedState) + 1024 > ctx->smem_optin) return GSOFA_ERR_UNSUPPORTED;
+    const int32_t bitmap_words = ((max_n + 31) / 32 + 3) / 4 * 4;
+    const size_t static_smem = sizeof(SharedState) + 1024;
+    if ((size_t)bitmap_words * 4 + 1024 * 4 + static_smem > ctx->smem_optin) return GSOFA_ERR_UNSUPPORTED;
+    // frontier ring: 8K entries when they fit beside the bitmap, else smaller
+    int ring = 8192;
+    while (ring > 1024 && (size_t)bitmap_words * 4 + (size_t)ring * 4 + static_smem > ctx->smem_optin)
+        ring >>= 1;
+    const size_t smem = (size_t)bitmap_words * 4 + (size_t)ring * 4;
     GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int occ = 0;
     GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, block, smem));
@@ -323,6 +328,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         a.queue = d_queue;
         a.qcap = qcap;
         a.bitmap_words = bitmap_words;
+        a.ring_size = ring;
         a.lanes = lanes;
         a.reuse = reuse;
         a.want_pattern = want_pattern ? 1 : 0;
@@ -486,7 +492,7 @@ void gsofa_default_params(gsofa_params *p)
     if (!p) return;
     std::memset(p, 0, sizeof(*p));
     p->want_pattern = 1;
-    p->reuse = 0;
+    p->reuse = -1;
     p->part_count = 1;
 }
 

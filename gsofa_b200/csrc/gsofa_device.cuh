@@ -67,7 +67,8 @@ struct JobArgs {
     unsigned long long *piece_counter; // dynamic fetch of work pieces
     int32_t *queue;            // gridDim.x * qcap
     int64_t qcap;
-    int32_t bitmap_words;      // shared-memory bitmap size (>= max n / 32)
+    int32_t bitmap_words;      // shared-memory bitmap size (>= max n / 32, multiple of 4)
+    int32_t ring_size;         // shared-memory frontier ring entries (power of two)
     int32_t lanes;             // lanes per frontier vertex: 1 (thread per vertex,
                                // warp for long rows) or 4..32
     int32_t reuse;
@@ -182,27 +183,53 @@ __device__ __forceinline__ bool test_and_set(uint32_t *bm, int32_t m)
     return !(atomicOr(w, bit) & bit);
 }
 
-// Appends m to the CTA's frontier queue; one shared atomic per coalesced
-// group of lanes (warp-aggregated enqueue).
-__device__ __forceinline__ void enqueue(int32_t *q, int64_t qcap, int *s_qtail,
-                                        uint32_t *status, int32_t m)
+// Frontier queue of one source: absolute positions 0, 1, 2, ... in BFS order.
+// A position p written while the writer's level started at w0 lives in the
+// shared-memory ring (ring_size entries, a power of two) when
+// p - w0 < ring_size and in the CTA's global spill array otherwise; readers
+// apply the same rule with the same w0.  Ring entries of one level and of the
+// level it feeds always lie within ring_size consecutive positions, so live
+// ring slots never collide.
+struct Frontier {
+    int32_t *ring;    // shared memory
+    int32_t *spill;   // global memory, qcap entries (this CTA's slice)
+    int64_t qcap;
+    uint32_t *status;
+    int ring_size;
+};
+
+__device__ __forceinline__ void fr_put(const Frontier &f, int p, int w0, int32_t m)
+{
+    if (p - w0 < f.ring_size) f.ring[p & (f.ring_size - 1)] = m;
+    else if ((int64_t)p < f.qcap) f.spill[p] = m;
+    else atomicOr(f.status, ERR_QUEUE_OVERFLOW);  // cannot happen: p < n <= qcap
+}
+
+__device__ __forceinline__ int32_t fr_get(const Frontier &f, int p, int w0)
+{
+    return (p - w0 < f.ring_size) ? f.ring[p & (f.ring_size - 1)] : f.spill[p];
+}
+
+// Appends m to the next level; one shared atomic per coalesced group of lanes
+// (warp-aggregated enqueue).  base: first position of the next level;
+// w0: first position of the current level.
+__device__ __forceinline__ void push(const Frontier &f, int *tail, int base, int w0, int32_t m)
 {
     cg::coalesced_group g = cg::coalesced_threads();
-    int base = 0;
-    if (g.thread_rank() == 0) base = atomicAdd(s_qtail, (int)g.size());
-    base = g.shfl(base, 0);
-    const int64_t pos = (int64_t)base + g.thread_rank();
-    if (pos < qcap) q[pos] = m;
-    else atomicOr(status, 2u);  // ERR_QUEUE_OVERFLOW; cannot happen with qcap >= n
+    int b = 0;
+    if (g.thread_rank() == 0) b = atomicAdd(tail, (int)g.size());
+    b = g.shfl(b, 0);
+    fr_put(f, base + b + (int)g.thread_rank(), w0, m);
 }
 
 struct SharedState {
     long long piece;
     int flag;
-    int qtail;
-    int qnext;
+    int tailc[3];     // entries pushed for level L live in tailc[L % 3]
+    int fetch[3];     // dynamic fetch counter of level L in fetch[L % 3]
     int chain_lo;     // lowest vertex set in the bitmap since the last clear
     int chain_hi;     // highest vertex set since the last clear
+    int seg[2];       // piece boundaries after chain alignment
     int64_t pool_base;
     int64_t warp[32];
 };
@@ -215,6 +242,41 @@ __device__ __forceinline__ void clear_range(uint32_t *bm, int lo, int hi)
     for (int w = (lo >> 5) + threadIdx.x; w <= (hi >> 5); w += BLOCK) bm[w] = 0u;
 }
 
+// True when x-1 is in adj(x); evaluated by one whole warp.
+__device__ __forceinline__ bool warp_has_prev(const PassGraph &g, int32_t x)
+{
+    const int lane = threadIdx.x & 31;
+    bool hit = false;
+    for (int32_t k = g.ptr[x] + lane; k < g.ptr[x + 1]; k += 32)
+        hit |= (g.adj[k] == x - 1);
+    return __any_sync(0xffffffffu, hit);
+}
+
+// The chain start at or below x: the lowest y with y+1 .. x each holding its
+// predecessor, searched at most `limit - 1` steps down; x itself when the
+// chain reaches further (then the cut is not aligned).  Warp 0 only.
+__device__ __forceinline__ int32_t chain_start(const PassGraph &g, int32_t x, int32_t limit)
+{
+    int32_t y = x;
+    for (int step = 0; step < limit - 1; step++) {
+        if (y == 0 || !warp_has_prev(g, y)) return y;
+        y--;
+    }
+    return (y == 0 || !warp_has_prev(g, y)) ? y : x;
+}
+
+// Visits neighbour m of a frontier vertex: marks it, and queues it for the
+// next level when it lies below the source.
+#define GSOFA_VISIT(m)                                                          \
+    do {                                                                        \
+        const int32_t _m = (m);                                                 \
+        if (test_and_set(bm, _m)) {                                             \
+            t_lo = min(t_lo, _m);                                               \
+            t_hi = max(t_hi, _m);                                               \
+            if (_m < s) push(f, tailp, end, start, _m);                         \
+        }                                                                       \
+    } while (0)
+
 // One source s of one pass: seeds from adj(s), expands the frontier level by
 // level through vertices < s, then counts (and optionally writes) hi(s).
 // With `reuse`, the bitmap still holds the finished traversal of s-1, which is
@@ -223,60 +285,58 @@ __device__ __forceinline__ void clear_range(uint32_t *bm, int lo, int hi)
 template <int BLOCK>
 __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                                int64_t line, int pass, int32_t s, uint32_t *bm,
-                               int32_t *q, SharedState &sh, int &t_lo, int &t_hi,
+                               const Frontier &f, SharedState &sh,
                                unsigned long long &edges, const int32_t *rawdeg,
                                unsigned long long &xcnt, unsigned long long &einsp)
 {
     const int tid = threadIdx.x;
+    const int lane = tid & 31;
     const int lanes = a.lanes;
     const int lane_in_group = tid & (lanes - 1);
-    const int lane = tid & 31;
-    const unsigned gmask = (lanes == 32) ? 0xffffffffu
-                                         : (((1u << lanes) - 1u) << (lane & ~(lanes - 1)));
-    (void)gmask;
+    int t_lo = INT32_MAX, t_hi = -1;
 
-    if (tid == 0) { sh.qtail = 0; }
-    // source bit
-    if (tid == 0 && test_and_set(bm, s)) { t_lo = min(t_lo, s); t_hi = max(t_hi, s); }
+    if (tid == 0) {
+        sh.tailc[0] = sh.tailc[1] = sh.tailc[2] = 0;
+        sh.fetch[0] = sh.fetch[1] = sh.fetch[2] = 0;
+        if (test_and_set(bm, s)) { t_lo = s; t_hi = s; }
+    }
     __syncthreads();
 
-    // seeding: every neighbour of s is structure of line s
-    const int32_t b0 = g.ptr[s], e0 = g.ptr[s + 1];
-    if (tid == 0) {
-        edges += (unsigned long long)(e0 - b0);
-        if (pass == 0) einsp += (unsigned long long)rawdeg[s];
-    }
-    for (int32_t k = b0 + tid; k < e0; k += BLOCK) {
-        int32_t m = g.adj[k];
-        if (test_and_set(bm, m)) {
-            t_lo = min(t_lo, m); t_hi = max(t_hi, m);
-            if (m < s) enqueue(q, a.qcap, &sh.qtail, a.status, m);
+    // seeding: every neighbour of s is structure of line s; level-0 items
+    {
+        const int32_t b0 = g.ptr[s], e0 = g.ptr[s + 1];
+        if (tid == 0) {
+            edges += (unsigned long long)(e0 - b0);
+            if (pass == 0) einsp += (unsigned long long)rawdeg[s];
         }
+        int *tailp = &sh.tailc[0];
+        const int end = 0, start = 0;
+        for (int32_t k = b0 + tid; k < e0; k += BLOCK) GSOFA_VISIT(g.adj[k]);
     }
 
-    // level-synchronous expansion restricted to vertices < s
-    int lo = 0;
-    for (;;) {
+    // level-synchronous expansion through vertices < s, one barrier a level
+    int start = 0, wstart = 0;
+    for (int L = 0;; L++) {
         __syncthreads();
-        const int hi = sh.qtail;
-        if (tid == 0) sh.qnext = lo;
-        __syncthreads();
-        if (hi == lo) break;
+        const int end = start + sh.tailc[L % 3];
+        if (end == start) break;
+        if (tid == 0) { sh.tailc[(L + 2) % 3] = 0; sh.fetch[(L + 1) % 3] = 0; }
+        int *tailp = &sh.tailc[(L + 1) % 3];
+        int *fetchp = &sh.fetch[L % 3];
         if (lanes == 1) {
-            // Thread-per-vertex expansion: a warp takes 32 queue items with one
-            // shared atomic, every lane loads its vertex's row bounds and up to
-            // eight adjacency ids before touching the bitmap (independent loads
-            // in flight hide the L2 latency).  Rows longer than HEAVY_ROW are
+            // One thread per vertex: a warp takes 32 items with one shared
+            // atomic; every lane loads its row bounds and up to eight ids
+            // before touching the bitmap.  Rows longer than HEAVY_ROW are
             // expanded by the whole warp.
             for (;;) {
                 int base = 0;
-                if (lane == 0) base = atomicAdd(&sh.qnext, 32);
-                base = __shfl_sync(0xffffffffu, base, 0);
-                if (base >= hi) break;
+                if (lane == 0) base = atomicAdd(fetchp, 32);
+                base = __shfl_sync(0xffffffffu, base, 0) + start;
+                if (base >= end) break;
                 const int it = base + lane;
                 int32_t b = 0, e = 0;
-                if (it < hi) {
-                    const int32_t v = q[it];
+                if (it < end) {
+                    const int32_t v = fr_get(f, it, wstart);
                     b = g.ptr[v];
                     e = g.ptr[v + 1];
                     edges += (unsigned long long)(e - b);
@@ -288,13 +348,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                     heavy &= heavy - 1u;
                     const int32_t hb = __shfl_sync(0xffffffffu, b, src);
                     const int32_t he = __shfl_sync(0xffffffffu, e, src);
-                    for (int32_t k = hb + lane; k < he; k += 32) {
-                        const int32_t m = g.adj[k];
-                        if (test_and_set(bm, m)) {
-                            t_lo = min(t_lo, m); t_hi = max(t_hi, m);
-                            if (m < s) enqueue(q, a.qcap, &sh.qtail, a.status, m);
-                        }
-                    }
+                    for (int32_t k = hb + lane; k < he; k += 32) GSOFA_VISIT(g.adj[k]);
                 }
                 if (e - b <= HEAVY_ROW) {
                     for (int32_t k0 = b; k0 < e; k0 += 8) {
@@ -302,113 +356,107 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
 #pragma unroll
                         for (int u = 0; u < 8; u++) buf[u] = (k0 + u < e) ? g.adj[k0 + u] : -1;
 #pragma unroll
-                        for (int u = 0; u < 8; u++) {
-                            const int32_t m = buf[u];
-                            if (m >= 0 && test_and_set(bm, m)) {
-                                t_lo = min(t_lo, m); t_hi = max(t_hi, m);
-                                if (m < s) enqueue(q, a.qcap, &sh.qtail, a.status, m);
-                            }
-                        }
+                        for (int u = 0; u < 8; u++)
+                            if (buf[u] >= 0) GSOFA_VISIT(buf[u]);
                     }
                 }
             }
-            lo = hi;
-            continue;
-        }
-        for (;;) {
-            int it = 0;
-            if (lane_in_group == 0) it = atomicAdd(&sh.qnext, 1);
-            it = __shfl_sync(gmask, it, 0, lanes);
-            if (it >= hi) break;
-            const int32_t v = q[it];
-            const int32_t b = g.ptr[v], e = g.ptr[v + 1];
-            if (lane_in_group == 0) {
-                edges += (unsigned long long)(e - b);
-                if (pass == 0) { xcnt++; einsp += (unsigned long long)rawdeg[v]; }
-            }
-            for (int32_t k = b + lane_in_group; k < e; k += lanes) {
-                const int32_t m = g.adj[k];
-                if (test_and_set(bm, m)) {
-                    t_lo = min(t_lo, m); t_hi = max(t_hi, m);
-                    if (m < s) enqueue(q, a.qcap, &sh.qtail, a.status, m);
+        } else {
+            // groups of `lanes` threads per vertex
+            const unsigned gmask = (lanes == 32)
+                                       ? 0xffffffffu
+                                       : (((1u << lanes) - 1u) << (lane & ~(lanes - 1)));
+            for (;;) {
+                int it = 0;
+                if (lane_in_group == 0) it = atomicAdd(fetchp, 1);
+                it = __shfl_sync(gmask, it, 0, lanes) + start;
+                if (it >= end) break;
+                const int32_t v = fr_get(f, it, wstart);
+                const int32_t b = g.ptr[v], e = g.ptr[v + 1];
+                if (lane_in_group == 0) {
+                    edges += (unsigned long long)(e - b);
+                    if (pass == 0) { xcnt++; einsp += (unsigned long long)rawdeg[v]; }
                 }
+                for (int32_t k = b + lane_in_group; k < e; k += lanes) GSOFA_VISIT(g.adj[k]);
             }
         }
-        lo = hi;
+        wstart = start;
+        start = end;
     }
 
-    // fold the per-thread touched range into the chain range
+    // fold the touched range into the chain range (warp reduce + shared atomics)
     {
-        int64_t vmax, vneg;
-        block_excl_max<BLOCK>((int64_t)t_hi, &vmax, sh.warp);
-        block_excl_max<BLOCK>(-(int64_t)t_lo, &vneg, sh.warp);
-        if (tid == 0) {
-            sh.chain_hi = max(sh.chain_hi, (int)vmax);
-            sh.chain_lo = min(sh.chain_lo, (int)(-vneg));
+        const int wl = __reduce_min_sync(0xffffffffu, t_lo);
+        const int wh = __reduce_max_sync(0xffffffffu, t_hi);
+        if (lane == 0) {
+            if (wl != INT32_MAX) atomicMin(&sh.chain_lo, wl);
+            if (wh >= 0) atomicMax(&sh.chain_hi, wh);
         }
         __syncthreads();
     }
     const int chain_hi = sh.chain_hi;
 
-    // hi(s) = set bits in (s, chain_hi]
+    // hi(s) = set bits in (s, chain_hi]; each thread owns a contiguous span of
+    // words, one block scan gives every span its output offset
     const int w0 = (s + 1) >> 5;
     const int w1 = (chain_hi > s) ? (chain_hi >> 5) : (w0 - 1);
+    const int nw = w1 - w0 + 1;
+    const int per = nw > 0 ? (nw + BLOCK - 1) / BLOCK : 0;
+    const int my0 = w0 + tid * per;
+    const int my1 = min(my0 + per, w1 + 1);
+    const uint32_t first_mask = ~0u << ((s + 1) & 31);
     int64_t count = 0;
-    for (int w = w0 + tid; w <= w1; w += BLOCK) {
+    for (int w = my0; w < my1; w++) {
         uint32_t x = bm[w];
-        if (w == w0) x &= ~0u << ((s + 1) & 31);
+        if (w == w0) x &= first_mask;
         count += __popc(x);
     }
-    const int64_t total = block_sum<BLOCK>(count, sh.warp);
+    int64_t total;
+    const int64_t off = block_excl_scan<BLOCK>(count, &total, sh.warp);
 
     const int64_t slot = (int64_t)pass * a.L + line;
     if (tid == 0) {
         a.cnt[slot] = (int32_t)total;
         a.nxt[slot] = (uint8_t)((s + 1 < n) && ((bm[(s + 1) >> 5] >> ((s + 1) & 31)) & 1u));
-    }
-    if (a.want_pattern) {
-        if (tid == 0) {
-            unsigned long long off = atomicAdd(a.pool_tail, (unsigned long long)total);
-            if ((int64_t)off + total > a.pool_cap) {
+        if (a.want_pattern) {
+            const unsigned long long o = atomicAdd(a.pool_tail, (unsigned long long)total);
+            if ((int64_t)o + total > a.pool_cap) {
                 atomicOr(a.status, ERR_POOL_OVERFLOW);
                 sh.pool_base = -1;
             } else {
-                sh.pool_base = (int64_t)off;
+                sh.pool_base = (int64_t)o;
             }
             a.poff[slot] = sh.pool_base;
         }
+    }
+    if (a.want_pattern) {
         __syncthreads();
         const int64_t base = sh.pool_base;
-        if (base >= 0 && total > 0) {
-            int64_t run = base;
-            // tiles of BLOCK words, block-wide scan for sorted output
-            for (int wt = w0; wt <= w1; wt += BLOCK) {
-                const int w = wt + tid;
-                uint32_t x = 0u;
-                if (w <= w1) {
-                    x = bm[w];
-                    if (w == w0 && ((s + 1) & 31)) x &= ~0u << ((s + 1) & 31);
-                }
-                int64_t tot;
-                int64_t pos = run + block_excl_scan<BLOCK>((int64_t)__popc(x), &tot, sh.warp);
+        if (base >= 0 && count > 0) {
+            int32_t *dst = a.pool + base + off;
+            for (int w = my0; w < my1; w++) {
+                uint32_t x = bm[w];
+                if (w == w0) x &= first_mask;
                 while (x) {
                     const int bit = __ffs(x) - 1;
                     x &= x - 1u;
-                    a.pool[pos++] = (w << 5) + bit;
+                    *dst++ = (w << 5) + bit;
                 }
-                run += tot;
             }
         }
     }
     __syncthreads();
 }
+#undef GSOFA_VISIT
 
 // ---------------------------------------------------------------------------
 // The persistent cooperative factorization kernel.
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
 {
-    extern __shared__ __align__(16) uint32_t bm[];
+    extern __shared__ __align__(16) uint32_t smem_dyn[];
+    uint32_t *bm = smem_dyn;                                  // bitmap_words
+    int32_t *ring = (int32_t *)(smem_dyn + a.bitmap_words);   // ring_size entries
     __shared__ SharedState sh;
     cg::grid_group grid = cg::this_grid();
     const int tid = threadIdx.x;
@@ -416,7 +464,7 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
     // ---- phase 1: traversals ------------------------------------------------
     for (int w = tid; w < a.bitmap_words; w += BLOCK) bm[w] = 0u;
     if (tid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
-    int32_t *q = a.queue + (int64_t)blockIdx.x * a.qcap;
+    const Frontier fr{ring, a.queue + (int64_t)blockIdx.x * a.qcap, a.qcap, a.status, a.ring_size};
     unsigned long long edges = 0, nsrc = 0, xcnt = 0, einsp = 0;
     __syncthreads();
     for (;;) {
@@ -440,15 +488,28 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
         const int64_t j0 = max((int64_t)0, j1 - rg.chunk);
         const MatDesc md = a.mats[rg.mat];
         const PassGraph g = md.g[pass];
+        int32_t s_lo = rg.offset + (int32_t)j0 * rg.stride;
+        int32_t s_hi = rg.offset + (int32_t)j1 * rg.stride;   // exclusive (stride 1)
+        if (a.reuse && rg.stride == 1) {
+            // cut pieces where chains start, so a piece's first source rarely
+            // has a predecessor whose traversal it could have reused
+            if (tid < 32) {
+                const int32_t lo = (j0 == 0) ? s_lo : chain_start(g, s_lo, rg.chunk);
+                const int32_t hi = (j1 == rg.nj) ? s_hi : chain_start(g, s_hi, rg.chunk);
+                if (tid == 0) { sh.seg[0] = lo; sh.seg[1] = hi; }
+            }
+            __syncthreads();
+            s_lo = sh.seg[0];
+            s_hi = sh.seg[1];
+        }
         int prev = -2;
-        for (int64_t j = j0; j < j1; j++) {
-            const int32_t s = rg.offset + (int32_t)j * rg.stride;
+        for (int32_t s = s_lo; s < s_hi; s += rg.stride) {
             int reuse = 0;
             if (a.reuse && prev == s - 1) {
-                if (tid == 0) sh.flag = 0;
-                __syncthreads();
-                for (int32_t k = g.ptr[s] + tid; k < g.ptr[s + 1]; k += BLOCK)
-                    if (g.adj[k] == s - 1) sh.flag = 1;
+                if (tid < 32) {
+                    const bool h = warp_has_prev(g, s);
+                    if (tid == 0) sh.flag = h ? 1 : 0;
+                }
                 __syncthreads();
                 reuse = sh.flag;
             }
@@ -458,13 +519,12 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
                 __syncthreads();
                 if (tid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
             }
-            int t_lo = INT32_MAX, t_hi = -1;
-            process_source<BLOCK>(a, g, md.n, md.line_base + s, pass, s, bm, q,
-                                  sh, t_lo, t_hi, edges, md.rawdeg, xcnt, einsp);
+            process_source<BLOCK>(a, g, md.n, md.line_base + s, pass, s, bm, fr, sh, edges,
+                                  md.rawdeg, xcnt, einsp);
             prev = s;
             nsrc++;
         }
-        // the next item starts from an empty bitmap
+        // the next piece starts from an empty bitmap
         {
             const int clo = sh.chain_lo, chi = sh.chain_hi;
             clear_range<BLOCK>(bm, clo, chi);

@@ -74,7 +74,7 @@ typedef struct gsofa_params {
     int32_t reuse;              /* 1: reuse traversal state along a chain of
                                    sources s-1 -> s when s-1 is in adj(s);
                                    0: every source starts from scratch;
-                                   -1: choose automatically (default 0)       */
+                                   -1 (default): automatic, currently 1       */
     int32_t flags;              /* GSOFA_FLAG_* bits                          */
     int32_t part_count;         /* >1: process only the sources s with        */
     int32_t part_index;         /*     s % part_count == part_index (the

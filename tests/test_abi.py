@@ -39,7 +39,7 @@ def test_abi_version_and_status_strings():
     for s in range(8):
         assert L.gsofa_status_str(s)
     p = gsofa_b200.Params.default()
-    assert p.want_pattern == 1 and p.part_count == 1 and p.reuse == 0
+    assert p.want_pattern == 1 and p.part_count == 1 and p.reuse == -1
 
 
 def test_params_layout_matches_header():
