@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--pattern", type=int, default=-1,
+                    help="materialize the L+U pattern (-1: yes except for the circuit workload, "
+                         "whose pattern does not fit in memory)")
     return ap.parse_args()
 
 
@@ -232,11 +235,12 @@ def main():
                                 device_id=torch.device("cuda", local))
 
     g, cfg = workload(args)
+    want_pattern = args.pattern if args.pattern >= 0 else int(args.workload != "circuit")
     ctx = gsofa_b200.Context(local)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
     m = ctx.upload(g)
-    params = gsofa_b200.Params.default(want_pattern=1, flags=gsofa_b200.FLAG_NO_DOWNLOAD,
+    params = gsofa_b200.Params.default(want_pattern=want_pattern, flags=gsofa_b200.FLAG_NO_DOWNLOAD,
                                        reuse=args.reuse, block_size=args.block,
                                        threads_per_source=args.lanes, ctas_per_sm=args.ctas_per_sm)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
@@ -283,7 +287,7 @@ def main():
         pb = torch.from_numpy(g.beg).pin_memory()
         pe = torch.from_numpy(g.end).pin_memory()
         pa = torch.from_numpy(g.adj).pin_memory()
-        pe2e = gsofa_b200.Params.default(want_pattern=1, reuse=args.reuse, block_size=args.block,
+        pe2e = gsofa_b200.Params.default(want_pattern=want_pattern, reuse=args.reuse, block_size=args.block,
                                          threads_per_source=args.lanes, ctas_per_sm=args.ctas_per_sm)
         # page-locked result buffers, sized from the warm-up result, reused
         n1 = g.n + 1
@@ -292,9 +296,10 @@ def main():
             return torch.empty(max(int(count), 1), dtype=dt).pin_memory().numpy()
 
         bufs = {"u_row_count": pinned(g.n, torch.int32), "l_col_count": pinned(g.n, torch.int32),
-                "l_row_count": pinned(g.n, torch.int32), "sn_start": pinned(g.n, torch.int32),
-                "u_ptr": pinned(n1, torch.int64), "l_ptr": pinned(n1, torch.int64),
-                "u_idx": pinned(res.nnz_u, torch.int32), "l_idx": pinned(res.nnz_l, torch.int32)}
+                "l_row_count": pinned(g.n, torch.int32), "sn_start": pinned(g.n, torch.int32)}
+        if want_pattern:
+            bufs.update(u_ptr=pinned(n1, torch.int64), l_ptr=pinned(n1, torch.int64),
+                        u_idx=pinned(res.nnz_u, torch.int32), l_idx=pinned(res.nnz_l, torch.int32))
         out = None
         for _ in range(1):   # warm the host-side allocations
             mm = ctx.upload(pb.numpy(), pe.numpy(), pa.numpy())
@@ -322,7 +327,9 @@ def main():
             te = float(tt.item())
         assert out.nnz_lu == nnz_lu and out.fill_count == res.fill_count
         h2d = (2 * g.n + g.nnz) * 4
-        d2h = 4 * (out.nnz_u + out.nnz_l) + 2 * 8 * (g.n + 1) + 3 * 4 * g.n + 4 * out.n_supernodes
+        d2h = 3 * 4 * g.n + 4 * out.n_supernodes
+        if want_pattern:
+            d2h += 4 * (out.nnz_u + out.nnz_l) + 2 * 8 * (g.n + 1)
         e2e = {"value": world * k2 * nnz_lu / (te / 1000.0), "unit": "nnz/s", "steps": k2,
                "ms_per_step": te / k2, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
 
@@ -339,7 +346,7 @@ def main():
     peak, peak_kind = hbm_peak()
     kms = statistics.mean(kernel_ms)
     n = g.n
-    b_alg = 8 * ideal.x_total + 8 * ideal.e_insp + 4 * nnz_lu + 8 * n
+    b_alg = 8 * ideal.x_total + 8 * ideal.e_insp + (4 * nnz_lu if want_pattern else 0) + 8 * n
     achieved = b_alg / (kms / 1000.0) / 1e9
     traffic = traffic_per_launch(cfg["workload"])
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -347,7 +354,9 @@ def main():
             "algorithmic_bytes": int(b_alg), "kernel_ms": kms, "x_total": ideal.x_total,
             "e_insp": ideal.e_insp, "edges_inspected": res.edges_inspected,
             "edges_inspected_without_reuse": ideal.edges_inspected,
-            "work_ratio": res.edges_inspected / max(ideal.edges_inspected, 1)}
+            "work_ratio": res.edges_inspected / max(ideal.edges_inspected, 1),
+            "levels": res.levels, "reused_sources": res.reused_sources, "sources": res.sources,
+            "cycles_expand_output_clear": list(res.cycles), "ctas": res.ctas}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -361,7 +370,8 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded generator)",
             "config": dict(cfg, nnz_lu=int(nnz_lu), fill_count=int(res.fill_count),
-                           supernodes=int(res.n_supernodes), pattern="on device",
+                           supernodes=int(res.n_supernodes),
+                           pattern="on device" if want_pattern else "counts only",
                            reuse=args.reuse, l2="flushed between steps (256 MiB write)",
                            parallelism=f"independent factorization per rank x{world}"),
             "factorizations_per_s": facts,

@@ -92,6 +92,10 @@ class _CResult(ctypes.Structure):
         ("sources", ctypes.c_uint64),
         ("x_total", ctypes.c_uint64),
         ("e_insp", ctypes.c_uint64),
+        ("levels", ctypes.c_uint64),
+        ("reused_sources", ctypes.c_uint64),
+        ("cycles", ctypes.c_uint64 * 3),
+        ("ctas", ctypes.c_uint64),
         ("kernel_ms", ctypes.c_double),
         ("u_row_count", _i32p),
         ("l_col_count", _i32p),
@@ -124,6 +128,10 @@ class Result:
     x_total: int
     e_insp: int
     kernel_ms: float
+    levels: int = 0
+    reused_sources: int = 0
+    cycles: tuple = (0, 0, 0)
+    ctas: int = 0
     u_row_count: Optional[np.ndarray] = None
     l_col_count: Optional[np.ndarray] = None
     l_row_count: Optional[np.ndarray] = None
@@ -207,7 +215,9 @@ def _convert(r: _CResult) -> Result:
     out = Result(n=n, fill_count=int(r.fill_count), nnz_lu=int(r.nnz_lu), nnz_u=int(r.nnz_u),
                  nnz_l=int(r.nnz_l), n_supernodes=int(r.n_supernodes),
                  edges_inspected=int(r.edges_inspected), sources=int(r.sources),
-                 x_total=int(r.x_total), e_insp=int(r.e_insp), kernel_ms=float(r.kernel_ms))
+                 x_total=int(r.x_total), e_insp=int(r.e_insp), kernel_ms=float(r.kernel_ms),
+                 levels=int(r.levels), reused_sources=int(r.reused_sources),
+                 cycles=tuple(int(c) for c in r.cycles), ctas=int(r.ctas))
     out.u_row_count = _arr(r.u_row_count, n, np.int32)
     out.l_col_count = _arr(r.l_col_count, n, np.int32)
     out.l_row_count = _arr(r.l_row_count, n, np.int32)

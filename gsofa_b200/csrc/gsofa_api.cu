@@ -296,8 +296,8 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         char *d_misc = (char *)ctx->grow(ctx->misc, 256);
         unsigned long long *d_piece = (unsigned long long *)d_misc;
         unsigned long long *d_tail = (unsigned long long *)(d_misc + 8);
-        unsigned long long *d_counters = (unsigned long long *)(d_misc + 16);
-        uint32_t *d_status = (uint32_t *)(d_misc + 64);
+        unsigned long long *d_counters = (unsigned long long *)(d_misc + 16);   // 12 counters
+        uint32_t *d_status = (uint32_t *)(d_misc + 128);
         int32_t *d_pool = nullptr, *d_out = nullptr;
         if (want_pattern) {
             d_pool = (int32_t *)ctx->grow(ctx->pool, (size_t)pool_cap * sizeof(int32_t));
@@ -357,17 +357,18 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         GS_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(block), args, smem, st));
         GS_CUDA(cudaEventRecord(ctx->ev1, st));
 
-        unsigned long long h_misc[9];
-        GS_CUDA(cudaMemcpyAsync(h_misc, d_misc, 72, cudaMemcpyDeviceToHost, st));
+        unsigned long long h_misc[17];
+        GS_CUDA(cudaMemcpyAsync(h_misc, d_misc, 136, cudaMemcpyDeviceToHost, st));
         int64_t tot[2];
         GS_CUDA(cudaMemcpyAsync(&tot[0], d_gptr + L, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
         GS_CUDA(cudaMemcpyAsync(&tot[1], d_gptr + (L + 1) + L, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
         GS_CUDA(cudaStreamSynchronize(st));
         float ms = 0.f;
         GS_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-        const uint32_t status = (uint32_t)(h_misc[8] & 0xffffffffu);
+        const uint32_t status = (uint32_t)(h_misc[16] & 0xffffffffu);
         const unsigned long long edges = h_misc[2], nsrc = h_misc[3], nsn = h_misc[4];
         const unsigned long long xtot = h_misc[5], einsp = h_misc[6];
+        const unsigned long long levels = h_misc[7], reused = h_misc[8];
 
         if (status & ERR_QUEUE_OVERFLOW) return GSOFA_ERR_QUEUE_OVERFLOW;
         if (want_pattern && (status & ERR_POOL_OVERFLOW)) {
@@ -401,6 +402,10 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
             r.sources = nsrc;
             r.x_total = xtot;
             r.e_insp = einsp;
+            r.levels = levels;
+            r.reused_sources = reused;
+            for (int q = 0; q < 3; q++) r.cycles[q] = h_misc[9 + q];
+            r.ctas = (uint64_t)grid;
             if (part_count == 1) {
                 r.fill_count = r.nnz_u - mats[i]->orig_up + r.nnz_l - mats[i]->orig_lo;
                 const_cast<gsofa_matrix *>(mats[i])->last_pattern_total = (int64_t)(r.nnz_u + r.nnz_l);

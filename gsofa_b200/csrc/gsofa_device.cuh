@@ -91,7 +91,9 @@ struct JobArgs {
     int64_t *tile_last;        // [ntiles] last supernode-run start, then prefix max
     int64_t *tile_sn;          // [ntiles] then exclusive prefix
     unsigned long long *counters; // [0] edges inspected, [1] sources, [2] sn total,
-                                  // [3] pass-G expansions, [4] pass-G input degrees
+                                  // [3] pass-G expansions, [4] pass-G input degrees,
+                                  // [5] levels, [6] sources that reused state,
+                                  // [7..9] cycles: expansion, output, clearing
     uint32_t *status;
 };
 
@@ -287,7 +289,8 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                                int64_t line, int pass, int32_t s, uint32_t *bm,
                                const Frontier &f, SharedState &sh,
                                unsigned long long &edges, const int32_t *rawdeg,
-                               unsigned long long &xcnt, unsigned long long &einsp)
+                               unsigned long long &xcnt, unsigned long long &einsp,
+                               unsigned long long *prof)
 {
     const int tid = threadIdx.x;
     const int lane = tid & 31;
@@ -295,7 +298,9 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
     const int lane_in_group = tid & (lanes - 1);
     int t_lo = INT32_MAX, t_hi = -1;
 
+    long long c0 = 0;
     if (tid == 0) {
+        c0 = clock64();
         sh.tailc[0] = sh.tailc[1] = sh.tailc[2] = 0;
         sh.fetch[0] = sh.fetch[1] = sh.fetch[2] = 0;
         if (test_and_set(bm, s)) { t_lo = s; t_hi = s; }
@@ -319,7 +324,10 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
     for (int L = 0;; L++) {
         __syncthreads();
         const int end = start + sh.tailc[L % 3];
-        if (end == start) break;
+        if (end == start) {
+            if (tid == 0) prof[0] += (unsigned long long)L;
+            break;
+        }
         if (tid == 0) { sh.tailc[(L + 2) % 3] = 0; sh.fetch[(L + 1) % 3] = 0; }
         int *tailp = &sh.tailc[(L + 1) % 3];
         int *fetchp = &sh.fetch[L % 3];
@@ -395,6 +403,8 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         __syncthreads();
     }
     const int chain_hi = sh.chain_hi;
+    long long c1 = 0;
+    if (tid == 0) { c1 = clock64(); prof[1] += (unsigned long long)(c1 - c0); }
 
     // hi(s) = set bits in (s, chain_hi]; each thread owns a contiguous span of
     // words, one block scan gives every span its output offset
@@ -446,6 +456,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         }
     }
     __syncthreads();
+    if (tid == 0) prof[2] += (unsigned long long)(clock64() - c1);
 }
 #undef GSOFA_VISIT
 
@@ -465,7 +476,8 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
     for (int w = tid; w < a.bitmap_words; w += BLOCK) bm[w] = 0u;
     if (tid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
     const Frontier fr{ring, a.queue + (int64_t)blockIdx.x * a.qcap, a.qcap, a.status, a.ring_size};
-    unsigned long long edges = 0, nsrc = 0, xcnt = 0, einsp = 0;
+    unsigned long long edges = 0, nsrc = 0, xcnt = 0, einsp = 0, nreuse = 0;
+    unsigned long long prof[4] = {0, 0, 0, 0};  // levels, expansion, output, clearing cycles
     __syncthreads();
     for (;;) {
         if (tid == 0) sh.piece = (long long)atomicAdd(a.piece_counter, 1ull);
@@ -514,13 +526,19 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
                 reuse = sh.flag;
             }
             if (!reuse) {
+                const long long cc = clock64();
                 const int clo = sh.chain_lo, chi = sh.chain_hi;
                 clear_range<BLOCK>(bm, clo, chi);
                 __syncthreads();
-                if (tid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
+                if (tid == 0) {
+                    sh.chain_lo = INT32_MAX; sh.chain_hi = -1;
+                    prof[3] += (unsigned long long)(clock64() - cc);
+                }
+            } else {
+                nreuse++;
             }
             process_source<BLOCK>(a, g, md.n, md.line_base + s, pass, s, bm, fr, sh, edges,
-                                  md.rawdeg, xcnt, einsp);
+                                  md.rawdeg, xcnt, einsp, prof);
             prev = s;
             nsrc++;
         }
@@ -542,6 +560,11 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
             atomicAdd(&a.counters[1], nsrc);
             atomicAdd(&a.counters[3], (unsigned long long)x);
             atomicAdd(&a.counters[4], (unsigned long long)ei);
+            atomicAdd(&a.counters[5], prof[0]);
+            atomicAdd(&a.counters[6], nreuse);
+            atomicAdd(&a.counters[7], prof[1]);
+            atomicAdd(&a.counters[8], prof[2]);
+            atomicAdd(&a.counters[9], prof[3]);
         }
     }
     grid.sync();

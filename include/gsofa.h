@@ -102,6 +102,11 @@ typedef struct gsofa_result {
                                 the vertices expanded, sum deg(s) + sum over
                                 X(s) of deg(v) (input degrees, diagonal and
                                 duplicates included)                      */
+    uint64_t levels;         /* frontier levels summed over the traversals  */
+    uint64_t reused_sources; /* traversals that started from s-1's state    */
+    uint64_t cycles[3];      /* SM cycles summed over CTAs: expansion,
+                                output (count + pattern), bitmap clearing  */
+    uint64_t ctas;           /* CTAs of the persistent launch               */
     double kernel_ms;        /* factorization kernel time on the device     */
     /* per-line arrays (host, library-owned; NULL with NO_DOWNLOAD) */
     int32_t *u_row_count;    /* [n] |U row s|                               */
