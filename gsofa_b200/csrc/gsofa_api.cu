@@ -221,15 +221,20 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     const int32_t bitmap_words = ((max_n + 31) / 32 + 3) / 4 * 4;
     const size_t static_smem = sizeof(SharedState) + 1024;
     if ((size_t)bitmap_words * 4 + 1024 * 4 + static_smem > ctx->smem_optin) return GSOFA_ERR_UNSUPPORTED;
-    // frontier ring: 8K entries when they fit beside the bitmap, else smaller
-    int ring = 8192;
-    while (ring > 1024 && (size_t)bitmap_words * 4 + (size_t)ring * 4 + static_smem > ctx->smem_optin)
-        ring >>= 1;
-    const size_t smem = (size_t)bitmap_words * 4 + (size_t)ring * 4;
-    GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int occ = 0;
-    GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, block, smem));
+    // frontier ring: the largest of 8K/4K/2K/1K entries that keeps the most
+    // CTAs (each with its own bitmap) resident on an SM
+    int ring = 0, occ = 0;
+    size_t smem = 0;
+    for (int cand = 8192; cand >= 1024; cand >>= 1) {
+        const size_t sm = (size_t)bitmap_words * 4 + (size_t)cand * 4;
+        if (sm + static_smem > ctx->smem_optin) continue;
+        GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        int o = 0;
+        GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kfn, block, sm));
+        if (o > occ) { occ = o; ring = cand; smem = sm; }
+    }
     if (occ <= 0) return GSOFA_ERR_UNSUPPORTED;
+    GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = p.ctas_per_sm > 0 ? std::min(p.ctas_per_sm, occ) : occ;
     const int grid = per_sm * ctx->sm_count;
 

@@ -332,40 +332,59 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         int *tailp = &sh.tailc[(L + 1) % 3];
         int *fetchp = &sh.fetch[L % 3];
         if (lanes == 1) {
-            // One thread per vertex: a warp takes 32 items with one shared
-            // atomic; every lane loads its row bounds and up to eight ids
-            // before touching the bitmap.  Rows longer than HEAVY_ROW are
-            // expanded by the whole warp.
+            // Edge-balanced warps: a warp takes 32 queue items with one shared
+            // atomic, scans their degrees, and walks the flattened edge list 32
+            // edges per round; lane j finds the item owning flat edge r + j
+            // with a 5-step shuffle search.  Lanes of one item read
+            // consecutive ids (coalesced), and every round keeps all lanes
+            // busy whatever the degree mix.  New vertices below s are
+            // enqueued with one ballot and one shared atomic per round.
             for (;;) {
                 int base = 0;
                 if (lane == 0) base = atomicAdd(fetchp, 32);
                 base = __shfl_sync(0xffffffffu, base, 0) + start;
                 if (base >= end) break;
                 const int it = base + lane;
-                int32_t b = 0, e = 0;
+                int32_t b = 0, d = 0;
                 if (it < end) {
                     const int32_t v = fr_get(f, it, wstart);
                     b = g.ptr[v];
-                    e = g.ptr[v + 1];
-                    edges += (unsigned long long)(e - b);
+                    d = g.ptr[v + 1] - b;
+                    edges += (unsigned long long)d;
                     if (pass == 0) { xcnt++; einsp += (unsigned long long)rawdeg[v]; }
                 }
-                unsigned heavy = __ballot_sync(0xffffffffu, e - b > HEAVY_ROW);
-                while (heavy) {
-                    const int src = __ffs(heavy) - 1;
-                    heavy &= heavy - 1u;
-                    const int32_t hb = __shfl_sync(0xffffffffu, b, src);
-                    const int32_t he = __shfl_sync(0xffffffffu, e, src);
-                    for (int32_t k = hb + lane; k < he; k += 32) GSOFA_VISIT(g.adj[k]);
+                int incl = d;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
                 }
-                if (e - b <= HEAVY_ROW) {
-                    for (int32_t k0 = b; k0 < e; k0 += 8) {
-                        int32_t buf[8];
+                const int total = __shfl_sync(0xffffffffu, incl, 31);
+                const int excl = incl - d;
+                for (int r0 = 0; r0 < total; r0 += 32) {
+                    const int pos = r0 + lane;
+                    int item = 0;
 #pragma unroll
-                        for (int u = 0; u < 8; u++) buf[u] = (k0 + u < e) ? g.adj[k0 + u] : -1;
-#pragma unroll
-                        for (int u = 0; u < 8; u++)
-                            if (buf[u] >= 0) GSOFA_VISIT(buf[u]);
+                    for (int step = 16; step; step >>= 1) {
+                        const int ex = __shfl_sync(0xffffffffu, excl, item + step);
+                        if (ex <= pos) item += step;
+                    }
+                    const int32_t ib = __shfl_sync(0xffffffffu, b, item);
+                    const int iex = __shfl_sync(0xffffffffu, excl, item);
+                    bool fresh = false;
+                    int32_t m = 0;
+                    if (pos < total) {
+                        m = g.adj[ib + (pos - iex)];
+                        fresh = test_and_set(bm, m);
+                        if (fresh) { t_lo = min(t_lo, m); t_hi = max(t_hi, m); }
+                    }
+                    const bool low = fresh && m < s;
+                    const unsigned bal = __ballot_sync(0xffffffffu, low);
+                    if (bal) {
+                        int pb = 0;
+                        if (lane == 0) pb = atomicAdd(tailp, __popc(bal));
+                        pb = __shfl_sync(0xffffffffu, pb, 0);
+                        if (low) fr_put(f, end + pb + __popc(bal & ((1u << lane) - 1u)), start, m);
                     }
                 }
             }
@@ -406,23 +425,40 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
     long long c1 = 0;
     if (tid == 0) { c1 = clock64(); prof[1] += (unsigned long long)(c1 - c0); }
 
-    // hi(s) = set bits in (s, chain_hi]; each thread owns a contiguous span of
-    // words, one block scan gives every span its output offset
+    // hi(s) = set bits in (s, chain_hi].  Each warp owns a run of 32-word
+    // chunks: it counts them, one cross-warp prefix gives its output offset,
+    // then per chunk a warp scan places every lane's bits in sorted order.
+    constexpr int NWARP = BLOCK / 32;
+    const int wid = tid >> 5;
     const int w0 = (s + 1) >> 5;
     const int w1 = (chain_hi > s) ? (chain_hi >> 5) : (w0 - 1);
-    const int nw = w1 - w0 + 1;
-    const int per = nw > 0 ? (nw + BLOCK - 1) / BLOCK : 0;
-    const int my0 = w0 + tid * per;
-    const int my1 = min(my0 + per, w1 + 1);
+    const int nchunks = (w1 - w0 + 1 + 31) >> 5;      // <= 0 when empty
+    const int per = nchunks > 0 ? (nchunks + NWARP - 1) / NWARP : 0;
+    const int ch0 = wid * per;
+    const int ch1 = min(ch0 + per, max(nchunks, 0));
     const uint32_t first_mask = ~0u << ((s + 1) & 31);
-    int64_t count = 0;
-    for (int w = my0; w < my1; w++) {
-        uint32_t x = bm[w];
+    int wcount = 0;
+    for (int c = ch0; c < ch1; c++) {
+        const int w = w0 + (c << 5) + lane;
+        uint32_t x = (w <= w1) ? bm[w] : 0u;
         if (w == w0) x &= first_mask;
-        count += __popc(x);
+        wcount += __popc(x);
     }
-    int64_t total;
-    const int64_t off = block_excl_scan<BLOCK>(count, &total, sh.warp);
+    wcount = __reduce_add_sync(0xffffffffu, wcount);
+    if (lane == 0) sh.warp[wid] = wcount;
+    __syncthreads();
+    int64_t wpre = 0, total = 0;
+    {
+        const int64_t v = lane < NWARP ? sh.warp[lane] : 0;
+        int64_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        total = __shfl_sync(0xffffffffu, x, 31);
+        wpre = __shfl_sync(0xffffffffu, x - v, wid);
+    }
 
     const int64_t slot = (int64_t)pass * a.L + line;
     if (tid == 0) {
@@ -442,16 +478,26 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
     if (a.want_pattern) {
         __syncthreads();
         const int64_t base = sh.pool_base;
-        if (base >= 0 && count > 0) {
-            int32_t *dst = a.pool + base + off;
-            for (int w = my0; w < my1; w++) {
-                uint32_t x = bm[w];
+        if (base >= 0 && wcount > 0) {
+            int64_t run = base + wpre;
+            for (int c = ch0; c < ch1; c++) {
+                const int w = w0 + (c << 5) + lane;
+                uint32_t x = (w <= w1) ? bm[w] : 0u;
                 if (w == w0) x &= first_mask;
+                const int pc = __popc(x);
+                int incl = pc;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                int32_t *dst = a.pool + run + (incl - pc);
                 while (x) {
                     const int bit = __ffs(x) - 1;
                     x &= x - 1u;
                     *dst++ = (w << 5) + bit;
                 }
+                run += __shfl_sync(0xffffffffu, incl, 31);
             }
         }
     }
