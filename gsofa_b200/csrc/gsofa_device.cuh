@@ -332,13 +332,13 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         int *tailp = &sh.tailc[(L + 1) % 3];
         int *fetchp = &sh.fetch[L % 3];
         if (lanes == 1) {
-            // Edge-balanced warps: a warp takes 32 queue items with one shared
-            // atomic, scans their degrees, and walks the flattened edge list 32
-            // edges per round; lane j finds the item owning flat edge r + j
-            // with a 5-step shuffle search.  Lanes of one item read
-            // consecutive ids (coalesced), and every round keeps all lanes
-            // busy whatever the degree mix.  New vertices below s are
-            // enqueued with one ballot and one shared atomic per round.
+            // One thread per vertex: a warp takes 32 queue items with one
+            // shared atomic; each lane loads its row bounds and then up to
+            // eight adjacency ids at once (independent loads in flight hide
+            // the L2 latency).  The id loop runs to the warp's longest light
+            // row so every step is warp-uniform and new vertices below s are
+            // enqueued with one ballot and one shared atomic.  Rows longer
+            // than HEAVY_ROW are expanded by the whole warp.
             for (;;) {
                 int base = 0;
                 if (lane == 0) base = atomicAdd(fetchp, 32);
@@ -353,38 +353,46 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                     edges += (unsigned long long)d;
                     if (pass == 0) { xcnt++; einsp += (unsigned long long)rawdeg[v]; }
                 }
-                int incl = d;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += y;
-                }
-                const int total = __shfl_sync(0xffffffffu, incl, 31);
-                const int excl = incl - d;
-                for (int r0 = 0; r0 < total; r0 += 32) {
-                    const int pos = r0 + lane;
-                    int item = 0;
-#pragma unroll
-                    for (int step = 16; step; step >>= 1) {
-                        const int ex = __shfl_sync(0xffffffffu, excl, item + step);
-                        if (ex <= pos) item += step;
-                    }
-                    const int32_t ib = __shfl_sync(0xffffffffu, b, item);
-                    const int iex = __shfl_sync(0xffffffffu, excl, item);
-                    bool fresh = false;
-                    int32_t m = 0;
-                    if (pos < total) {
-                        m = g.adj[ib + (pos - iex)];
-                        fresh = test_and_set(bm, m);
+                unsigned heavy = __ballot_sync(0xffffffffu, d > HEAVY_ROW);
+                while (heavy) {
+                    const int src = __ffs(heavy) - 1;
+                    heavy &= heavy - 1u;
+                    const int32_t hb = __shfl_sync(0xffffffffu, b, src);
+                    const int32_t hd = __shfl_sync(0xffffffffu, d, src);
+                    for (int32_t k0 = 0; k0 < hd; k0 += 32) {
+                        const bool on = k0 + lane < hd;
+                        const int32_t m = on ? g.adj[hb + k0 + lane] : 0;
+                        const bool fresh = on && test_and_set(bm, m);
                         if (fresh) { t_lo = min(t_lo, m); t_hi = max(t_hi, m); }
+                        const bool low = fresh && m < s;
+                        const unsigned bal = __ballot_sync(0xffffffffu, low);
+                        if (bal) {
+                            int pb = 0;
+                            if (lane == 0) pb = atomicAdd(tailp, __popc(bal));
+                            pb = __shfl_sync(0xffffffffu, pb, 0);
+                            if (low) fr_put(f, end + pb + __popc(bal & ((1u << lane) - 1u)), start, m);
+                        }
                     }
-                    const bool low = fresh && m < s;
-                    const unsigned bal = __ballot_sync(0xffffffffu, low);
-                    if (bal) {
-                        int pb = 0;
-                        if (lane == 0) pb = atomicAdd(tailp, __popc(bal));
-                        pb = __shfl_sync(0xffffffffu, pb, 0);
-                        if (low) fr_put(f, end + pb + __popc(bal & ((1u << lane) - 1u)), start, m);
+                }
+                const int dl = d > HEAVY_ROW ? 0 : d;
+                const int dmax = __reduce_max_sync(0xffffffffu, dl);
+                for (int k0 = 0; k0 < dmax; k0 += 8) {
+                    int32_t buf[8];
+#pragma unroll
+                    for (int u = 0; u < 8; u++) buf[u] = (k0 + u < dl) ? g.adj[b + k0 + u] : -1;
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        const int32_t m = buf[u];
+                        const bool fresh = m >= 0 && test_and_set(bm, m);
+                        if (fresh) { t_lo = min(t_lo, m); t_hi = max(t_hi, m); }
+                        const bool low = fresh && m < s;
+                        const unsigned bal = __ballot_sync(0xffffffffu, low);
+                        if (bal) {
+                            int pb = 0;
+                            if (lane == 0) pb = atomicAdd(tailp, __popc(bal));
+                            pb = __shfl_sync(0xffffffffu, pb, 0);
+                            if (low) fr_put(f, end + pb + __popc(bal & ((1u << lane) - 1u)), start, m);
+                        }
                     }
                 }
             }
