@@ -320,7 +320,7 @@ class Context:
         _check(lib().gsofa_symbfact(self._h, m.handle, ctypes.byref(p), ctypes.byref(r)), "gsofa_symbfact")
         try:
             res = _convert(r)
-            need = {"u_row_count": r.n, "l_col_count": r.n, "l_row_count": r.n,
+            need = {"u_row_count": r.n, "l_col_count": r.n, "l_row_count": r.n if p.want_pattern else 0,
                     "sn_start": r.n_supernodes, "u_ptr": r.n + 1, "l_ptr": r.n + 1,
                     "u_idx": r.nnz_u if p.want_pattern else 0, "l_idx": r.nnz_l if p.want_pattern else 0}
             ptrs = {}

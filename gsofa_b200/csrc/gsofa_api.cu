@@ -418,7 +418,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
             if (download_lines) {
                 r.u_row_count = download(st, d_cnt, lb, n);
                 r.l_col_count = download(st, d_cnt, L + lb, n);
-                r.l_row_count = download(st, d_lrow, lb, n);
+                if (want_pattern) r.l_row_count = download(st, d_lrow, lb, n);
             }
             if (want_pattern && download_lines) {
                 r.u_ptr = download(st, d_gptr, lb, n + 1);
@@ -808,6 +808,7 @@ gsofa_status gsofa_result_fetch(gsofa_ctx *c, const gsofa_result *r, int32_t *u_
         };
         cp(u_row_count, cnt + lb, (size_t)n * 4);
         cp(l_col_count, cnt + L + lb, (size_t)n * 4);
+        if (l_row_count && !outb) return GSOFA_ERR_INVALID_INPUT;   // counted with the pattern only
         cp(l_row_count, (const int32_t *)c->lrow.p + lb, (size_t)n * 4);
         if ((u_ptr || u_idx || l_ptr || l_idx) && !outb) return GSOFA_ERR_INVALID_INPUT;
         cp(u_ptr, gptr + lb, (size_t)(n + 1) * 8);

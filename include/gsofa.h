@@ -111,7 +111,7 @@ typedef struct gsofa_result {
     /* per-line arrays (host, library-owned; NULL with NO_DOWNLOAD) */
     int32_t *u_row_count;    /* [n] |U row s|                               */
     int32_t *l_col_count;    /* [n] |L column j|                            */
-    int32_t *l_row_count;    /* [n] |L row s|                               */
+    int32_t *l_row_count;    /* [n] |L row s| (with want_pattern only)      */
     int32_t *sn_start;       /* [n_supernodes] first line of each supernode */
     /* pattern (host, library-owned; NULL unless want_pattern) */
     int64_t *u_ptr;          /* [n+1] */
