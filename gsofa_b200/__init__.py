@@ -188,6 +188,10 @@ def lib():
     L.gsofa_result_fetch.argtypes = [vp, ctypes.POINTER(_CResult), _i32p, _i32p, _i32p, _i32p,
                                      _i64p, _i32p, _i64p, _i32p]
     L.gsofa_result_fetch.restype = ctypes.c_int
+    L.gsofa_symbfact_counts_noalloc.argtypes = [ctypes.c_int, vp, ctypes.c_int32, ctypes.c_int64,
+                                                vp, vp, vp, ctypes.c_int32, vp, vp, vp,
+                                                ctypes.POINTER(ctypes.c_uint64)]
+    L.gsofa_symbfact_counts_noalloc.restype = ctypes.c_int
     L.gsofa_predict_scratch_bytes.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(Params)]
     L.gsofa_predict_scratch_bytes.restype = ctypes.c_size_t
     L.gsofa_symbfact_min_id.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.c_int,
@@ -386,9 +390,38 @@ def symbfact_min_id(argv: Sequence[str], myrank: int = 0):
     return int(fc.value), float(t.value)
 
 
+NOALLOC_MAX_N = 16384
+NOALLOC_MAX_NNZ = 262144
+
+
+def symbfact_counts_noalloc(device: int, stream: int, n: int, nnz: int, d_beg: int, d_end: int,
+                            d_adj: int, d_u_row_count: int, d_l_col_count: int, d_sn_start: int,
+                            max_supernode_size: int = 0):
+    """Counts-only factorization that allocates no device memory.
+
+    For callers that cannot call cudaMalloc (code living under a host
+    framework's own device allocator or memory budget, or on a path where
+    cudaMalloc's implicit synchronisation is not allowed).  All arguments are
+    raw device addresses (ints) of buffers the caller owns: the
+    colbeg/colend/csr triple and outputs of n int32 each.  Scratch comes from
+    a static device array inside the library (n <= NOALLOC_MAX_N,
+    nnz <= NOALLOC_MAX_NNZ).  Returns (fill_count, nnz_lu, n_supernodes);
+    the first n_supernodes entries of the sn_start buffer are the supernode
+    starts.  Calls on one device share the scratch, so issue them one at a
+    time."""
+    summary = (ctypes.c_uint64 * 3)()
+    vp = ctypes.c_void_p
+    _check(lib().gsofa_symbfact_counts_noalloc(int(device), vp(int(stream) or None), int(n), int(nnz),
+                                               vp(d_beg), vp(d_end), vp(d_adj), int(max_supernode_size),
+                                               vp(d_u_row_count), vp(d_l_col_count), vp(d_sn_start),
+                                               summary), "gsofa_symbfact_counts_noalloc")
+    return int(summary[0]), int(summary[1]), int(summary[2])
+
+
 def exported_symbols() -> List[str]:
     """Names of the C ABI entry points declared in include/gsofa.h."""
     return ["gsofa_symbfact_min_id", "gsofa_status_str", "gsofa_abi_version", "gsofa_default_params",
             "gsofa_create", "gsofa_destroy", "gsofa_set_stream", "gsofa_read_text", "gsofa_free", "gsofa_upload",
             "gsofa_matrix_free", "gsofa_matrix_n", "gsofa_symbfact", "gsofa_symbfact_batch",
-            "gsofa_result_free", "gsofa_result_fetch", "gsofa_predict_scratch_bytes"]
+            "gsofa_result_free", "gsofa_result_fetch", "gsofa_predict_scratch_bytes",
+            "gsofa_symbfact_counts_noalloc"]

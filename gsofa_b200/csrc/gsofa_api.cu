@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -909,3 +910,229 @@ gsofa_status gsofa_symbfact_min_id(int argc, char **argv, int myrank, uint64_t *
 }
 
 }  // extern "C"
+
+// ============================================================================
+// Factorization without device allocation (gsofa_symbfact_counts_noalloc).
+//
+// Every intermediate array of the counts-only factorization sits in one
+// file-scope static device array.  Host code cannot use the array's name as a
+// device address, so the address is looked up once per device with
+// cudaGetSymbolAddress while that device is current.
+
+namespace {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[GSOFA_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_base[kNoallocMaxDevices];
+int g_noalloc_sms[kNoallocMaxDevices];
+size_t g_noalloc_smem[kNoallocMaxDevices];
+
+// Carves the static array for an n-line, nnz-entry input: sequential,
+// 256-byte aligned slices.
+struct NoallocLayout {
+    size_t off = 0;
+    char *base = nullptr;
+    size_t limit = 0;
+    bool ok = true;
+    template <class T>
+    T *take(size_t count)
+    {
+        off = (off + 255) / 256 * 256;
+        T *p = (T *)(base + off);
+        off += std::max<size_t>(count, 1) * sizeof(T);
+        if (off > limit) ok = false;
+        return p;
+    }
+};
+
+}  // namespace
+
+extern "C" gsofa_status gsofa_symbfact_counts_noalloc(int device, void *cuda_stream, int32_t n,
+                                                      int64_t nnz, const int32_t *d_beg,
+                                                      const int32_t *d_end, const int32_t *d_adj,
+                                                      int32_t max_supernode_size,
+                                                      int32_t *d_u_row_count,
+                                                      int32_t *d_l_col_count,
+                                                      int32_t *d_sn_start, uint64_t *summary)
+{
+    if (n < 0 || nnz < 0 || !summary) return GSOFA_ERR_INVALID_INPUT;
+    if (n > GSOFA_NOALLOC_MAX_N || nnz > GSOFA_NOALLOC_MAX_NNZ) return GSOFA_ERR_UNSUPPORTED;
+    if (n > 0 && (!d_beg || !d_end || !d_u_row_count || !d_l_col_count || !d_sn_start))
+        return GSOFA_ERR_INVALID_INPUT;
+    if (nnz > 0 && !d_adj) return GSOFA_ERR_INVALID_INPUT;
+    if (device < 0 || device >= kNoallocMaxDevices) return GSOFA_ERR_INVALID_INPUT;
+    summary[0] = summary[1] = summary[2] = 0;
+    if (n == 0) return GSOFA_OK;
+    try {
+        GS_CUDA(cudaSetDevice(device));
+        {
+            std::lock_guard<std::mutex> lk(g_noalloc_mu);
+            if (!g_noalloc_base[device]) {
+                void *p = nullptr;
+                GS_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+                cudaDeviceProp prop;
+                GS_CUDA(cudaGetDeviceProperties(&prop, device));
+                if (prop.major < 10 || !prop.cooperativeLaunch) return GSOFA_ERR_UNSUPPORTED;
+                g_noalloc_sms[device] = prop.multiProcessorCount;
+                g_noalloc_smem[device] = prop.sharedMemPerBlockOptin;
+                g_noalloc_base[device] = p;
+            }
+        }
+        cudaStream_t st = (cudaStream_t)cuda_stream;
+        const int sms = g_noalloc_sms[device];
+
+        // launch shape: 256 threads, one CTA per SM (its queue slice is n ints)
+        constexpr int BLOCK = 256;
+        void *kfn = factor_kernel_for(BLOCK);
+        const int32_t bitmap_words = ((n + 31) / 32 + 3) / 4 * 4;
+        const int ring = 4096;
+        const size_t smem = (size_t)bitmap_words * 4 + (size_t)ring * 4;
+        GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int occ = 0;
+        GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, BLOCK, smem));
+        if (occ <= 0) return GSOFA_ERR_UNSUPPORTED;
+        const int grid = sms;
+        const int64_t L = n;
+        const int64_t ntiles = (L + TILE - 1) / TILE;
+        const int64_t scan_tiles = ((int64_t)n + 1 + 255) / 256 + 1;
+
+        NoallocLayout lay;
+        lay.base = (char *)g_noalloc_base[device];
+        lay.limit = GSOFA_NOALLOC_SCRATCH_BYTES;
+        int32_t *gptr_g = lay.take<int32_t>(n + 1);
+        int32_t *gadj = lay.take<int32_t>((size_t)nnz);
+        int32_t *tptr = lay.take<int32_t>(n + 1);
+        int32_t *tadj = lay.take<int32_t>((size_t)nnz);
+        int32_t *deg = lay.take<int32_t>(n + 1);
+        int32_t *indeg = lay.take<int32_t>(n + 1);
+        int32_t *tcur = lay.take<int32_t>(n + 1);
+        int32_t *orig_up = lay.take<int32_t>(n);
+        int32_t *orig_lo = lay.take<int32_t>(n);
+        int32_t *rawdeg = lay.take<int32_t>(n);
+        int64_t *tsum = lay.take<int64_t>(2 * scan_tiles);
+        unsigned long long *ucounts = lay.take<unsigned long long>(8);
+        int32_t *cnt = lay.take<int32_t>(2 * L);
+        uint8_t *nxt = lay.take<uint8_t>(2 * L);
+        int64_t *gp = lay.take<int64_t>(2 * (L + 1));
+        int32_t *lrow = lay.take<int32_t>(L);
+        uint8_t *snind = lay.take<uint8_t>(L);
+        int64_t *tiles = lay.take<int64_t>(4 * ntiles);
+        char *misc = lay.take<char>(256);
+        MatDesc *dmat = lay.take<MatDesc>(1);
+        Range *drange = lay.take<Range>(1);
+        int32_t *queue = lay.take<int32_t>((size_t)grid * n);
+        if (!lay.ok) return GSOFA_ERR_UNSUPPORTED;
+
+        // ---- graph build (validation, G without diagonal/duplicates, G^T) ----
+        GS_CUDA(cudaMemsetAsync(indeg, 0, (size_t)(n + 1) * 4, st));
+        GS_CUDA(cudaMemsetAsync(deg, 0, (size_t)(n + 1) * 4, st));
+        GS_CUDA(cudaMemsetAsync(orig_lo, 0, (size_t)n * 4, st));
+        GS_CUDA(cudaMemsetAsync(ucounts, 0, 64, st));
+        UploadArgs u{};
+        u.n = n;
+        u.nnz = nnz;
+        u.beg = d_beg;
+        u.end = d_end;
+        u.adj = d_adj;
+        u.deg = deg;
+        u.indeg = indeg;
+        u.orig_up = orig_up;
+        u.orig_lo = orig_lo;
+        u.rawdeg = rawdeg;
+        u.counts = ucounts;
+        u.status = (uint32_t *)(ucounts + 4);
+        const int ugrid = (int)std::min<int64_t>(((int64_t)n * 32 + 255) / 256, (int64_t)sms * 16);
+        upload_count_kernel<<<ugrid, 256, 0, st>>>(u);
+        GS_CUDA(cudaGetLastError());
+        const int64_t ntl = ((int64_t)n + 255) / 256;
+        int32_t *scan_in[2] = {deg, indeg};
+        int32_t *scan_out[2] = {gptr_g, tptr};
+        for (int k = 0; k < 2; k++) {
+            int64_t *ts = tsum + k * scan_tiles;
+            int64_t *dt = (int64_t *)(ucounts + 2 + k);
+            scan_tiles_kernel<256><<<(unsigned)ntl, 256, 0, st>>>(scan_in[k], n, ts);
+            scan_partials_kernel<256><<<1, 256, 0, st>>>(ts, ntl, dt);
+            scan_apply_kernel<256><<<(unsigned)ntl, 256, 0, st>>>(scan_in[k], n, ts, scan_out[k], dt);
+            GS_CUDA(cudaGetLastError());
+        }
+        unsigned long long hc[5];
+        GS_CUDA(cudaMemcpyAsync(hc, ucounts, sizeof(hc), cudaMemcpyDeviceToHost, st));
+        GS_CUDA(cudaStreamSynchronize(st));
+        if ((uint32_t)(hc[4] & 0xffffffffu) & 1u) return GSOFA_ERR_INVALID_INPUT;
+        if ((int64_t)hc[2] > nnz || (int64_t)hc[3] > nnz) return GSOFA_ERR_INVALID_INPUT;
+        GS_CUDA(cudaMemcpyAsync(tcur, tptr, (size_t)(n + 1) * 4, cudaMemcpyDeviceToDevice, st));
+        upload_fill_kernel<<<ugrid, 256, 0, st>>>(u, gptr_g, gadj, tcur, tadj);
+        GS_CUDA(cudaGetLastError());
+
+        // ---- factorization (counts only) ----
+        MatDesc md{};
+        md.n = n;
+        md.line_base = 0;
+        md.g[0] = PassGraph{gptr_g, gadj};
+        md.g[1] = PassGraph{tptr, tadj};
+        md.rawdeg = rawdeg;
+        Range rg{};
+        rg.mat = 0;
+        rg.chunk = 32;
+        rg.nj = n;
+        rg.stride = 1;
+        rg.offset = 0;
+        rg.piece_base = 0;
+        rg.npieces = 2 * (((int64_t)n + 31) / 32);
+        GS_CUDA(cudaMemcpyAsync(dmat, &md, sizeof(md), cudaMemcpyHostToDevice, st));
+        GS_CUDA(cudaMemcpyAsync(drange, &rg, sizeof(rg), cudaMemcpyHostToDevice, st));
+        GS_CUDA(cudaMemsetAsync(misc, 0, 256, st));
+        JobArgs a{};
+        a.mats = dmat;
+        a.nmats = 1;
+        a.nranges = 1;
+        a.ranges = drange;
+        a.npieces = rg.npieces;
+        a.piece_counter = (unsigned long long *)misc;
+        a.queue = queue;
+        a.qcap = n;
+        a.bitmap_words = bitmap_words;
+        a.ring_size = ring;
+        a.lanes = 1;
+        a.reuse = 1;
+        a.want_pattern = 0;
+        a.max_sn = max_supernode_size;
+        a.L = L;
+        a.cnt = cnt;
+        a.nxt = nxt;
+        a.poff = nullptr;
+        a.pool = nullptr;
+        a.pool_cap = 0;
+        a.pool_tail = (unsigned long long *)(misc + 8);
+        a.gptr = gp;
+        a.out = nullptr;
+        a.lrow = lrow;
+        a.snind = snind;
+        a.sn_list = d_sn_start;
+        a.ntiles = ntiles;
+        a.tile_sum = tiles;
+        a.tile_last = tiles + 2 * ntiles;
+        a.tile_sn = tiles + 3 * ntiles;
+        a.counters = (unsigned long long *)(misc + 16);
+        a.status = (uint32_t *)(misc + 128);
+        void *args[] = {&a};
+        GS_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(BLOCK), args, smem, st));
+        GS_CUDA(cudaMemcpyAsync(d_u_row_count, cnt, (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
+        GS_CUDA(cudaMemcpyAsync(d_l_col_count, cnt + L, (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
+        unsigned long long hm[17];
+        int64_t tot[2];
+        GS_CUDA(cudaMemcpyAsync(hm, misc, sizeof(hm), cudaMemcpyDeviceToHost, st));
+        GS_CUDA(cudaMemcpyAsync(&tot[0], gp + L, 8, cudaMemcpyDeviceToHost, st));
+        GS_CUDA(cudaMemcpyAsync(&tot[1], gp + (L + 1) + L, 8, cudaMemcpyDeviceToHost, st));
+        GS_CUDA(cudaStreamSynchronize(st));
+        if ((uint32_t)(hm[16] & 0xffffffffu) & ERR_QUEUE_OVERFLOW) return GSOFA_ERR_QUEUE_OVERFLOW;
+        summary[0] = (uint64_t)(tot[0] + tot[1]) - hc[0] - hc[1];
+        summary[1] = (uint64_t)(tot[0] + tot[1] + n);
+        summary[2] = hm[4];
+    } catch (CudaFail &f) {
+        return fail_cuda(f.e);
+    }
+    return GSOFA_OK;
+}

@@ -193,6 +193,42 @@ gsofa_status gsofa_result_fetch(gsofa_ctx *ctx, const gsofa_result *r,
 size_t gsofa_predict_scratch_bytes(const gsofa_ctx *ctx, int32_t n, int64_t nnz,
                                    const gsofa_params *params);
 
+/* ---- factorization without device allocation ------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * code embedded in an application whose own allocator owns all device memory
+ * (a solver plugin under a host framework's memory pool or budget), and code
+ * on latency-critical paths where cudaMalloc's implicit device-wide
+ * synchronisation is not acceptable.  The caller passes device pointers for
+ * the input (the colbeg/colend/csr triple, already on `device`) and for the
+ * outputs; every intermediate array lives in one file-scope static device
+ * array of GSOFA_NOALLOC_SCRATCH_BYTES that each GPU loading this library
+ * holds until the process exits.  Nothing here calls cudaMalloc, cudaFree or
+ * an allocating library routine.
+ *
+ * Limits: n <= GSOFA_NOALLOC_MAX_N and the line ranges' total length
+ * <= GSOFA_NOALLOC_MAX_NNZ; larger inputs return GSOFA_ERR_UNSUPPORTED before
+ * any work is issued.  Counts only (no pattern): per-line U row counts,
+ * L column counts, the supernode starts and a host summary
+ * summary[0] = fill count, [1] = nnz(L+U), [2] = number of supernodes.
+ *
+ * The first call on a device looks up the static array's device address
+ * (with that device current); make that first call before any stream
+ * capture.  All calls on a device share the one array and it keeps the last
+ * call's contents (everything that must start at zero is cleared by the
+ * call), so calls that overlap on the GPU race: issue them one at a time.
+ * The call returns after its work on `cuda_stream` (NULL: the legacy default
+ * stream) has finished. */
+#define GSOFA_NOALLOC_MAX_N 16384
+#define GSOFA_NOALLOC_MAX_NNZ 262144
+#define GSOFA_NOALLOC_SCRATCH_BYTES (16u << 20)
+gsofa_status gsofa_symbfact_counts_noalloc(int device, void *cuda_stream, int32_t n,
+                                           int64_t nnz, const int32_t *d_beg,
+                                           const int32_t *d_end, const int32_t *d_adj,
+                                           int32_t max_supernode_size,
+                                           int32_t *d_u_row_count,
+                                           int32_t *d_l_col_count,
+                                           int32_t *d_sn_start, uint64_t *summary);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,66 @@
+"""The factorization entry point that allocates no device memory.
+
+gsofa_symbfact_counts_noalloc serves callers that cannot call cudaMalloc:
+code embedded under a host application's own device allocator or memory
+budget, and code on paths where cudaMalloc's implicit device-wide
+synchronisation is not allowed.  Its scratch is a static device array inside
+the library, shared by every call on a device.  These tests call it through
+the C ABI with caller-owned device buffers and compare every output with the
+regular entry point (gsofa_symbfact, counts only), on calls made back to back
+so that leftovers of one call in the shared scratch would show up in the
+next.  This file is collected last on purpose."""
+import numpy as np
+import pytest
+
+import gsofa_b200
+from gsofa_b200 import matgen
+from tests.common import bundled, random_graph
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _noalloc(g, max_sn):
+    dev = torch.device("cuda", 0)
+    beg = torch.from_numpy(g.beg).to(dev)
+    end = torch.from_numpy(g.end).to(dev)
+    adj = torch.from_numpy(g.adj if g.nnz else np.zeros(1, np.int32)).to(dev)
+    u = torch.full((max(g.n, 1),), -1, dtype=torch.int32, device=dev)
+    lc = torch.full((max(g.n, 1),), -1, dtype=torch.int32, device=dev)
+    sn = torch.full((max(g.n, 1),), -1, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    fills, nnz_lu, nsn = gsofa_b200.symbfact_counts_noalloc(
+        0, stream.cuda_stream, g.n, g.nnz, beg.data_ptr(), end.data_ptr(), adj.data_ptr(),
+        u.data_ptr(), lc.data_ptr(), sn.data_ptr(), max_sn)
+    return fills, nnz_lu, u.cpu().numpy()[:g.n], lc.cpu().numpy()[:g.n], sn.cpu().numpy()[:nsn]
+
+
+def _regular(ctx, g, max_sn):
+    r = ctx.symbfact(ctx.upload(g), want_pattern=0, max_supernode_size=max_sn)
+    return r.fill_count, r.nnz_lu, r.u_row_count, r.l_col_count, r.sn_start
+
+
+def _same(a, b, where):
+    assert a[0] == b[0], f"{where}: fill count {a[0]} != {b[0]}"
+    assert a[1] == b[1], f"{where}: nnz(L+U) {a[1]} != {b[1]}"
+    for k, name in ((2, "u_row_count"), (3, "l_col_count"), (4, "sn_start")):
+        assert np.array_equal(a[k], b[k]), f"{where}: {name} differs"
+
+
+def test_noalloc_matches_regular_entry_on_consecutive_calls():
+    mats = [(bundled(), 0), (matgen.grid3d(16, ordering="nd", drop_frac=0.1, seed=4), 8),
+            (random_graph(700, 0.01, 21), 0), (bundled(), 4)]
+    with gsofa_b200.Context(0) as ctx:
+        for i, (g, max_sn) in enumerate(mats):
+            _same(_noalloc(g, max_sn), _regular(ctx, g, max_sn), f"call {i} ({g.name})")
+
+
+def test_noalloc_rejects_oversized_inputs():
+    n = gsofa_b200.NOALLOC_MAX_N + 1
+    with pytest.raises(gsofa_b200.GsofaError) as e:
+        gsofa_b200.symbfact_counts_noalloc(0, 0, n, 10, 1, 1, 1, 1, 1, 1)
+    assert e.value.status == 7
+    with pytest.raises(gsofa_b200.GsofaError) as e:
+        gsofa_b200.symbfact_counts_noalloc(0, 0, 100, gsofa_b200.NOALLOC_MAX_NNZ + 1, 1, 1, 1, 1, 1, 1)
+    assert e.value.status == 7
