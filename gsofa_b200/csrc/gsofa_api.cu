@@ -70,6 +70,10 @@ struct gsofa_ctx {
     DevBuf st_beg, st_end, st_adj, st_tmp;
     std::vector<gsofa_matrix *> matrices;
     uint64_t job_id = 0;      // incremented by every factorization
+    DevBuf matinfo;
+    // launch shapes already sized: (block, bitmap words) -> (ring, CTAs/SM)
+    struct Shape { int block; int32_t words; int ring; int occ; };
+    std::vector<Shape> shapes;
 
     void *grow(DevBuf &b, size_t bytes)
     {
@@ -118,7 +122,7 @@ struct ResultInternal {
     uint64_t job_id;
     int64_t L, line_base, n;
     int64_t u0, l0;         // first index of the U rows / L columns in `out`
-    std::vector<int32_t> sn;  // supernode starts (relative)
+    int64_t sn0;            // first supernode of this matrix in the device list
 };
 
 int pick_block(int32_t max_n)
@@ -177,9 +181,17 @@ void free_result_arrays(gsofa_result *r)
 }
 
 // The factorization of `count` matrices in one cooperative launch.
+double now_ms()
+{
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
 gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
                      const gsofa_params *pin, gsofa_result *out)
 {
+    static const bool host_timing = std::getenv("GSOFA_HOST_TIMING") != nullptr;
+    const double t_enter = now_ms();
     gsofa_params p;
     resolve_params(pin, &p);
     if (count <= 0 || !mats || !out) return GSOFA_ERR_INVALID_INPUT;
@@ -223,18 +235,29 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     const size_t static_smem = sizeof(SharedState) + 1024;
     if ((size_t)bitmap_words * 4 + 1024 * 4 + static_smem > ctx->smem_optin) return GSOFA_ERR_UNSUPPORTED;
     // frontier ring: the largest of 8K/4K/2K/1K entries that keeps the most
-    // CTAs (each with its own bitmap) resident on an SM
+    // CTAs (each with its own bitmap) resident on an SM; sized once per shape
     int ring = 0, occ = 0;
     size_t smem = 0;
-    for (int cand = 8192; cand >= 1024; cand >>= 1) {
-        const size_t sm = (size_t)bitmap_words * 4 + (size_t)cand * 4;
-        if (sm + static_smem > ctx->smem_optin) continue;
-        GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        int o = 0;
-        GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kfn, block, sm));
-        if (o > occ) { occ = o; ring = cand; smem = sm; }
+    bool cached = false;
+    for (const auto &sh : ctx->shapes)
+        if (sh.block == block && sh.words == bitmap_words) {
+            ring = sh.ring; occ = sh.occ; cached = true;
+        }
+    if (cached) {
+        smem = (size_t)bitmap_words * 4 + (size_t)ring * 4;
+    } else {
+        for (int cand = 8192; cand >= 1024; cand >>= 1) {
+            const size_t sm = (size_t)bitmap_words * 4 + (size_t)cand * 4;
+            if (sm + static_smem > ctx->smem_optin) continue;
+            GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            int o = 0;
+            GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kfn, block, sm));
+            if (o > occ) { occ = o; ring = cand; smem = sm; }
+        }
+        if (occ <= 0) return GSOFA_ERR_UNSUPPORTED;
+        ctx->shapes.push_back({block, bitmap_words, ring, occ});
     }
-    if (occ <= 0) return GSOFA_ERR_UNSUPPORTED;
+    // the attribute belongs to the kernel, which other callers may resize
     GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = p.ctas_per_sm > 0 ? std::min(p.ctas_per_sm, occ) : occ;
     const int grid = per_sm * ctx->sm_count;
@@ -310,6 +333,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
             d_out = (int32_t *)ctx->grow(ctx->out, (size_t)pool_cap * sizeof(int32_t));
         }
         MatDesc *d_mats = (MatDesc *)ctx->grow(ctx->mats, md.size() * sizeof(MatDesc));
+        int64_t *d_minfo = (int64_t *)ctx->grow(ctx->matinfo, (size_t)3 * count * sizeof(int64_t));
         Range *d_ranges = (Range *)ctx->grow(ctx->ranges, std::max<size_t>(ranges.size(), 1) * sizeof(Range));
 
         cudaStream_t st = ctx->stream;
@@ -351,6 +375,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         a.lrow = d_lrow;
         a.snind = d_snind;
         a.sn_list = d_sn;
+        a.mat_info = d_minfo;
         a.ntiles = ntiles;
         a.tile_sum = d_tiles;
         a.tile_last = d_tiles + 2 * ntiles;
@@ -359,6 +384,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         a.status = d_status;
 
         void *args[] = {&a};
+        const double t_launch = now_ms();
         GS_CUDA(cudaEventRecord(ctx->ev0, st));
         GS_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(block), args, smem, st));
         GS_CUDA(cudaEventRecord(ctx->ev1, st));
@@ -369,6 +395,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         GS_CUDA(cudaMemcpyAsync(&tot[0], d_gptr + L, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
         GS_CUDA(cudaMemcpyAsync(&tot[1], d_gptr + (L + 1) + L, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
         GS_CUDA(cudaStreamSynchronize(st));
+        const double t_done = now_ms();
         float ms = 0.f;
         GS_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
         const uint32_t status = (uint32_t)(h_misc[16] & 0xffffffffu);
@@ -385,24 +412,34 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
             return GSOFA_ERR_QUEUE_OVERFLOW;
         }
 
-        // per-matrix results
-        std::vector<int64_t> gp0(count + 1), gp1(count + 1);
-        std::vector<int32_t> snl;
+        // per-matrix results: offsets at every matrix's first line come from
+        // mat_info (empty matrices take their successor's values)
+        std::vector<int64_t> mi((size_t)3 * count);
+        GS_CUDA(cudaMemcpyAsync(mi.data(), d_minfo, mi.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        GS_CUDA(cudaStreamSynchronize(st));
+        std::vector<int64_t> s0(count + 1), s1(count + 1), ss(count + 1);
+        s0[count] = tot[0];
+        s1[count] = tot[1];
+        ss[count] = (int64_t)nsn;
+        for (int i = count - 1; i >= 0; i--) {
+            if (md[i].n > 0) {
+                s0[i] = mi[3 * i];
+                s1[i] = mi[3 * i + 1];
+                ss[i] = mi[3 * i + 2];
+            } else {
+                s0[i] = s0[i + 1];
+                s1[i] = s1[i + 1];
+                ss[i] = ss[i + 1];
+            }
+        }
         const bool download_lines = !(p.flags & GSOFA_FLAG_NO_DOWNLOAD);
         for (int i = 0; i < count; i++) {
-            int64_t lb = md[i].line_base, n = md[i].n;
-            int64_t v[4];
-            GS_CUDA(cudaMemcpyAsync(&v[0], d_gptr + lb, 8, cudaMemcpyDeviceToHost, st));
-            GS_CUDA(cudaMemcpyAsync(&v[1], d_gptr + lb + n, 8, cudaMemcpyDeviceToHost, st));
-            GS_CUDA(cudaMemcpyAsync(&v[2], d_gptr + (L + 1) + lb, 8, cudaMemcpyDeviceToHost, st));
-            GS_CUDA(cudaMemcpyAsync(&v[3], d_gptr + (L + 1) + lb + n, 8, cudaMemcpyDeviceToHost, st));
-            GS_CUDA(cudaStreamSynchronize(st));
+            const int64_t lb = md[i].line_base, n = md[i].n;
             gsofa_result &r = out[i];
-            gp0[i] = v[0];
-            gp1[i] = tot[0] + v[2];
-            r.nnz_u = (uint64_t)(v[1] - v[0]);
-            r.nnz_l = (uint64_t)(v[3] - v[2]);
+            r.nnz_u = (uint64_t)(s0[i + 1] - s0[i]);
+            r.nnz_l = (uint64_t)(s1[i + 1] - s1[i]);
             r.nnz_lu = r.nnz_u + r.nnz_l + (uint64_t)n;
+            r.n_supernodes = (int32_t)(ss[i + 1] - ss[i]);
             r.kernel_ms = ms;
             r.edges_inspected = edges;
             r.sources = nsrc;
@@ -420,44 +457,33 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
                 r.u_row_count = download(st, d_cnt, lb, n);
                 r.l_col_count = download(st, d_cnt, L + lb, n);
                 if (want_pattern) r.l_row_count = download(st, d_lrow, lb, n);
-            }
-            if (want_pattern && download_lines) {
-                r.u_ptr = download(st, d_gptr, lb, n + 1);
-                r.l_ptr = download(st, d_gptr, (L + 1) + lb, n + 1);
-                r.u_idx = download(st, d_out, v[0], v[1] - v[0]);
-                r.l_idx = download(st, d_out, tot[0] + v[2], v[3] - v[2]);
-            }
-        }
-        if (download_lines || true) {
-            snl.resize((size_t)nsn);
-            if (nsn) GS_CUDA(cudaMemcpyAsync(snl.data(), d_sn, nsn * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-        }
-        GS_CUDA(cudaStreamSynchronize(st));
-        for (int i = 0; i < count; i++) {
-            gsofa_result &r = out[i];
-            const int64_t lb = md[i].line_base, n = md[i].n;
-            auto b = std::lower_bound(snl.begin(), snl.end(), (int32_t)lb);
-            auto e = std::lower_bound(snl.begin(), snl.end(), (int32_t)(lb + n));
-            r.n_supernodes = (int32_t)(e - b);
-            if (download_lines) {
-                r.sn_start = (int32_t *)std::malloc(std::max<size_t>((size_t)(e - b), 1) * sizeof(int32_t));
-                if (!r.sn_start) throw std::bad_alloc();
-                for (auto it = b; it != e; ++it) r.sn_start[it - b] = *it - (int32_t)lb;
+                r.sn_start = download(st, d_sn, ss[i], r.n_supernodes);
+                if (want_pattern) {
+                    r.u_ptr = download(st, d_gptr, lb, n + 1);
+                    r.l_ptr = download(st, d_gptr, (L + 1) + lb, n + 1);
+                    r.u_idx = download(st, d_out, s0[i], (int64_t)r.nnz_u);
+                    r.l_idx = download(st, d_out, tot[0] + s1[i], (int64_t)r.nnz_l);
+                }
             } else {
                 ResultInternal *ri = new ResultInternal();
                 ri->job_id = ctx->job_id;
                 ri->L = L;
                 ri->line_base = lb;
                 ri->n = n;
-                ri->u0 = gp0[i];
-                ri->l0 = gp1[i];
-                ri->sn.reserve((size_t)(e - b));
-                for (auto it = b; it != e; ++it) ri->sn.push_back(*it - (int32_t)lb);
+                ri->u0 = s0[i];
+                ri->l0 = tot[0] + s1[i];
+                ri->sn0 = ss[i];
                 r.internal = ri;
             }
-            if (want_pattern && download_lines) {
+        }
+        GS_CUDA(cudaStreamSynchronize(st));
+        for (int i = 0; i < count && download_lines; i++) {
+            gsofa_result &r = out[i];
+            const int64_t lb = md[i].line_base, n = md[i].n;
+            for (int32_t k = 0; k < r.n_supernodes; k++) r.sn_start[k] -= (int32_t)lb;
+            if (want_pattern) {
                 const int64_t u0 = r.u_ptr[0], l0 = r.l_ptr[0];
-                for (int64_t s = 0; s <= n; s++) { r.u_ptr[s] -= u0; r.l_ptr[s] -= l0; }
+                for (int64_t q = 0; q <= n; q++) { r.u_ptr[q] -= u0; r.l_ptr[q] -= l0; }
             }
             if (part_count > 1) {
                 // fills of the processed lines: subtract their original entries
@@ -465,7 +491,22 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
                 GS_CUDA(cudaMemcpy(ou.data(), mats[i]->d_orig_up, n * 4, cudaMemcpyDeviceToHost));
                 GS_CUDA(cudaMemcpy(ol.data(), mats[i]->d_orig_lo, n * 4, cudaMemcpyDeviceToHost));
                 uint64_t o = 0;
-                for (int64_t s = part_index; s < n; s += part_count) o += (uint64_t)ou[s] + (uint64_t)ol[s];
+                for (int64_t q = part_index; q < n; q += part_count) o += (uint64_t)ou[q] + (uint64_t)ol[q];
+                r.fill_count = r.nnz_u + r.nnz_l - o;
+            }
+        }
+        if (host_timing)
+            std::fprintf(stderr, "gsofa host: setup %.3f ms, launch..sync %.3f ms (kernel %.3f), results %.3f ms\n",
+                         t_launch - t_enter, t_done - t_launch, ms, now_ms() - t_done);
+        if (part_count > 1 && !download_lines) {
+            for (int i = 0; i < count; i++) {
+                gsofa_result &r = out[i];
+                const int64_t n = md[i].n;
+                std::vector<int32_t> ou((size_t)n), ol((size_t)n);
+                GS_CUDA(cudaMemcpy(ou.data(), mats[i]->d_orig_up, n * 4, cudaMemcpyDeviceToHost));
+                GS_CUDA(cudaMemcpy(ol.data(), mats[i]->d_orig_lo, n * 4, cudaMemcpyDeviceToHost));
+                uint64_t o = 0;
+                for (int64_t q = part_index; q < n; q += part_count) o += (uint64_t)ou[q] + (uint64_t)ol[q];
                 r.fill_count = r.nnz_u + r.nnz_l - o;
             }
         }
@@ -571,7 +612,7 @@ void gsofa_destroy(gsofa_ctx *c)
     while (!c->matrices.empty()) gsofa_matrix_free(c->matrices.back());
     DevBuf *bufs[] = {&c->queue, &c->cnt, &c->nxt, &c->poff, &c->gptr, &c->lrow, &c->snind,
                       &c->snlist, &c->tiles, &c->misc, &c->pool, &c->out, &c->mats, &c->ranges,
-                      &c->st_beg, &c->st_end, &c->st_adj, &c->st_tmp};
+                      &c->st_beg, &c->st_end, &c->st_adj, &c->st_tmp, &c->matinfo};
     for (DevBuf *b : bufs) c->release(*b);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -816,8 +857,10 @@ gsofa_status gsofa_result_fetch(gsofa_ctx *c, const gsofa_result *r, int32_t *u_
         cp(l_ptr, gptr + (L + 1) + lb, (size_t)(n + 1) * 8);
         cp(u_idx, outb + ri->u0, (size_t)r->nnz_u * 4);
         cp(l_idx, outb + ri->l0, (size_t)r->nnz_l * 4);
+        cp(sn_start, (const int32_t *)c->snlist.p + ri->sn0, (size_t)r->n_supernodes * 4);
         GS_CUDA(cudaStreamSynchronize(st));
-        if (sn_start && !ri->sn.empty()) std::memcpy(sn_start, ri->sn.data(), ri->sn.size() * 4);
+        if (sn_start)
+            for (int32_t k = 0; k < r->n_supernodes; k++) sn_start[k] -= (int32_t)lb;
         if (u_ptr) {
             const int64_t b = u_ptr[0];
             for (int64_t s = 0; s <= n; s++) u_ptr[s] -= b;

@@ -86,6 +86,8 @@ struct JobArgs {
     int32_t *lrow;             // [L]
     uint8_t *snind;            // [L]
     int32_t *sn_list;          // [L]
+    int64_t *mat_info;         // [nmats][3] at each matrix's first line: pass-0 and
+                               // pass-1 CSR offsets, supernodes before it
     int64_t ntiles;
     int64_t *tile_sum;         // [2][ntiles] then exclusive prefix (in place)
     int64_t *tile_last;        // [ntiles] last supernode-run start, then prefix max
@@ -746,6 +748,14 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
             int64_t tot;
             int64_t e = block_excl_scan<BLOCK>(v, &tot, sh.warp);
             if (v) a.sn_list[c + e] = (int32_t)l;
+            if (in && a.mat_info) {
+                const int mi = mat_of(l);
+                if (a.mats[mi].line_base == l) {
+                    a.mat_info[3 * mi + 0] = a.gptr[l];
+                    a.mat_info[3 * mi + 1] = a.gptr[(L + 1) + l];
+                    a.mat_info[3 * mi + 2] = c + e;
+                }
+            }
             c += tot;
         }
     }
