@@ -38,6 +38,7 @@ STATUS_NAMES = {
 
 FLAG_NO_DOWNLOAD = 0x1
 FLAG_DEVICE_TIMING = 0x2
+FLAG_GRAPH = 0x4
 
 
 class GsofaError(RuntimeError):

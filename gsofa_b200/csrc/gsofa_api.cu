@@ -55,6 +55,16 @@ struct DevBuf {
 
 }  // namespace
 
+// A captured factorization job and what it was captured from.
+struct GraphCache {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<char> key;
+    std::vector<MatDesc> md;     // host sources of the captured copies
+    std::vector<Range> ranges;
+    JobArgs args{};
+    cudaStream_t stream = nullptr;
+};
+
 struct gsofa_ctx {
     int device = 0;
     int sm_count = 0;
@@ -71,6 +81,7 @@ struct gsofa_ctx {
     std::vector<gsofa_matrix *> matrices;
     uint64_t job_id = 0;      // incremented by every factorization
     DevBuf matinfo;
+    GraphCache graph;         // last captured job (GSOFA_FLAG_GRAPH)
     // launch shapes already sized: (block, bitmap words) -> (ring, CTAs/SM)
     struct Shape { int block; int32_t words; int ring; int occ; };
     std::vector<Shape> shapes;
@@ -337,17 +348,6 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         Range *d_ranges = (Range *)ctx->grow(ctx->ranges, std::max<size_t>(ranges.size(), 1) * sizeof(Range));
 
         cudaStream_t st = ctx->stream;
-        GS_CUDA(cudaMemcpyAsync(d_mats, md.data(), md.size() * sizeof(MatDesc), cudaMemcpyHostToDevice, st));
-        if (!ranges.empty())
-            GS_CUDA(cudaMemcpyAsync(d_ranges, ranges.data(), ranges.size() * sizeof(Range),
-                                    cudaMemcpyHostToDevice, st));
-        GS_CUDA(cudaMemsetAsync(d_misc, 0, 256, st));
-        GS_CUDA(cudaMemsetAsync(d_lrow, 0, (size_t)L * sizeof(int32_t), st));
-        if (part_count > 1) {
-            GS_CUDA(cudaMemsetAsync(d_cnt, 0, (size_t)2 * L * sizeof(int32_t), st));
-            GS_CUDA(cudaMemsetAsync(d_nxt, 0, (size_t)2 * L, st));
-        }
-
         JobArgs a{};
         a.mats = d_mats;
         a.nmats = count;
@@ -383,10 +383,71 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         a.counters = d_counters;
         a.status = d_status;
 
+        // The job: descriptor copies, clears and the cooperative launch.  With
+        // GSOFA_FLAG_GRAPH it is captured once into a CUDA graph and replayed
+        // while the same job (matrices, parameters, buffers) comes back.
+        const MatDesc *md_src = md.data();
+        const Range *rg_src = ranges.data();
+        auto issue = [&](void *const *kargs) {
+            GS_CUDA(cudaMemcpyAsync(d_mats, md_src, md.size() * sizeof(MatDesc), cudaMemcpyHostToDevice, st));
+            if (!ranges.empty())
+                GS_CUDA(cudaMemcpyAsync(d_ranges, rg_src, ranges.size() * sizeof(Range),
+                                        cudaMemcpyHostToDevice, st));
+            GS_CUDA(cudaMemsetAsync(d_misc, 0, 256, st));
+            GS_CUDA(cudaMemsetAsync(d_lrow, 0, (size_t)L * sizeof(int32_t), st));
+            if (part_count > 1) {
+                GS_CUDA(cudaMemsetAsync(d_cnt, 0, (size_t)2 * L * sizeof(int32_t), st));
+                GS_CUDA(cudaMemsetAsync(d_nxt, 0, (size_t)2 * L, st));
+            }
+            GS_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(block), (void **)kargs, smem, st));
+        };
         void *args[] = {&a};
+        bool graphed = false;
+        if (p.flags & GSOFA_FLAG_GRAPH) {
+            std::vector<char> key(sizeof(JobArgs) + md.size() * sizeof(MatDesc) +
+                                  ranges.size() * sizeof(Range) + 4 * sizeof(int64_t));
+            char *kp = key.data();
+            std::memcpy(kp, &a, sizeof(JobArgs)); kp += sizeof(JobArgs);
+            std::memcpy(kp, md.data(), md.size() * sizeof(MatDesc)); kp += md.size() * sizeof(MatDesc);
+            if (!ranges.empty()) std::memcpy(kp, ranges.data(), ranges.size() * sizeof(Range));
+            kp += ranges.size() * sizeof(Range);
+            const int64_t extra[4] = {(int64_t)(intptr_t)kfn, grid, block, (int64_t)smem};
+            std::memcpy(kp, extra, sizeof(extra));
+            GraphCache &gc = ctx->graph;
+            if (!(gc.exec && gc.key == key && gc.stream == st)) {
+                if (gc.exec) { cudaGraphExecDestroy(gc.exec); gc.exec = nullptr; }
+                gc.key = key;
+                gc.md = md;
+                gc.ranges = ranges;
+                gc.stream = st;
+                md_src = gc.md.data();
+                rg_src = gc.ranges.data();
+                gc.args = a;
+                void *gargs[] = {&gc.args};
+                cudaGraph_t graph = nullptr;
+                bool ok = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+                if (ok) {
+                    try {
+                        issue(gargs);
+                    } catch (CudaFail &) {
+                        ok = false;
+                    }
+                    ok = (cudaStreamEndCapture(st, &graph) == cudaSuccess) && ok;
+                }
+                if (ok) ok = cudaGraphInstantiate(&gc.exec, graph, 0) == cudaSuccess;
+                if (graph) cudaGraphDestroy(graph);
+                if (!ok) {
+                    cudaGetLastError();
+                    gc.exec = nullptr;
+                    gc.key.clear();
+                }
+            }
+            graphed = gc.exec != nullptr;
+        }
         const double t_launch = now_ms();
         GS_CUDA(cudaEventRecord(ctx->ev0, st));
-        GS_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(block), args, smem, st));
+        if (graphed) GS_CUDA(cudaGraphLaunch(ctx->graph.exec, st));
+        else issue(args);
         GS_CUDA(cudaEventRecord(ctx->ev1, st));
 
         unsigned long long h_misc[17];
@@ -614,6 +675,7 @@ void gsofa_destroy(gsofa_ctx *c)
                       &c->snlist, &c->tiles, &c->misc, &c->pool, &c->out, &c->mats, &c->ranges,
                       &c->st_beg, &c->st_end, &c->st_adj, &c->st_tmp, &c->matinfo};
     for (DevBuf *b : bufs) c->release(*b);
+    if (c->graph.exec) cudaGraphExecDestroy(c->graph.exec);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);

@@ -85,6 +85,9 @@ typedef struct gsofa_params {
 
 #define GSOFA_FLAG_NO_DOWNLOAD 0x1 /* keep per-line arrays on the device only */
 #define GSOFA_FLAG_DEVICE_TIMING 0x2 /* record the traversal kernel time       */
+#define GSOFA_FLAG_GRAPH 0x4       /* capture the launch in a CUDA graph and
+                                      replay it while the same job (matrices,
+                                      parameters, buffers) repeats            */
 
 typedef struct gsofa_result {
     int32_t n;

@@ -187,3 +187,31 @@ def test_fetch_into_caller_buffers(ctx):
     assert np.array_equal(z, ref["u_row_count"])
     L.gsofa_result_free(r1)
     L.gsofa_result_free(r2)
+
+
+def test_graph_replay(ctx):
+    gs = [matgen.grid3d(9, seed=1), matgen.powerlaw(600, seed=2), bundled()]
+    ms = [ctx.upload(g) for g in gs]
+    p = gsofa_b200.Params.default(flags=gsofa_b200.FLAG_GRAPH, max_supernode_size=8)
+    refs = [_oracle(g, 8) for g in gs]
+    for rep in range(3):
+        rs = ctx.symbfact_batch(ms, p)
+        for g, r, ref in zip(gs, rs, refs):
+            assert_same(r, ref, where=f"graph replay {rep} {g.name}")
+    # a different job replaces the captured one
+    rs = ctx.symbfact_batch(ms[1:], p)
+    for g, r, ref in zip(gs[1:], rs, refs[1:]):
+        assert_same(r, ref, where=f"graph recapture {g.name}")
+
+
+def test_autotune_choice_is_cached_and_exact(ctx, tmp_path):
+    from gsofa_b200 import autotune
+    gs = [matgen.grid3d(12, seed=3), matgen.powerlaw(900, seed=4), matgen.grid2d(30)]
+    ms = [ctx.upload(g) for g in gs]
+    cache = str(tmp_path / "tune.json")
+    best, rep = autotune.autotune(ctx, ms, cache_path=cache)
+    assert not rep["cached"] and len(rep["timings"]) == len(autotune.DEFAULT_CANDIDATES)
+    best2, rep2 = autotune.autotune(ctx, ms, cache_path=cache)
+    assert rep2["cached"] and rep2["choice"] == rep["choice"]
+    for g, r in zip(gs, ctx.symbfact_batch(ms, best2)):
+        assert_same(r, _oracle(g), where=f"autotuned {g.name}")
