@@ -83,7 +83,7 @@ struct gsofa_ctx {
     DevBuf matinfo;
     GraphCache graph;         // last captured job (GSOFA_FLAG_GRAPH)
     // launch shapes already sized: (block, bitmap words) -> (ring, CTAs/SM)
-    struct Shape { int block; int32_t words; int ring; int occ; };
+    struct Shape { int block; int32_t words; bool paired; int ring; int occ; };
     std::vector<Shape> shapes;
 
     void *grow(DevBuf &b, size_t bytes)
@@ -142,19 +142,19 @@ int pick_block(int32_t max_n)
     return 512;
 }
 
-template <int BLOCK>
+template <int BLOCK, bool PAIRED>
 void *factor_fn()
 {
-    return (void *)factor_kernel<BLOCK>;
+    return (void *)factor_kernel<BLOCK, PAIRED>;
 }
 
-void *factor_kernel_for(int block)
+void *factor_kernel_for(int block, bool paired)
 {
     switch (block) {
-    case 128: return factor_fn<128>();
-    case 256: return factor_fn<256>();
-    case 512: return factor_fn<512>();
-    case 1024: return factor_fn<1024>();
+    case 128: return paired ? nullptr : factor_fn<128, false>();
+    case 256: return paired ? factor_fn<256, true>() : factor_fn<256, false>();
+    case 512: return paired ? factor_fn<512, true>() : factor_fn<512, false>();
+    case 1024: return paired ? factor_fn<1024, true>() : factor_fn<1024, false>();
     default: return nullptr;
     }
 }
@@ -215,7 +215,10 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     const int part_index = p.part_count > 1 ? p.part_index : 0;
     if (part_index < 0 || part_index >= part_count) return GSOFA_ERR_INVALID_INPUT;
     const bool want_pattern = p.want_pattern != 0 && part_count == 1;
-    const int reuse = (p.reuse != 0 && part_count == 1) ? 1 : 0;   // -1 (auto): on
+    // reuse: -1 (auto) or 1 = paired passes with exact reuse when two bitmaps
+    // fit in shared memory, else adjacency chains; 2 = adjacency chains;
+    // 0 = every source from scratch
+    const int reuse = (p.reuse != 0 && part_count == 1) ? 1 : 0;
 
     // line space and per-matrix descriptors
     std::vector<MatDesc> md(count);
@@ -234,31 +237,36 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     if (L == 0) return GSOFA_OK;
 
     // parameters
-    int block = p.block_size ? p.block_size : pick_block(max_n);
-    void *kfn = factor_kernel_for(block);
+    const int32_t words_needed = ((max_n + 31) / 32 + 3) / 4 * 4;
+    const bool paired = reuse && p.reuse != 2 &&
+                        (size_t)2 * words_needed * 4 + 2 * 1024 * 4 + sizeof(SharedState) * 2 + 1024 <=
+                            ctx->smem_optin;
+    int block = p.block_size ? p.block_size : pick_block(max_n) * (paired ? 2 : 1);
+    void *kfn = factor_kernel_for(block, paired);
     if (!kfn) return GSOFA_ERR_INVALID_INPUT;
+    const int NS = paired ? 2 : 1;
     int lanes = p.threads_per_source ? p.threads_per_source : 1;
     if (lanes != 1 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
         return GSOFA_ERR_INVALID_INPUT;
     int chunk = p.src_chunk > 0 ? p.src_chunk : (reuse ? 32 : 1);
 
-    const int32_t bitmap_words = ((max_n + 31) / 32 + 3) / 4 * 4;
-    const size_t static_smem = sizeof(SharedState) + 1024;
-    if ((size_t)bitmap_words * 4 + 1024 * 4 + static_smem > ctx->smem_optin) return GSOFA_ERR_UNSUPPORTED;
+    const int32_t bitmap_words = words_needed;
+    const size_t static_smem = sizeof(SharedState) * NS + 1024;
+    if ((size_t)NS * (bitmap_words * 4 + 1024 * 4) + static_smem > ctx->smem_optin) return GSOFA_ERR_UNSUPPORTED;
     // frontier ring: the largest of 8K/4K/2K/1K entries that keeps the most
     // CTAs (each with its own bitmap) resident on an SM; sized once per shape
     int ring = 0, occ = 0;
     size_t smem = 0;
     bool cached = false;
     for (const auto &sh : ctx->shapes)
-        if (sh.block == block && sh.words == bitmap_words) {
+        if (sh.block == block && sh.words == bitmap_words && sh.paired == paired) {
             ring = sh.ring; occ = sh.occ; cached = true;
         }
     if (cached) {
-        smem = (size_t)bitmap_words * 4 + (size_t)ring * 4;
+        smem = (size_t)NS * ((size_t)bitmap_words * 4 + (size_t)ring * 4);
     } else {
         for (int cand = 8192; cand >= 1024; cand >>= 1) {
-            const size_t sm = (size_t)bitmap_words * 4 + (size_t)cand * 4;
+            const size_t sm = (size_t)NS * ((size_t)bitmap_words * 4 + (size_t)cand * 4);
             if (sm + static_smem > ctx->smem_optin) continue;
             GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
             int o = 0;
@@ -266,7 +274,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
             if (o > occ) { occ = o; ring = cand; smem = sm; }
         }
         if (occ <= 0) return GSOFA_ERR_UNSUPPORTED;
-        ctx->shapes.push_back({block, bitmap_words, ring, occ});
+        ctx->shapes.push_back({block, bitmap_words, paired, ring, occ});
     }
     // the attribute belongs to the kernel, which other callers may resize
     GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -290,7 +298,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         r.offset = part_index;
         r.nj = (n - part_index + part_count - 1) / part_count;
         r.piece_base = npieces;
-        r.npieces = 2 * (((int64_t)r.nj + chunk - 1) / chunk);
+        r.npieces = (paired ? 1 : 2) * (((int64_t)r.nj + chunk - 1) / chunk);
         npieces += r.npieces;
         ranges.push_back(r);
     }
@@ -323,7 +331,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     ctx->job_id++;
     for (int attempt = 0; attempt < 2; attempt++) {
         // scratch
-        int32_t *d_queue = (int32_t *)ctx->grow(ctx->queue, (size_t)grid * qcap * sizeof(int32_t));
+        int32_t *d_queue = (int32_t *)ctx->grow(ctx->queue, (size_t)grid * NS * qcap * sizeof(int32_t));
         int32_t *d_cnt = (int32_t *)ctx->grow(ctx->cnt, (size_t)2 * L * sizeof(int32_t));
         uint8_t *d_nxt = (uint8_t *)ctx->grow(ctx->nxt, (size_t)2 * L);
         int64_t *d_poff = (int64_t *)ctx->grow(ctx->poff, (size_t)2 * L * sizeof(int64_t));
@@ -1090,7 +1098,7 @@ extern "C" gsofa_status gsofa_symbfact_counts_noalloc(int device, void *cuda_str
 
         // launch shape: 256 threads, one CTA per SM (its queue slice is n ints)
         constexpr int BLOCK = 256;
-        void *kfn = factor_kernel_for(BLOCK);
+        void *kfn = factor_kernel_for(BLOCK, false);
         const int32_t bitmap_words = ((n + 31) / 32 + 3) / 4 * 4;
         const int ring = 4096;
         const size_t smem = (size_t)bitmap_words * 4 + (size_t)ring * 4;

@@ -238,12 +238,23 @@ struct SharedState {
     int64_t warp[32];
 };
 
-// Clears the bitmap words covering vertices [lo, hi].
-template <int BLOCK>
-__device__ __forceinline__ void clear_range(uint32_t *bm, int lo, int hi)
+// Clears the bitmap words covering vertices [lo, hi]; gtid/GT: the calling
+// thread's index and the size of the thread group that shares the bitmap.
+template <int GT>
+__device__ __forceinline__ void clear_range(uint32_t *bm, int lo, int hi, int gtid)
 {
     if (hi < lo) return;
-    for (int w = (lo >> 5) + threadIdx.x; w <= (hi >> 5); w += BLOCK) bm[w] = 0u;
+    for (int w = (lo >> 5) + gtid; w <= (hi >> 5); w += GT) bm[w] = 0u;
+}
+
+// Barrier of the GT threads that work on one traversal: the whole CTA
+// (bar == 0) or one half of it (named barrier `bar`).
+template <int GT>
+__device__ __forceinline__ void gsync(int bar)
+{
+    if (bar == 0) __syncthreads();
+    else if (bar == 1) asm volatile("bar.sync 1, %0;" ::"n"(GT) : "memory");
+    else asm volatile("bar.sync 2, %0;" ::"n"(GT) : "memory");
 }
 
 // True when x-1 is in adj(x); evaluated by one whole warp.
@@ -286,15 +297,15 @@ __device__ __forceinline__ int32_t chain_start(const PassGraph &g, int32_t x, in
 // With `reuse`, the bitmap still holds the finished traversal of s-1, which is
 // valid because s-1 in adj(s) implies X(s-1) u {s-1} is inside X(s) and
 // hi(s-1) minus (s-1, s] is inside hi(s).
-template <int BLOCK>
+template <int GT>
 __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                                int64_t line, int pass, int32_t s, uint32_t *bm,
                                const Frontier &f, SharedState &sh,
                                unsigned long long &edges, const int32_t *rawdeg,
                                unsigned long long &xcnt, unsigned long long &einsp,
-                               unsigned long long *prof)
+                               unsigned long long *prof, const int gtid, const int bar)
 {
-    const int tid = threadIdx.x;
+    const int tid = gtid;
     const int lane = tid & 31;
     const int lanes = a.lanes;
     const int lane_in_group = tid & (lanes - 1);
@@ -307,7 +318,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         sh.fetch[0] = sh.fetch[1] = sh.fetch[2] = 0;
         if (test_and_set(bm, s)) { t_lo = s; t_hi = s; }
     }
-    __syncthreads();
+    gsync<GT>(bar);
 
     // seeding: every neighbour of s is structure of line s; level-0 items
     {
@@ -318,13 +329,13 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         }
         int *tailp = &sh.tailc[0];
         const int end = 0, start = 0;
-        for (int32_t k = b0 + tid; k < e0; k += BLOCK) GSOFA_VISIT(g.adj[k]);
+        for (int32_t k = b0 + tid; k < e0; k += GT) GSOFA_VISIT(g.adj[k]);
     }
 
     // level-synchronous expansion through vertices < s, one barrier a level
     int start = 0, wstart = 0;
     for (int L = 0;; L++) {
-        __syncthreads();
+        gsync<GT>(bar);
         const int end = start + sh.tailc[L % 3];
         if (end == start) {
             if (tid == 0) prof[0] += (unsigned long long)L;
@@ -429,7 +440,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
             if (wl != INT32_MAX) atomicMin(&sh.chain_lo, wl);
             if (wh >= 0) atomicMax(&sh.chain_hi, wh);
         }
-        __syncthreads();
+        gsync<GT>(bar);
     }
     const int chain_hi = sh.chain_hi;
     long long c1 = 0;
@@ -438,7 +449,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
     // hi(s) = set bits in (s, chain_hi].  Each warp owns a run of 32-word
     // chunks: it counts them, one cross-warp prefix gives its output offset,
     // then per chunk a warp scan places every lane's bits in sorted order.
-    constexpr int NWARP = BLOCK / 32;
+    constexpr int NWARP = GT / 32;
     const int wid = tid >> 5;
     const int w0 = (s + 1) >> 5;
     const int w1 = (chain_hi > s) ? (chain_hi >> 5) : (w0 - 1);
@@ -456,7 +467,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
     }
     wcount = __reduce_add_sync(0xffffffffu, wcount);
     if (lane == 0) sh.warp[wid] = wcount;
-    __syncthreads();
+    gsync<GT>(bar);
     int64_t wpre = 0, total = 0;
     {
         const int64_t v = lane < NWARP ? sh.warp[lane] : 0;
@@ -473,7 +484,9 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
     const int64_t slot = (int64_t)pass * a.L + line;
     if (tid == 0) {
         a.cnt[slot] = (int32_t)total;
-        a.nxt[slot] = (uint8_t)((s + 1 < n) && ((bm[(s + 1) >> 5] >> ((s + 1) & 31)) & 1u));
+        const int nx = (s + 1 < n) && ((bm[(s + 1) >> 5] >> ((s + 1) & 31)) & 1u);
+        a.nxt[slot] = (uint8_t)nx;
+        sh.flag = nx;
         if (a.want_pattern) {
             const unsigned long long o = atomicAdd(a.pool_tail, (unsigned long long)total);
             if ((int64_t)o + total > a.pool_cap) {
@@ -486,7 +499,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         }
     }
     if (a.want_pattern) {
-        __syncthreads();
+        gsync<GT>(bar);
         const int64_t base = sh.pool_base;
         if (base >= 0 && wcount > 0) {
             int64_t run = base + wpre;
@@ -511,34 +524,51 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
             }
         }
     }
-    __syncthreads();
+    gsync<GT>(bar);
     if (tid == 0) prof[2] += (unsigned long long)(clock64() - c1);
 }
 #undef GSOFA_VISIT
 
 // ---------------------------------------------------------------------------
 // The persistent cooperative factorization kernel.
-template <int BLOCK>
+//
+// PAIRED = false: every CTA runs one traversal at a time; a work piece is one
+// pass of a run of sources, and s reuses s-1's state when s-1 is in adj(s).
+// PAIRED = true: the CTA's two halves run pass G and pass G^T of the same
+// source side by side, each with its own bitmap and frontier ring, and
+// exchange their s+1 flags after every source.  By the fill-path theorem,
+// s-1 is in X_G(s) exactly when s is in hi_{G^T}(s-1) (and likewise with G
+// and G^T swapped), so each half reuses s-1's state whenever it is valid.
+template <int BLOCK, bool PAIRED>
 __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
 {
+    constexpr int GT = PAIRED ? BLOCK / 2 : BLOCK;
+    constexpr int NS = PAIRED ? 2 : 1;
     extern __shared__ __align__(16) uint32_t smem_dyn[];
-    uint32_t *bm = smem_dyn;                                  // bitmap_words
-    int32_t *ring = (int32_t *)(smem_dyn + a.bitmap_words);   // ring_size entries
-    __shared__ SharedState sh;
+    __shared__ SharedState shs[NS];
+    __shared__ int pair_flag[2][2];   // [source parity][pass]: s+1 in hi(s)
+    __shared__ long long s_piece;
     cg::grid_group grid = cg::this_grid();
     const int tid = threadIdx.x;
+    const int half = PAIRED ? tid / GT : 0;
+    const int gtid = PAIRED ? tid % GT : tid;
+    const int bar = PAIRED ? 1 + half : 0;
+    SharedState &sh = shs[half];
+    uint32_t *bm = smem_dyn + (size_t)half * a.bitmap_words;
+    int32_t *ring = (int32_t *)(smem_dyn + (size_t)NS * a.bitmap_words) + (size_t)half * a.ring_size;
 
     // ---- phase 1: traversals ------------------------------------------------
-    for (int w = tid; w < a.bitmap_words; w += BLOCK) bm[w] = 0u;
-    if (tid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
-    const Frontier fr{ring, a.queue + (int64_t)blockIdx.x * a.qcap, a.qcap, a.status, a.ring_size};
+    for (int w = tid; w < NS * a.bitmap_words; w += BLOCK) smem_dyn[w] = 0u;
+    if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
+    const Frontier fr{ring, a.queue + ((int64_t)blockIdx.x * NS + half) * a.qcap, a.qcap, a.status,
+                      a.ring_size};
     unsigned long long edges = 0, nsrc = 0, xcnt = 0, einsp = 0, nreuse = 0;
     unsigned long long prof[4] = {0, 0, 0, 0};  // levels, expansion, output, clearing cycles
     __syncthreads();
     for (;;) {
-        if (tid == 0) sh.piece = (long long)atomicAdd(a.piece_counter, 1ull);
+        if (tid == 0) s_piece = (long long)atomicAdd(a.piece_counter, 1ull);
         __syncthreads();
-        const int64_t pc = sh.piece;
+        const int64_t pc = s_piece;
         if (pc >= a.npieces) break;
         int r = 0;
         {
@@ -550,17 +580,17 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
         }
         const Range rg = a.ranges[r];
         const int64_t k = pc - rg.piece_base;
-        const int pass = (int)(k & 1);
-        const int64_t c = k >> 1;
+        const int pass = PAIRED ? half : (int)(k & 1);
+        const int64_t c = PAIRED ? k : (k >> 1);
         const int64_t j1 = (int64_t)rg.nj - c * rg.chunk;
         const int64_t j0 = max((int64_t)0, j1 - rg.chunk);
         const MatDesc md = a.mats[rg.mat];
         const PassGraph g = md.g[pass];
         int32_t s_lo = rg.offset + (int32_t)j0 * rg.stride;
         int32_t s_hi = rg.offset + (int32_t)j1 * rg.stride;   // exclusive (stride 1)
-        if (a.reuse && rg.stride == 1) {
-            // cut pieces where chains start, so a piece's first source rarely
-            // has a predecessor whose traversal it could have reused
+        if (!PAIRED && a.reuse && rg.stride == 1) {
+            // cut pieces where adjacency chains start, so a piece's first
+            // source rarely has a predecessor it could have reused
             if (tid < 32) {
                 const int32_t lo = (j0 == 0) ? s_lo : chain_start(g, s_lo, rg.chunk);
                 const int32_t hi = (j1 == rg.nj) ? s_hi : chain_start(g, s_hi, rg.chunk);
@@ -571,56 +601,70 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
             s_hi = sh.seg[1];
         }
         int prev = -2;
-        for (int32_t s = s_lo; s < s_hi; s += rg.stride) {
+        int idx = 0;
+        for (int32_t s = s_lo; s < s_hi; s += rg.stride, idx++) {
             int reuse = 0;
             if (a.reuse && prev == s - 1) {
-                if (tid < 32) {
-                    const bool h = warp_has_prev(g, s);
-                    if (tid == 0) sh.flag = h ? 1 : 0;
+                if (PAIRED) {
+                    reuse = pair_flag[(idx - 1) & 1][1 - half];
+                } else {
+                    if (tid < 32) {
+                        const bool h = warp_has_prev(g, s);
+                        if (tid == 0) sh.flag = h ? 1 : 0;
+                    }
+                    __syncthreads();
+                    reuse = sh.flag;
                 }
-                __syncthreads();
-                reuse = sh.flag;
             }
             if (!reuse) {
                 const long long cc = clock64();
                 const int clo = sh.chain_lo, chi = sh.chain_hi;
-                clear_range<BLOCK>(bm, clo, chi);
-                __syncthreads();
-                if (tid == 0) {
+                clear_range<GT>(bm, clo, chi, gtid);
+                gsync<GT>(bar);
+                if (gtid == 0) {
                     sh.chain_lo = INT32_MAX; sh.chain_hi = -1;
                     prof[3] += (unsigned long long)(clock64() - cc);
                 }
-            } else {
+            } else if (gtid == 0) {
                 nreuse++;
             }
-            process_source<BLOCK>(a, g, md.n, md.line_base + s, pass, s, bm, fr, sh, edges,
-                                  md.rawdeg, xcnt, einsp, prof);
+            process_source<GT>(a, g, md.n, md.line_base + s, pass, s, bm, fr, sh, edges,
+                               md.rawdeg, xcnt, einsp, prof, gtid, bar);
+            if (PAIRED) {
+                if (gtid == 0) pair_flag[idx & 1][half] = sh.flag;
+                __syncthreads();
+            }
             prev = s;
-            nsrc++;
+            if (gtid == 0) nsrc++;
         }
         // the next piece starts from an empty bitmap
         {
             const int clo = sh.chain_lo, chi = sh.chain_hi;
-            clear_range<BLOCK>(bm, clo, chi);
+            clear_range<GT>(bm, clo, chi, gtid);
             __syncthreads();
-            if (tid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
+            if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
             __syncthreads();
         }
     }
     {
-        const int64_t e = block_sum<BLOCK>((int64_t)edges, sh.warp);
-        const int64_t x = block_sum<BLOCK>((int64_t)xcnt, sh.warp);
-        const int64_t ei = block_sum<BLOCK>((int64_t)einsp, sh.warp);
+        int64_t *wsum = shs[0].warp;
+        const int64_t e = block_sum<BLOCK>((int64_t)edges, wsum);
+        const int64_t x = block_sum<BLOCK>((int64_t)xcnt, wsum);
+        const int64_t ei = block_sum<BLOCK>((int64_t)einsp, wsum);
+        const int64_t ns = block_sum<BLOCK>((int64_t)nsrc, wsum);
+        const int64_t nr = block_sum<BLOCK>((int64_t)nreuse, wsum);
+        int64_t pv[4];
+        for (int q = 0; q < 4; q++) pv[q] = block_sum<BLOCK>((int64_t)prof[q], wsum);
         if (tid == 0) {
             atomicAdd(&a.counters[0], (unsigned long long)e);
-            atomicAdd(&a.counters[1], nsrc);
+            atomicAdd(&a.counters[1], (unsigned long long)ns);
             atomicAdd(&a.counters[3], (unsigned long long)x);
             atomicAdd(&a.counters[4], (unsigned long long)ei);
-            atomicAdd(&a.counters[5], prof[0]);
-            atomicAdd(&a.counters[6], nreuse);
-            atomicAdd(&a.counters[7], prof[1]);
-            atomicAdd(&a.counters[8], prof[2]);
-            atomicAdd(&a.counters[9], prof[3]);
+            atomicAdd(&a.counters[5], (unsigned long long)pv[0]);
+            atomicAdd(&a.counters[6], (unsigned long long)nr);
+            atomicAdd(&a.counters[7], (unsigned long long)pv[1]);
+            atomicAdd(&a.counters[8], (unsigned long long)pv[2]);
+            atomicAdd(&a.counters[9], (unsigned long long)pv[3]);
         }
     }
     grid.sync();
@@ -654,10 +698,10 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
             s1 += a.cnt[L + l];
             if (sn_flag(l)) last = max(last, l);
         }
-        int64_t t0 = block_sum<BLOCK>(s0, sh.warp);
-        int64_t t1 = block_sum<BLOCK>(s1, sh.warp);
+        int64_t t0 = block_sum<BLOCK>(s0, shs[0].warp);
+        int64_t t1 = block_sum<BLOCK>(s1, shs[0].warp);
         int64_t tl;
-        block_excl_max<BLOCK>(last, &tl, sh.warp);
+        block_excl_max<BLOCK>(last, &tl, shs[0].warp);
         if (tid == 0) {
             a.tile_sum[t] = t0;
             a.tile_sum[ntiles + t] = t1;
@@ -675,9 +719,9 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
             const int64_t v1 = t < ntiles ? a.tile_sum[ntiles + t] : 0;
             const int64_t vm = t < ntiles ? a.tile_last[t] : -1;
             int64_t tot0, tot1, totm;
-            const int64_t e0 = block_excl_scan<BLOCK>(v0, &tot0, sh.warp);
-            const int64_t e1 = block_excl_scan<BLOCK>(v1, &tot1, sh.warp);
-            const int64_t em = block_excl_max<BLOCK>(vm, &totm, sh.warp);
+            const int64_t e0 = block_excl_scan<BLOCK>(v0, &tot0, shs[0].warp);
+            const int64_t e1 = block_excl_scan<BLOCK>(v1, &tot1, shs[0].warp);
+            const int64_t em = block_excl_max<BLOCK>(vm, &totm, shs[0].warp);
             if (t < ntiles) {
                 a.tile_sum[t] = c0 + e0;
                 a.tile_sum[ntiles + t] = c1 + e1;
@@ -703,10 +747,10 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
             int64_t v1 = in ? a.cnt[L + l] : 0;
             bool f = in && sn_flag(l);
             int64_t tot0, tot1;
-            int64_t e0 = block_excl_scan<BLOCK>(v0, &tot0, sh.warp);
-            int64_t e1 = block_excl_scan<BLOCK>(v1, &tot1, sh.warp);
+            int64_t e0 = block_excl_scan<BLOCK>(v0, &tot0, shs[0].warp);
+            int64_t e1 = block_excl_scan<BLOCK>(v1, &tot1, shs[0].warp);
             int64_t sub_last;
-            int64_t rs = block_excl_max<BLOCK>(f ? l : -1, &sub_last, sh.warp);
+            int64_t rs = block_excl_max<BLOCK>(f ? l : -1, &sub_last, shs[0].warp);
             rs = max(max(rs, f ? l : (int64_t)-1), carry);
             bool start = false;
             if (in) {
@@ -715,7 +759,7 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
                 start = f || (a.max_sn > 0 && ((l - rs) % a.max_sn) == 0);
                 a.snind[l] = start ? 1 : 0;
             }
-            const int64_t ns = block_sum<BLOCK>(start ? 1 : 0, sh.warp);
+            const int64_t ns = block_sum<BLOCK>(start ? 1 : 0, shs[0].warp);
             carry = max(carry, sub_last);   // run start carried to the next sub-tile
             c0 += tot0; c1 += tot1; nsn += ns;
         }
@@ -730,7 +774,7 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
             const int64_t t = base + tid;
             int64_t v = t < ntiles ? a.tile_sn[t] : 0;
             int64_t tot;
-            int64_t e = block_excl_scan<BLOCK>(v, &tot, sh.warp);
+            int64_t e = block_excl_scan<BLOCK>(v, &tot, shs[0].warp);
             if (t < ntiles) a.tile_sn[t] = c + e;
             c += tot;
         }
@@ -746,7 +790,7 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
             const bool in = l < min(L, (t + 1) * TILE);
             int64_t v = (in && a.snind[l]) ? 1 : 0;
             int64_t tot;
-            int64_t e = block_excl_scan<BLOCK>(v, &tot, sh.warp);
+            int64_t e = block_excl_scan<BLOCK>(v, &tot, shs[0].warp);
             if (v) a.sn_list[c + e] = (int32_t)l;
             if (in && a.mat_info) {
                 const int mi = mat_of(l);

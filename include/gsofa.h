@@ -71,10 +71,14 @@ typedef struct gsofa_params {
     int64_t pool_capacity;      /* pattern entries kept on the device         */
     int32_t max_supernode_size; /* 0 or negative: unbounded                   */
     int32_t want_pattern;       /* 1: return u/l index arrays                 */
-    int32_t reuse;              /* 1: reuse traversal state along a chain of
-                                   sources s-1 -> s when s-1 is in adj(s);
-                                   0: every source starts from scratch;
-                                   -1 (default): automatic, currently 1       */
+    int32_t reuse;              /* -1 (default) or 1: a source reuses the
+                                   finished traversal of s-1 whenever s-1 is
+                                   reachable from s; the two passes of a
+                                   source run side by side in one CTA and
+                                   exchange the flags that decide it (when
+                                   two bitmaps fit, else as with 2);
+                                   2: reuse only when s-1 is in adj(s);
+                                   0: every source starts from scratch        */
     int32_t flags;              /* GSOFA_FLAG_* bits                          */
     int32_t part_count;         /* >1: process only the sources s with        */
     int32_t part_index;         /*     s % part_count == part_index (the

@@ -50,7 +50,11 @@ def test_grid3d_nd(ctx, side):
 @pytest.mark.parametrize("n", [500, 3000])
 def test_powerlaw(ctx, n):
     g = matgen.powerlaw(n, seed=n)
-    assert_same(ctx.symbfact(ctx.upload(g)), _oracle(g), where=f"powerlaw {n}")
+    ref = _oracle(g, 12)
+    m = ctx.upload(g)
+    for reuse in (-1, 2, 0):
+        r = ctx.symbfact(m, reuse=reuse, max_supernode_size=12)
+        assert_same(r, ref, where=f"powerlaw {n} reuse {reuse}")
 
 
 @pytest.mark.parametrize("seed", range(10))
@@ -71,7 +75,8 @@ def test_empty_and_tiny(ctx):
 
 @pytest.mark.parametrize("block,lanes,reuse,chunk,per_sm", [
     (128, 4, 0, 1, 0), (256, 8, 1, 7, 1), (512, 16, 1, 32, 0), (1024, 32, 0, 3, 0),
-    (256, 32, 1, 1, 2), (512, 8, 1, 200, 0), (128, 1, 0, 1, 0), (1024, 1, 1, 16, 1)])
+    (256, 32, 1, 1, 2), (512, 8, 1, 200, 0), (128, 1, 0, 1, 0), (1024, 1, 1, 16, 1),
+    (512, 1, 2, 32, 0), (256, 1, 2, 5, 0), (1024, 1, 2, 64, 1), (512, 1, -1, 3, 2)])
 def test_parameters_do_not_change_results(ctx, block, lanes, reuse, chunk, per_sm):
     g = matgen.grid3d(14, ordering="nd", drop_frac=0.1, seed=5)
     ref = _oracle(g, 8)
