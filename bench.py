@@ -50,9 +50,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["nd3d", "plain2d", "circuit", "bundled", "batch"],
+    ap.add_argument("--workload", choices=["nd3d", "plain2d", "circuit", "bundled", "batch", "serve"],
                     default="nd3d")
     ap.add_argument("--batch-count", type=int, default=256, help="matrices in the batch workload")
+    ap.add_argument("--serve-count", type=int, default=120, help="requests in the serving stream")
+    ap.add_argument("--serve-nmax", type=int, default=1_000_000, help="largest n of the serving stream")
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate (1/s)")
     ap.add_argument("--side", type=int, default=80, help="grid side of the nd3d workload")
     ap.add_argument("--reuse", type=int, default=-1,
                     help="reuse traversals along s-1 -> s chains (-1: library default, on)")
@@ -312,12 +315,64 @@ def batch_main(args):
     return 0
 
 
+def _make_graph(spec):
+    from gsofa_b200 import matgen
+    kind, n, seed = spec
+    return matgen.make(kind, n, seed)
+
+
+def serve_main(args):
+    """The serving stream: seeded Poisson arrivals of mixed-kind requests with
+    n log-uniform in [1,000, n_max], served by continuous batching under a
+    120 GB admission budget, then the same stream one request per launch."""
+    import multiprocessing as mp
+    import torch
+    import gsofa_b200
+    from gsofa_b200 import matgen, serve
+
+    spec = matgen.mixed_spec(args.serve_count, 1000, args.serve_nmax, matgen.SEEDS["serve"])
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        graphs = pool.map(_make_graph, spec)
+    rng = np.random.default_rng(matgen.SEEDS["serve"] + 1)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, size=len(graphs)))
+    reqs = [serve.Request(i, float(a), g) for i, (a, g) in enumerate(zip(arrivals, graphs))]
+    torch.cuda.set_device(0)
+    ctx = gsofa_b200.Context(0)
+    params = gsofa_b200.Params.default(want_pattern=0)
+    srv = serve.Server(ctx, params, mem_budget_bytes=120 << 30)
+    # warm the launch shapes on a few small requests
+    srv.run([serve.Request(-1, 0.0, g) for g in sorted(graphs, key=lambda g: g.n)[:4]])
+    with ClockSampler(0) as clk:
+        cont = srv.run(reqs)
+    single = serve.one_at_a_time(ctx, reqs, params)
+    for a, b in zip(cont["completions"], single["completions"]):
+        assert (a.result.fill_count, a.result.nnz_lu, a.result.n_supernodes) == \
+               (b.result.fill_count, b.result.nnz_lu, b.result.n_supernodes)
+    rep, one = cont["report"], single["report"]
+    line = {
+        "metric": "nnz(L+U)/s", "value": rep["nnz_lu_per_s"], "unit": "nnz/s", "n_gpus": 1,
+        "steps": 1, "warmup": 1, "ms_per_step": rep["span_s"] * 1000.0, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator)",
+        "config": {"workload": f"serve_{len(reqs)}_poisson_{args.serve_rate:g}hz_n1k-{args.serve_nmax}",
+                   "requests": len(reqs), "admission_budget_gb": 120, "pattern": "counts only",
+                   "seed": matgen.SEEDS["serve"]},
+        "serving": rep, "one_at_a_time": one,
+        "factorizations_per_s": rep["factorizations_per_s"],
+        "clocks": clk.summary(), "gpu_launches": rep["launches"],
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return reference_arm(args)
     if args.workload == "batch":
         return batch_main(args)
+    if args.workload == "serve":
+        return serve_main(args)
 
     import torch
     import torch.distributed as dist

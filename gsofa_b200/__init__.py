@@ -102,6 +102,7 @@ class _CResult(ctypes.Structure):
         ("l_col_count", _i32p),
         ("l_row_count", _i32p),
         ("sn_start", _i32p),
+        ("line_flags", ctypes.POINTER(ctypes.c_uint8)),
         ("u_ptr", _i64p),
         ("u_idx", _i32p),
         ("l_ptr", _i64p),
@@ -137,6 +138,7 @@ class Result:
     l_col_count: Optional[np.ndarray] = None
     l_row_count: Optional[np.ndarray] = None
     sn_start: Optional[np.ndarray] = None
+    line_flags: Optional[np.ndarray] = None
     u_ptr: Optional[np.ndarray] = None
     u_idx: Optional[np.ndarray] = None
     l_ptr: Optional[np.ndarray] = None
@@ -193,6 +195,9 @@ def lib():
                                                 vp, vp, vp, ctypes.c_int32, vp, vp, vp,
                                                 ctypes.POINTER(ctypes.c_uint64)]
     L.gsofa_symbfact_counts_noalloc.restype = ctypes.c_int
+    L.gsofa_supernodes_from_lines.argtypes = [ctypes.c_int32, _i32p, ctypes.POINTER(ctypes.c_uint8),
+                                              ctypes.c_int32, _i32p]
+    L.gsofa_supernodes_from_lines.restype = ctypes.c_int32
     L.gsofa_predict_scratch_bytes.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(Params)]
     L.gsofa_predict_scratch_bytes.restype = ctypes.c_size_t
     L.gsofa_symbfact_min_id.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.c_int,
@@ -227,6 +232,7 @@ def _convert(r: _CResult) -> Result:
     out.l_col_count = _arr(r.l_col_count, n, np.int32)
     out.l_row_count = _arr(r.l_row_count, n, np.int32)
     out.sn_start = _arr(r.sn_start, int(r.n_supernodes), np.int32)
+    out.line_flags = _arr(r.line_flags, n, np.uint8)
     out.u_ptr = _arr(r.u_ptr, n + 1, np.int64)
     out.l_ptr = _arr(r.l_ptr, n + 1, np.int64)
     out.u_idx = _arr(r.u_idx, int(r.nnz_u), np.int32)
@@ -419,10 +425,24 @@ def symbfact_counts_noalloc(device: int, stream: int, n: int, nnz: int, d_beg: i
     return int(summary[0]), int(summary[1]), int(summary[2])
 
 
+def supernodes_from_lines(u_row_count, line_flags, max_supernode_size: int = 0) -> np.ndarray:
+    """Supernode starts from per-line U row counts and link flags (host)."""
+    u = np.ascontiguousarray(u_row_count, dtype=np.int32)
+    f = np.ascontiguousarray(line_flags, dtype=np.uint8)
+    n = u.shape[0]
+    out = np.zeros(max(n, 1), np.int32)
+    k = lib().gsofa_supernodes_from_lines(n, u.ctypes.data_as(_i32p),
+                                          f.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+                                          int(max_supernode_size), out.ctypes.data_as(_i32p))
+    if k < 0:
+        raise GsofaError(1, "gsofa_supernodes_from_lines")
+    return out[:k].copy()
+
+
 def exported_symbols() -> List[str]:
     """Names of the C ABI entry points declared in include/gsofa.h."""
     return ["gsofa_symbfact_min_id", "gsofa_status_str", "gsofa_abi_version", "gsofa_default_params",
             "gsofa_create", "gsofa_destroy", "gsofa_set_stream", "gsofa_read_text", "gsofa_free", "gsofa_upload",
             "gsofa_matrix_free", "gsofa_matrix_n", "gsofa_symbfact", "gsofa_symbfact_batch",
             "gsofa_result_free", "gsofa_result_fetch", "gsofa_predict_scratch_bytes",
-            "gsofa_symbfact_counts_noalloc"]
+            "gsofa_symbfact_counts_noalloc", "gsofa_supernodes_from_lines"]

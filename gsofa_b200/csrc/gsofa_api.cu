@@ -182,6 +182,8 @@ void free_result_arrays(gsofa_result *r)
     std::free(r->l_col_count);
     std::free(r->l_row_count);
     std::free(r->sn_start);
+    std::free(r->line_flags);
+    r->line_flags = nullptr;
     std::free(r->u_ptr);
     std::free(r->u_idx);
     std::free(r->l_ptr);
@@ -502,6 +504,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
             }
         }
         const bool download_lines = !(p.flags & GSOFA_FLAG_NO_DOWNLOAD);
+        std::vector<uint8_t *> lflags;
         for (int i = 0; i < count; i++) {
             const int64_t lb = md[i].line_base, n = md[i].n;
             gsofa_result &r = out[i];
@@ -527,6 +530,9 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
                 r.l_col_count = download(st, d_cnt, L + lb, n);
                 if (want_pattern) r.l_row_count = download(st, d_lrow, lb, n);
                 r.sn_start = download(st, d_sn, ss[i], r.n_supernodes);
+                // link flags: bit 0 from pass G, bit 1 from pass G^T (merged below)
+                r.line_flags = download(st, d_nxt, lb, n);
+                lflags.push_back(download(st, d_nxt, L + lb, n));
                 if (want_pattern) {
                     r.u_ptr = download(st, d_gptr, lb, n + 1);
                     r.l_ptr = download(st, d_gptr, (L + 1) + lb, n + 1);
@@ -549,6 +555,9 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         for (int i = 0; i < count && download_lines; i++) {
             gsofa_result &r = out[i];
             const int64_t lb = md[i].line_base, n = md[i].n;
+            for (int64_t q = 0; q < n; q++) r.line_flags[q] = (uint8_t)(r.line_flags[q] | (lflags[i][q] << 1));
+            std::free(lflags[i]);
+            lflags[i] = nullptr;
             for (int32_t k = 0; k < r.n_supernodes; k++) r.sn_start[k] -= (int32_t)lb;
             if (want_pattern) {
                 const int64_t u0 = r.u_ptr[0], l0 = r.l_ptr[0];
@@ -943,6 +952,26 @@ gsofa_status gsofa_result_fetch(gsofa_ctx *c, const gsofa_result *r, int32_t *u_
         return fail_cuda(f.e);
     }
     return GSOFA_OK;
+}
+
+int32_t gsofa_supernodes_from_lines(int32_t n, const int32_t *ucnt, const uint8_t *flags,
+                                    int32_t max_size, int32_t *sn_start)
+{
+    if (n < 0 || (n > 0 && (!ucnt || !flags || !sn_start))) return -1;
+    int32_t k = 0, run = 0;
+    for (int32_t s = 0; s < n; s++) {
+        // lines s-1 and s are linked when s-1 is in line s (bit 1 of s-1),
+        // s is in line s-1 (bit 0 of s-1) and U row s is U row s-1 minus s
+        const bool linked = s > 0 && (flags[s - 1] & 2) && (flags[s - 1] & 1) &&
+                            ucnt[s] == ucnt[s - 1] - 1;
+        if (linked && (max_size <= 0 || run < max_size)) {
+            run++;
+        } else {
+            sn_start[k++] = s;
+            run = 1;
+        }
+    }
+    return k;
 }
 
 size_t gsofa_predict_scratch_bytes(const gsofa_ctx *c, int32_t n, int64_t nnz,

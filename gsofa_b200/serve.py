@@ -1,0 +1,154 @@
+"""Serving loop: symbolic factorizations as a request stream on one GPU.
+
+Requests (matrices) arrive over time.  The loop keeps every admitted
+request's CSR and scratch resident on the device and runs continuous
+batching at launch granularity: whenever the GPU finishes a persistent
+launch, every request that has arrived in the meantime and fits the memory
+budget is uploaded and joins the next launch, so the work of all of them
+overlaps on the device.  Admission is by predicted device bytes: the
+matrix's own storage plus the per-line state and the frontier queues of the
+launch (n x concurrent sources x per-source state, from
+gsofa_predict_scratch_bytes).  A request whose result is delivered releases
+its bytes.
+
+Latency is measured per request from its arrival to the moment its result is
+on the host; the report gives p50/p99 and sustained factorizations/s, and
+`one_at_a_time` runs the same stream with batches of one for comparison.
+Every result is the same whether the request ran alone or in a mix (the
+launch processes each matrix independently; the test-suite checks it).
+"""
+from __future__ import annotations
+
+import collections
+import dataclasses
+import time
+from typing import Callable, Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import Context, Params, Result
+from .matgen import Graph
+
+
+@dataclasses.dataclass
+class Request:
+    rid: int
+    arrival_s: float          # offset from the start of the stream
+    graph: Graph
+
+
+@dataclasses.dataclass
+class Completion:
+    rid: int
+    arrival_s: float
+    start_s: float            # when its launch began
+    done_s: float             # when its result was on the host
+    result: Result
+
+    @property
+    def latency_s(self) -> float:
+        return self.done_s - self.arrival_s
+
+
+def matrix_bytes(g: Graph) -> int:
+    """Device bytes of an uploaded matrix: G and G^T (int32 CSR) plus the
+    per-line counts kept with it."""
+    return 8 * (g.n + 1) + 8 * g.nnz + 12 * g.n
+
+
+class Server:
+    """Continuous-batching factorization server on one device."""
+
+    def __init__(self, ctx: Context, params: Optional[Params] = None,
+                 mem_budget_bytes: int = 120 << 30, max_batch: int = 64,
+                 max_lines_per_launch: int = 4_000_000):
+        self.ctx = ctx
+        self.params = params if params is not None else Params.default(want_pattern=0)
+        self.budget = int(mem_budget_bytes)
+        self.max_batch = int(max_batch)
+        self.max_lines = int(max_lines_per_launch)
+
+    def predicted_bytes(self, g: Graph) -> int:
+        return matrix_bytes(g) + self.ctx.predict_scratch_bytes(g.n, g.nnz, self.params)
+
+    def run(self, requests: Sequence[Request], clock: Callable[[], float] = time.perf_counter,
+            on_result: Optional[Callable[[Completion], None]] = None) -> Dict:
+        """Serves `requests` (sorted by arrival) in real time; returns the
+        report and the completions (with results)."""
+        reqs = sorted(requests, key=lambda r: r.arrival_s)
+        for r in reqs:
+            if self.predicted_bytes(r.graph) > self.budget:
+                raise ValueError(f"request {r.rid} (n={r.graph.n}) exceeds the memory budget by itself")
+        t0 = clock()
+        now = lambda: clock() - t0  # noqa: E731
+        pending = collections.deque(reqs)   # not yet arrived
+        waiting: collections.deque = collections.deque()
+        done: List[Completion] = []
+        launches = 0
+        batch_sizes: List[int] = []
+        in_use = 0
+        while pending or waiting:
+            t = now()
+            while pending and pending[0].arrival_s <= t:
+                waiting.append(pending.popleft())
+            if not waiting:
+                # idle: sleep until the next arrival
+                time.sleep(max(0.0, min(pending[0].arrival_s - t, 0.05)))
+                continue
+            # admit in arrival order while the budget and the launch size allow
+            batch: List[Request] = []
+            lines = 0
+            in_use = 0
+            while waiting and len(batch) < self.max_batch:
+                r = waiting[0]
+                b = self.predicted_bytes(r.graph)
+                if batch and (in_use + b > self.budget or lines + r.graph.n > self.max_lines):
+                    break
+                waiting.popleft()
+                batch.append(r)
+                in_use += b
+                lines += r.graph.n
+            start = now()
+            mats = [self.ctx.upload(r.graph) for r in batch]
+            results = self.ctx.symbfact_batch(mats, self.params)
+            for m in mats:
+                m.free()          # releases the request's bytes
+            fin = now()
+            launches += 1
+            batch_sizes.append(len(batch))
+            for r, res in zip(batch, results):
+                c = Completion(r.rid, r.arrival_s, start, fin, res)
+                done.append(c)
+                if on_result:
+                    on_result(c)
+        lat = np.array([c.latency_s for c in done])
+        span = max(c.done_s for c in done) - min(c.arrival_s for c in done) if done else 0.0
+        report = {
+            "requests": len(done),
+            "launches": launches,
+            "mean_batch": float(np.mean(batch_sizes)) if batch_sizes else 0.0,
+            "p50_ms": float(np.percentile(lat, 50) * 1000) if len(lat) else None,
+            "p99_ms": float(np.percentile(lat, 99) * 1000) if len(lat) else None,
+            "mean_ms": float(lat.mean() * 1000) if len(lat) else None,
+            "factorizations_per_s": len(done) / span if span > 0 else None,
+            "nnz_lu_per_s": sum(c.result.nnz_lu for c in done) / span if span > 0 else None,
+            "span_s": span,
+        }
+        return {"report": report, "completions": sorted(done, key=lambda c: c.rid)}
+
+
+def one_at_a_time(ctx: Context, requests: Sequence[Request], params: Optional[Params] = None,
+                  clock: Callable[[], float] = time.perf_counter) -> Dict:
+    """The same stream served one request per launch (no batching)."""
+    srv = Server(ctx, params, max_batch=1)
+    return srv.run(requests, clock)
+
+
+def make_stream(count: int, n_lo: int, n_hi: int, rate_hz: float, seed: int,
+                build: Callable[[str, int, int], Graph]) -> List[Request]:
+    """A seeded Poisson stream of `count` requests of the mixed kinds."""
+    from . import matgen
+    spec = matgen.mixed_spec(count, n_lo, n_hi, seed)
+    rng = np.random.default_rng(seed + 1)
+    t = np.cumsum(rng.exponential(1.0 / rate_hz, size=count))
+    return [Request(i, float(a), build(k, n, s)) for i, (a, (k, n, s)) in enumerate(zip(t, spec))]

@@ -120,6 +120,8 @@ typedef struct gsofa_result {
     int32_t *l_col_count;    /* [n] |L column j|                            */
     int32_t *l_row_count;    /* [n] |L row s| (with want_pattern only)      */
     int32_t *sn_start;       /* [n_supernodes] first line of each supernode */
+    uint8_t *line_flags;     /* [n] bit 0: s+1 in U row s; bit 1: s+1 in
+                                L column s (the supernode link flags)       */
     /* pattern (host, library-owned; NULL unless want_pattern) */
     int64_t *u_ptr;          /* [n+1] */
     int32_t *u_idx;          /* [nnz_u] */
@@ -194,6 +196,14 @@ gsofa_status gsofa_result_fetch(gsofa_ctx *ctx, const gsofa_result *r,
                                 int32_t *l_row_count, int32_t *sn_start,
                                 int64_t *u_ptr, int32_t *u_idx,
                                 int64_t *l_ptr, int32_t *l_idx);
+
+/* Supernode partition from per-line U row counts and link flags (as in
+ * gsofa_result), computed on the host: used to finish a factorization whose
+ * lines were computed in partitions (on several GPUs) and summed.  Writes the
+ * starts to sn_start (capacity n) and returns their number (-1: bad input). */
+int32_t gsofa_supernodes_from_lines(int32_t n, const int32_t *u_row_count,
+                                    const uint8_t *line_flags,
+                                    int32_t max_supernode_size, int32_t *sn_start);
 
 /* Device scratch bytes a factorization of an n-line, nnz-entry matrix needs
  * with these parameters, excluding the pattern pool (admission control). */

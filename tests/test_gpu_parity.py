@@ -220,3 +220,26 @@ def test_autotune_choice_is_cached_and_exact(ctx, tmp_path):
     assert rep2["cached"] and rep2["choice"] == rep["choice"]
     for g, r in zip(gs, ctx.symbfact_batch(ms, best2)):
         assert_same(r, _oracle(g), where=f"autotuned {g.name}")
+
+
+def test_sharded_partitions_assemble_on_one_gpu(ctx):
+    """The multi-GPU assembly with three partitions run one after another on
+    this GPU: summing their per-line arrays gives the full factorization."""
+    from gsofa_b200 import distributed
+    g = bundled()
+    m = ctx.upload(g)
+    world = 3
+    parts = []
+    for rank in range(world):
+        r = ctx.symbfact(m, want_pattern=0, part_count=world, part_index=rank)
+        parts.append(np.concatenate([r.u_row_count.astype(np.int64), r.l_col_count.astype(np.int64),
+                                     r.line_flags.astype(np.int64), [r.fill_count]]))
+    total = np.sum(parts, axis=0)
+    out = distributed.combine(g.n, parts[0][:g.n], parts[0][g.n:2 * g.n], parts[0][2 * g.n:3 * g.n],
+                              int(parts[0][-1]), lambda x: total, max_supernode_size=8)
+    ref = _oracle(g, 8, pattern=False)
+    assert out["fill_count"] == ref["fill_count"] and out["nnz_lu"] == ref["nnz_lu"]
+    assert np.array_equal(out["u_row_count"], ref["u_row_count"])
+    assert np.array_equal(out["sn_start"], ref["sn_start"])
+    full = ctx.symbfact(m, want_pattern=0, max_supernode_size=8)
+    assert np.array_equal(full.line_flags, out["line_flags"])
