@@ -463,12 +463,20 @@ def main():
         f0 = torch.cuda.Event(enable_timing=True)
         f1 = torch.cuda.Event(enable_timing=True)
         f0.record(stream)
+        phases = {"upload_ms": 0.0, "factor_and_fetch_ms": 0.0, "free_ms": 0.0}
         for i in range(k2):
             if i:
                 flush.fill_(i & 0xff)
+            h0 = time.perf_counter()
             mm = ctx.upload(pb.numpy(), pe.numpy(), pa.numpy())
+            h1 = time.perf_counter()
             out = ctx.symbfact_into(mm, pe2e, bufs)
+            h2 = time.perf_counter()
             mm.free()
+            h3 = time.perf_counter()
+            phases["upload_ms"] += 1000 * (h1 - h0) / k2
+            phases["factor_and_fetch_ms"] += 1000 * (h2 - h1) / k2
+            phases["free_ms"] += 1000 * (h3 - h2) / k2
         f1.record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -483,7 +491,8 @@ def main():
         if want_pattern:
             d2h += 4 * (out.nnz_u + out.nnz_l) + 2 * 8 * (g.n + 1)
         e2e = {"value": world * k2 * nnz_lu / (te / 1000.0), "unit": "nnz/s", "steps": k2,
-               "ms_per_step": te / k2, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+               "ms_per_step": te / k2, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "host_phases": phases, "kernel_ms": out.kernel_ms}
 
     # ---- roofline of the factorization kernel --------------------------------
     # Algorithmic bytes follow the per-source traversal model: every source
