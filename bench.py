@@ -339,15 +339,21 @@ def serve_main(args):
     torch.cuda.set_device(0)
     ctx = gsofa_b200.Context(0)
     params = gsofa_b200.Params.default(want_pattern=0)
-    srv = serve.Server(ctx, params, mem_budget_bytes=120 << 30)
-    # warm the launch shapes on a few small requests
-    srv.run([serve.Request(-1, 0.0, g) for g in sorted(graphs, key=lambda g: g.n)[:4]])
+    srv = gsofa_b200.StreamServer(0, mem_budget_bytes=120 << 30)
+    oversize = lambda g: ctx.symbfact(ctx.upload(g), params)  # noqa: E731
+    cs = serve.ContinuousServer(srv, oversize=oversize, max_n=srv.max_n)
+    # warm up on a few small requests
+    cs.run([serve.Request(-1, 0.0, g) for g in sorted(graphs, key=lambda g: g.n)[:4]])
     with ClockSampler(0) as clk:
-        cont = srv.run(reqs)
+        cont = cs.run(reqs)
+    srv.drain()
+    srv.close()
+    launch = serve.Server(ctx, params, mem_budget_bytes=120 << 30).run(reqs)
     single = serve.one_at_a_time(ctx, reqs, params)
-    for a, b in zip(cont["completions"], single["completions"]):
+    for a, b, c in zip(cont["completions"], single["completions"], launch["completions"]):
         assert (a.result.fill_count, a.result.nnz_lu, a.result.n_supernodes) == \
-               (b.result.fill_count, b.result.nnz_lu, b.result.n_supernodes)
+               (b.result.fill_count, b.result.nnz_lu, b.result.n_supernodes) == \
+               (c.result.fill_count, c.result.nnz_lu, c.result.n_supernodes)
     rep, one = cont["report"], single["report"]
     line = {
         "metric": "nnz(L+U)/s", "value": rep["nnz_lu_per_s"], "unit": "nnz/s", "n_gpus": 1,
@@ -356,9 +362,10 @@ def serve_main(args):
         "config": {"workload": f"serve_{len(reqs)}_poisson_{args.serve_rate:g}hz_n1k-{args.serve_nmax}",
                    "requests": len(reqs), "admission_budget_gb": 120, "pattern": "counts only",
                    "seed": matgen.SEEDS["serve"]},
-        "serving": rep, "one_at_a_time": one,
+        "serving": rep, "one_at_a_time": one, "launch_batching": launch["report"],
+        "serving_kernel_max_n": cs.max_n,
         "factorizations_per_s": rep["factorizations_per_s"],
-        "clocks": clk.summary(), "gpu_launches": rep["launches"],
+        "clocks": clk.summary(), "gpu_launches": None,
     }
     print(json.dumps(line), flush=True)
     ctx.close()

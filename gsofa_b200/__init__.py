@@ -33,8 +33,9 @@ OK = 0
 STATUS_NAMES = {
     0: "ok", 1: "invalid input", 2: "out of memory", 3: "queue or pattern pool overflow",
     4: "device wait timed out", 5: "CUDA error", 6: "input file error",
-    7: "unsupported device or size",
+    7: "unsupported device or size", 8: "no room for the request now",
 }
+BUSY = 8
 
 FLAG_NO_DOWNLOAD = 0x1
 FLAG_DEVICE_TIMING = 0x2
@@ -79,6 +80,21 @@ class Params(ctypes.Structure):
 
 _i32p = ctypes.POINTER(ctypes.c_int32)
 _i64p = ctypes.POINTER(ctypes.c_int64)
+
+
+class ServerConfig(ctypes.Structure):
+    """gsofa_server_config; zero fields mean 'choose automatically'."""
+
+    _fields_ = [
+        ("device", ctypes.c_int32),
+        ("max_n", ctypes.c_int32),
+        ("mem_budget_bytes", ctypes.c_int64),
+        ("max_supernode_size", ctypes.c_int32),
+        ("src_chunk", ctypes.c_int32),
+        ("max_requests", ctypes.c_int32),
+        ("idle_exit_us", ctypes.c_int32),
+        ("max_n_out", ctypes.c_int32),
+    ]
 
 
 class _CResult(ctypes.Structure):
@@ -198,6 +214,22 @@ def lib():
     L.gsofa_supernodes_from_lines.argtypes = [ctypes.c_int32, _i32p, ctypes.POINTER(ctypes.c_uint8),
                                               ctypes.c_int32, _i32p]
     L.gsofa_supernodes_from_lines.restype = ctypes.c_int32
+    L.gsofa_server_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(ServerConfig)]
+    L.gsofa_server_create.restype = ctypes.c_int
+    L.gsofa_server_destroy.argtypes = [vp]
+    L.gsofa_server_destroy.restype = None
+    L.gsofa_server_drain.argtypes = [vp]
+    L.gsofa_server_drain.restype = ctypes.c_int
+    L.gsofa_server_request_bytes.argtypes = [vp, ctypes.c_int32, ctypes.c_int64]
+    L.gsofa_server_request_bytes.restype = ctypes.c_size_t
+    L.gsofa_server_submit.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, _i32p, _i32p, _i32p,
+                                      ctypes.POINTER(ctypes.c_int64)]
+    L.gsofa_server_submit.restype = ctypes.c_int
+    L.gsofa_server_poll.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int32,
+                                    ctypes.POINTER(ctypes.c_int32)]
+    L.gsofa_server_poll.restype = ctypes.c_int
+    L.gsofa_server_result.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(_CResult)]
+    L.gsofa_server_result.restype = ctypes.c_int
     L.gsofa_predict_scratch_bytes.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(Params)]
     L.gsofa_predict_scratch_bytes.restype = ctypes.c_size_t
     L.gsofa_symbfact_min_id.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.c_int,
@@ -368,6 +400,76 @@ class Context:
         return int(lib().gsofa_predict_scratch_bytes(self._h, int(n), int(nnz), ctypes.byref(p)))
 
 
+class StreamServer:
+    """A persistent-kernel factorization server (continuous batching).
+
+    submit() uploads a matrix and publishes its work to the running kernel;
+    it returns None when the request does not fit right now (poll, fetch
+    finished results, try again).  poll() lists finished request ids;
+    result() returns one (counts, line flags, supernodes, totals) and frees
+    its device memory."""
+
+    def __init__(self, device: int = 0, mem_budget_bytes: int = 0, max_n: int = 0,
+                 max_supernode_size: int = 0, src_chunk: int = 0, max_requests: int = 0,
+                 idle_exit_us: int = 0):
+        cfg = ServerConfig(device, max_n, mem_budget_bytes, max_supernode_size, src_chunk,
+                           max_requests, idle_exit_us, 0)
+        h = ctypes.c_void_p()
+        _check(lib().gsofa_server_create(ctypes.byref(h), ctypes.byref(cfg)), "gsofa_server_create")
+        self._h = h
+        self.max_n = int(cfg.max_n_out)
+        self._ids = (ctypes.c_int64 * 4096)()
+
+    def close(self) -> None:
+        if self._h:
+            lib().gsofa_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def drain(self) -> None:
+        """Waits until every published request is done and the kernel exited."""
+        _check(lib().gsofa_server_drain(self._h), "gsofa_server_drain")
+
+    def request_bytes(self, n: int, nnz: int) -> int:
+        return int(lib().gsofa_server_request_bytes(self._h, int(n), int(nnz)))
+
+    def submit(self, g: Graph) -> Optional[int]:
+        beg = np.ascontiguousarray(g.beg, dtype=np.int32)
+        end = np.ascontiguousarray(g.end, dtype=np.int32)
+        adj = np.ascontiguousarray(g.adj if g.nnz else np.zeros(1, np.int32), dtype=np.int32)
+        rid = ctypes.c_int64()
+        st = lib().gsofa_server_submit(self._h, g.n, g.nnz, beg.ctypes.data_as(_i32p), end.ctypes.data_as(_i32p),
+                                       adj.ctypes.data_as(_i32p), ctypes.byref(rid))
+        if st == BUSY:
+            return None
+        _check(st, "gsofa_server_submit")
+        return int(rid.value)
+
+    def poll(self) -> List[int]:
+        cnt = ctypes.c_int32()
+        _check(lib().gsofa_server_poll(self._h, self._ids, len(self._ids), ctypes.byref(cnt)), "gsofa_server_poll")
+        return [int(self._ids[i]) for i in range(cnt.value)]
+
+    def result(self, rid: int) -> Result:
+        r = _CResult()
+        _check(lib().gsofa_server_result(self._h, int(rid), ctypes.byref(r)), "gsofa_server_result")
+        try:
+            return _convert(r)
+        finally:
+            lib().gsofa_result_free(ctypes.byref(r))
+
+
 def read_text(beg_file: str, end_file: str, csr_file: str) -> Graph:
     """Reads the reference's colbeg/colend/csr text files through the library."""
     n = ctypes.c_int32()
@@ -445,4 +547,6 @@ def exported_symbols() -> List[str]:
             "gsofa_create", "gsofa_destroy", "gsofa_set_stream", "gsofa_read_text", "gsofa_free", "gsofa_upload",
             "gsofa_matrix_free", "gsofa_matrix_n", "gsofa_symbfact", "gsofa_symbfact_batch",
             "gsofa_result_free", "gsofa_result_fetch", "gsofa_predict_scratch_bytes",
-            "gsofa_symbfact_counts_noalloc", "gsofa_supernodes_from_lines"]
+            "gsofa_symbfact_counts_noalloc", "gsofa_supernodes_from_lines", "gsofa_server_create",
+            "gsofa_server_destroy", "gsofa_server_request_bytes", "gsofa_server_submit",
+            "gsofa_server_poll", "gsofa_server_result", "gsofa_server_drain"]

@@ -7,17 +7,21 @@
 // reference, nothing here exits the process; every failure is a status code.
 #include "../../include/gsofa.h"
 #include "gsofa_device.cuh"
+#include "gsofa_server.cuh"
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <chrono>
+#include <map>
+#include <unordered_map>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -611,6 +615,7 @@ const char *gsofa_status_str(gsofa_status s)
     case GSOFA_ERR_CUDA: return "CUDA error";
     case GSOFA_ERR_IO: return "input file error";
     case GSOFA_ERR_UNSUPPORTED: return "unsupported device or size";
+    case GSOFA_ERR_BUSY: return "no room for the request now";
     }
     return "unknown status";
 }
@@ -1278,3 +1283,509 @@ extern "C" gsofa_status gsofa_symbfact_counts_noalloc(int device, void *cuda_str
     }
     return GSOFA_OK;
 }
+
+// ============================================================================
+// Serving: persistent kernel fed by the host (gsofa_server_*).
+
+namespace {
+
+// First-fit allocator over [0, size) units, with coalescing frees.
+struct RangeAlloc {
+    std::map<int64_t, int64_t> free_;   // offset -> length
+    void init(int64_t size) { free_.clear(); if (size > 0) free_[0] = size; }
+    bool alloc(int64_t len, int64_t *off)
+    {
+        if (len <= 0) { *off = 0; return true; }
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second >= len) {
+                *off = it->first;
+                const int64_t rest = it->second - len, at = it->first + len;
+                free_.erase(it);
+                if (rest > 0) free_[at] = rest;
+                return true;
+            }
+        }
+        return false;
+    }
+    void release(int64_t off, int64_t len)
+    {
+        if (len <= 0) return;
+        auto it = free_.emplace(off, len).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+};
+
+constexpr int64_t kArenaUnit = 256;   // bytes
+inline int64_t units(int64_t bytes) { return (bytes + kArenaUnit - 1) / kArenaUnit; }
+
+struct ServerReq {
+    int slot = -1;
+    int32_t n = 0;
+    int64_t nnz = 0;
+    int64_t lb = 0;                 // first line in the line arena
+    int64_t g_off = 0, g_units = 0; // graph region in the arena
+    uint64_t npieces = 0;
+    uint64_t orig_up = 0, orig_lo = 0;
+    bool done = false;
+};
+
+}  // namespace
+
+struct gsofa_server {
+    int device = 0, sms = 0;
+    size_t optin = 0;
+    int32_t max_n = 0;
+    int32_t max_sn = 0;
+    int32_t chunk = 32;
+    int32_t max_slots = 4096;
+    int idle_spins = 10000;
+    int block = 512, ring = 1024, grid = 0;
+    int32_t bitmap_words = 0;
+    size_t smem = 0;
+    cudaStream_t run = nullptr, io = nullptr;
+    ServeCtl *d_ctl = nullptr;
+    ServePiece *d_pieces = nullptr;
+    unsigned long long piece_cap = 1ull << 20;
+    MatDesc *d_slots = nullptr;
+    unsigned int *d_done = nullptr;
+    int32_t *d_cnt = nullptr;
+    uint8_t *d_nxt = nullptr;
+    int64_t lmax = 0;
+    int32_t *d_queue = nullptr;
+    uint32_t *d_status = nullptr;
+    char *d_arena = nullptr;
+    int64_t arena_units = 0;
+    RangeAlloc arena, lines;
+    std::vector<int> free_slots;
+    std::unordered_map<int64_t, ServerReq> reqs;
+    std::vector<unsigned int> h_done;
+    int64_t next_id = 1;
+    unsigned long long published = 0;
+    unsigned long long taken_seen = 0;
+};
+
+namespace {
+
+// Bytes of a request's resident graph: G and G^T offsets and ids, per-line
+// originals and input degrees.
+int64_t server_graph_bytes(int32_t n, int64_t nnz)
+{
+    const int64_t a = 256;
+    auto r = [&](int64_t b) { return (b + a - 1) / a * a; };
+    return 2 * r(4 * ((int64_t)n + 1)) + 2 * r(4 * std::max<int64_t>(nnz, 1)) + 3 * r(4 * std::max<int32_t>(n, 1));
+}
+
+// Upload staging: input copy, degree arrays, scan partials, counters.
+int64_t server_staging_bytes(int32_t n, int64_t nnz)
+{
+    const int64_t a = 256;
+    auto r = [&](int64_t b) { return (b + a - 1) / a * a; };
+    const int64_t scan_tiles = ((int64_t)n + 1 + 255) / 256 + 1;
+    return 2 * r(4 * std::max<int32_t>(n, 1)) + r(4 * std::max<int64_t>(nnz, 1)) + 3 * r(4 * ((int64_t)n + 1)) +
+           r(8 * 2 * scan_tiles) + r(64);
+}
+
+gsofa_status server_launch_if_idle(gsofa_server *s)
+{
+    const cudaError_t q = cudaStreamQuery(s->run);
+    if (q == cudaErrorNotReady) return GSOFA_OK;
+    if (q != cudaSuccess) return fail_cuda(q);
+    ServeArgs sa{};
+    JobArgs &a = sa.job;
+    a.queue = s->d_queue;
+    a.qcap = s->max_n;
+    a.bitmap_words = s->bitmap_words;
+    a.ring_size = s->ring;
+    a.lanes = 1;
+    a.reuse = 1;
+    a.want_pattern = 0;
+    a.L = s->lmax;
+    a.cnt = s->d_cnt;
+    a.nxt = s->d_nxt;
+    a.status = s->d_status;
+    sa.ctl = s->d_ctl;
+    sa.pieces = s->d_pieces;
+    sa.piece_cap = s->piece_cap;
+    sa.slots = s->d_slots;
+    sa.slot_done = s->d_done;
+    sa.idle_spins = s->idle_spins;
+    serve_kernel<512><<<s->grid, 512, s->smem, s->run>>>(sa);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? GSOFA_OK : fail_cuda(e);
+}
+
+void server_release(gsofa_server *s, ServerReq &r)
+{
+    if (r.slot >= 0) s->free_slots.push_back(r.slot);
+    s->lines.release(r.lb, r.n);
+    s->arena.release(r.g_off, r.g_units);
+    r.slot = -1;
+}
+
+}  // namespace
+
+extern "C" {
+
+gsofa_status gsofa_server_create(gsofa_server **out, gsofa_server_config *cfg)
+{
+    if (!out || !cfg) return GSOFA_ERR_INVALID_INPUT;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return GSOFA_ERR_UNSUPPORTED;
+    }
+    if (cfg->device < 0 || cfg->device >= ndev) return GSOFA_ERR_INVALID_INPUT;
+    gsofa_server *s = new (std::nothrow) gsofa_server();
+    if (!s) return GSOFA_ERR_OOM;
+    try {
+        s->device = cfg->device;
+        GS_CUDA(cudaSetDevice(s->device));
+        cudaDeviceProp prop;
+        GS_CUDA(cudaGetDeviceProperties(&prop, s->device));
+        if (prop.major < 10) { delete s; return GSOFA_ERR_UNSUPPORTED; }
+        s->sms = prop.multiProcessorCount;
+        s->optin = prop.sharedMemPerBlockOptin;
+        const size_t static_smem = 2 * sizeof(SharedState) + 1024;
+        const int32_t limit_n =
+            (int32_t)std::min<int64_t>(((int64_t)(s->optin - static_smem) / 2 - 1024 * 4) / 4 / 4 * 4 * 32, INT32_MAX);
+        s->max_n = cfg->max_n > 0 ? cfg->max_n : limit_n;
+        if (s->max_n > limit_n || s->max_n <= 0) { delete s; return GSOFA_ERR_UNSUPPORTED; }
+        s->max_sn = cfg->max_supernode_size;
+        s->chunk = cfg->src_chunk > 0 ? cfg->src_chunk : 32;
+        s->max_slots = cfg->max_requests > 0 ? cfg->max_requests : 4096;
+        s->idle_spins = std::max(1, (cfg->idle_exit_us > 0 ? cfg->idle_exit_us : 20000) / 2);
+        s->bitmap_words = ((s->max_n + 31) / 32 + 3) / 4 * 4;
+        // frontier ring: the largest that fits beside the two bitmaps
+        void *kfn = (void *)serve_kernel<512>;
+        s->ring = 0;
+        for (int cand = 8192; cand >= 1024; cand >>= 1) {
+            const size_t sm = 2 * ((size_t)s->bitmap_words * 4 + (size_t)cand * 4);
+            if (sm + static_smem <= s->optin) { s->ring = cand; s->smem = sm; break; }
+        }
+        if (!s->ring) { delete s; return GSOFA_ERR_UNSUPPORTED; }
+        GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem));
+        int occ = 0;
+        GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, 512, s->smem));
+        if (occ <= 0) { delete s; return GSOFA_ERR_UNSUPPORTED; }
+        s->grid = s->sms;   // one CTA per SM leaves room for the upload kernels
+        GS_CUDA(cudaStreamCreateWithFlags(&s->run, cudaStreamNonBlocking));
+        GS_CUDA(cudaStreamCreateWithFlags(&s->io, cudaStreamNonBlocking));
+        size_t fr = 0, tot = 0;
+        GS_CUDA(cudaMemGetInfo(&fr, &tot));
+        const int64_t budget = cfg->mem_budget_bytes > 0 ? cfg->mem_budget_bytes : (int64_t)(0.9 * (double)fr);
+        s->lmax = std::max<int64_t>(4 * (int64_t)s->max_n, 1 << 24);
+        const int64_t fixed = (int64_t)s->grid * 2 * s->max_n * 4 + (int64_t)s->piece_cap * sizeof(ServePiece) +
+                              (int64_t)s->max_slots * (sizeof(MatDesc) + 4) + s->lmax * 10 + 4096;
+        s->arena_units = (budget - fixed) / kArenaUnit;
+        if (s->arena_units < units(server_graph_bytes(s->max_n, 8 * (int64_t)s->max_n))) {
+            gsofa_server_destroy(s);
+            return GSOFA_ERR_OOM;
+        }
+        GS_CUDA(cudaMalloc(&s->d_ctl, sizeof(ServeCtl) + 64));
+        s->d_status = (uint32_t *)((char *)s->d_ctl + sizeof(ServeCtl));
+        GS_CUDA(cudaMalloc(&s->d_pieces, s->piece_cap * sizeof(ServePiece)));
+        GS_CUDA(cudaMalloc(&s->d_slots, (size_t)s->max_slots * sizeof(MatDesc)));
+        GS_CUDA(cudaMalloc(&s->d_done, (size_t)s->max_slots * 4));
+        GS_CUDA(cudaMalloc(&s->d_cnt, (size_t)2 * s->lmax * 4));
+        GS_CUDA(cudaMalloc(&s->d_nxt, (size_t)2 * s->lmax));
+        GS_CUDA(cudaMalloc(&s->d_queue, (size_t)s->grid * 2 * s->max_n * 4));
+        GS_CUDA(cudaMalloc(&s->d_arena, (size_t)s->arena_units * kArenaUnit));
+        GS_CUDA(cudaMemsetAsync(s->d_ctl, 0, sizeof(ServeCtl) + 64, s->io));
+        GS_CUDA(cudaMemsetAsync(s->d_done, 0, (size_t)s->max_slots * 4, s->io));
+        GS_CUDA(cudaStreamSynchronize(s->io));
+        s->arena.init(s->arena_units);
+        s->lines.init(s->lmax);
+        for (int i = s->max_slots - 1; i >= 0; i--) s->free_slots.push_back(i);
+        s->h_done.assign((size_t)s->max_slots, 0u);
+    } catch (CudaFail &f) {
+        gsofa_server_destroy(s);
+        return fail_cuda(f.e);
+    }
+    cfg->max_n_out = s->max_n;
+    *out = s;
+    return GSOFA_OK;
+}
+
+gsofa_status gsofa_server_drain(gsofa_server *s)
+{
+    if (!s) return GSOFA_ERR_INVALID_INPUT;
+    try {
+        GS_CUDA(cudaSetDevice(s->device));
+        // every published piece is taken before CTAs go idle, so setting
+        // `stop` lets the kernel finish its work and then exit
+        const int32_t one = 1, zero = 0;
+        GS_CUDA(cudaMemcpyAsync(&s->d_ctl->stop, &one, 4, cudaMemcpyHostToDevice, s->io));
+        GS_CUDA(cudaStreamSynchronize(s->io));
+        GS_CUDA(cudaStreamSynchronize(s->run));
+        GS_CUDA(cudaMemcpyAsync(&s->d_ctl->stop, &zero, 4, cudaMemcpyHostToDevice, s->io));
+        GS_CUDA(cudaStreamSynchronize(s->io));
+    } catch (CudaFail &f) {
+        return fail_cuda(f.e);
+    }
+    return GSOFA_OK;
+}
+
+void gsofa_server_destroy(gsofa_server *s)
+{
+    if (!s) return;
+    cudaSetDevice(s->device);
+    if (s->d_ctl && s->io) {
+        const int32_t one = 1;
+        cudaMemcpyAsync(&s->d_ctl->stop, &one, 4, cudaMemcpyHostToDevice, s->io);
+        cudaStreamSynchronize(s->io);
+    }
+    if (s->run) cudaStreamSynchronize(s->run);   // idle CTAs see `stop` and exit
+    cudaFree(s->d_ctl);
+    cudaFree(s->d_pieces);
+    cudaFree(s->d_slots);
+    cudaFree(s->d_done);
+    cudaFree(s->d_cnt);
+    cudaFree(s->d_nxt);
+    cudaFree(s->d_queue);
+    cudaFree(s->d_arena);
+    if (s->run) cudaStreamDestroy(s->run);
+    if (s->io) cudaStreamDestroy(s->io);
+    delete s;
+}
+
+size_t gsofa_server_request_bytes(const gsofa_server *s, int32_t n, int64_t nnz)
+{
+    if (!s || n < 0 || nnz < 0) return 0;
+    return (size_t)(server_graph_bytes(n, nnz) + server_staging_bytes(n, nnz) + 10 * (int64_t)n);
+}
+
+gsofa_status gsofa_server_submit(gsofa_server *s, int32_t n, int64_t nnz, const int32_t *beg,
+                                 const int32_t *end, const int32_t *adj, int64_t *id)
+{
+    if (!s || !id || n <= 0 || nnz < 0 || nnz > INT32_MAX || !beg || !end || (nnz > 0 && !adj))
+        return GSOFA_ERR_INVALID_INPUT;
+    if (n > s->max_n) return GSOFA_ERR_UNSUPPORTED;
+    ServerReq r;
+    r.n = n;
+    r.nnz = nnz;
+    const uint64_t npieces = ((uint64_t)n + s->chunk - 1) / s->chunk;
+    if (s->free_slots.empty()) return GSOFA_ERR_BUSY;
+    if (s->published + npieces - s->taken_seen > s->piece_cap) return GSOFA_ERR_BUSY;
+    int64_t st_off = 0;
+    const int64_t st_units = units(server_staging_bytes(n, nnz));
+    r.g_units = units(server_graph_bytes(n, nnz));
+    if (!s->lines.alloc(n, &r.lb)) return GSOFA_ERR_BUSY;
+    if (!s->arena.alloc(r.g_units, &r.g_off)) {
+        s->lines.release(r.lb, n);
+        return GSOFA_ERR_BUSY;
+    }
+    if (!s->arena.alloc(st_units, &st_off)) {
+        s->lines.release(r.lb, n);
+        s->arena.release(r.g_off, r.g_units);
+        return GSOFA_ERR_BUSY;
+    }
+    r.slot = s->free_slots.back();
+    s->free_slots.pop_back();
+    gsofa_status status = GSOFA_OK;
+    try {
+        GS_CUDA(cudaSetDevice(s->device));
+        cudaStream_t st = s->io;
+        // carve the graph region and the staging region
+        char *gb = s->d_arena + r.g_off * kArenaUnit;
+        char *sb = s->d_arena + st_off * kArenaUnit;
+        auto take = [](char *&p, int64_t bytes) {
+            char *q = p;
+            p += (bytes + 255) / 256 * 256;
+            return q;
+        };
+        int32_t *gptr = (int32_t *)take(gb, 4 * ((int64_t)n + 1));
+        int32_t *tptr = (int32_t *)take(gb, 4 * ((int64_t)n + 1));
+        int32_t *gadj = (int32_t *)take(gb, 4 * std::max<int64_t>(nnz, 1));
+        int32_t *tadj = (int32_t *)take(gb, 4 * std::max<int64_t>(nnz, 1));
+        int32_t *orig_up = (int32_t *)take(gb, 4 * (int64_t)n);
+        int32_t *orig_lo = (int32_t *)take(gb, 4 * (int64_t)n);
+        int32_t *rawdeg = (int32_t *)take(gb, 4 * (int64_t)n);
+        const int64_t scan_tiles = ((int64_t)n + 1 + 255) / 256 + 1;
+        int32_t *d_beg = (int32_t *)take(sb, 4 * (int64_t)n);
+        int32_t *d_end = (int32_t *)take(sb, 4 * (int64_t)n);
+        int32_t *d_adj = (int32_t *)take(sb, 4 * std::max<int64_t>(nnz, 1));
+        int32_t *deg = (int32_t *)take(sb, 4 * ((int64_t)n + 1));
+        int32_t *indeg = (int32_t *)take(sb, 4 * ((int64_t)n + 1));
+        int32_t *tcur = (int32_t *)take(sb, 4 * ((int64_t)n + 1));
+        int64_t *tsum = (int64_t *)take(sb, 8 * 2 * scan_tiles);
+        unsigned long long *cnts = (unsigned long long *)take(sb, 64);
+
+        GS_CUDA(cudaMemcpyAsync(d_beg, beg, (size_t)n * 4, cudaMemcpyHostToDevice, st));
+        GS_CUDA(cudaMemcpyAsync(d_end, end, (size_t)n * 4, cudaMemcpyHostToDevice, st));
+        if (nnz > 0) GS_CUDA(cudaMemcpyAsync(d_adj, adj, (size_t)nnz * 4, cudaMemcpyHostToDevice, st));
+        GS_CUDA(cudaMemsetAsync(indeg, 0, (size_t)(n + 1) * 4, st));
+        GS_CUDA(cudaMemsetAsync(deg, 0, (size_t)(n + 1) * 4, st));
+        GS_CUDA(cudaMemsetAsync(orig_lo, 0, (size_t)n * 4, st));
+        GS_CUDA(cudaMemsetAsync(cnts, 0, 64, st));
+        UploadArgs u{};
+        u.n = n;
+        u.nnz = nnz;
+        u.beg = d_beg;
+        u.end = d_end;
+        u.adj = d_adj;
+        u.deg = deg;
+        u.indeg = indeg;
+        u.orig_up = orig_up;
+        u.orig_lo = orig_lo;
+        u.rawdeg = rawdeg;
+        u.counts = cnts;
+        u.status = (uint32_t *)(cnts + 4);
+        const int ugrid = (int)std::min<int64_t>(((int64_t)n * 32 + 255) / 256, (int64_t)s->sms * 16);
+        upload_count_kernel<<<ugrid, 256, 0, st>>>(u);
+        GS_CUDA(cudaGetLastError());
+        const int64_t ntl = ((int64_t)n + 255) / 256;
+        int32_t *scan_in[2] = {deg, indeg};
+        int32_t *scan_out[2] = {gptr, tptr};
+        for (int k = 0; k < 2; k++) {
+            int64_t *ts = tsum + k * scan_tiles;
+            int64_t *dt = (int64_t *)(cnts + 2 + k);
+            scan_tiles_kernel<256><<<(unsigned)ntl, 256, 0, st>>>(scan_in[k], n, ts);
+            scan_partials_kernel<256><<<1, 256, 0, st>>>(ts, ntl, dt);
+            scan_apply_kernel<256><<<(unsigned)ntl, 256, 0, st>>>(scan_in[k], n, ts, scan_out[k], dt);
+            GS_CUDA(cudaGetLastError());
+        }
+        unsigned long long hc[5];
+        GS_CUDA(cudaMemcpyAsync(hc, cnts, sizeof(hc), cudaMemcpyDeviceToHost, st));
+        GS_CUDA(cudaStreamSynchronize(st));
+        if ((uint32_t)(hc[4] & 0xffffffffu) & 1u) throw std::invalid_argument("input");
+        r.orig_up = hc[0];
+        r.orig_lo = hc[1];
+        GS_CUDA(cudaMemcpyAsync(tcur, tptr, (size_t)(n + 1) * 4, cudaMemcpyDeviceToDevice, st));
+        upload_fill_kernel<<<ugrid, 256, 0, st>>>(u, gptr, gadj, tcur, tadj);
+        GS_CUDA(cudaGetLastError());
+
+        // publish: descriptor, cleared counter, pieces, then the new total
+        MatDesc md{};
+        md.n = n;
+        md.line_base = r.lb;
+        md.g[0] = PassGraph{gptr, gadj};
+        md.g[1] = PassGraph{tptr, tadj};
+        md.rawdeg = rawdeg;
+        GS_CUDA(cudaMemcpyAsync(s->d_slots + r.slot, &md, sizeof(md), cudaMemcpyHostToDevice, st));
+        GS_CUDA(cudaMemsetAsync(s->d_done + r.slot, 0, 4, st));
+        std::vector<ServePiece> pcs((size_t)npieces);
+        for (uint64_t k = 0; k < npieces; k++) {
+            // highest sources first: they carry the largest traversals
+            const int64_t hi = (int64_t)n - (int64_t)k * s->chunk;
+            pcs[k] = ServePiece{r.slot, (int32_t)std::max<int64_t>(0, hi - s->chunk), (int32_t)hi, 0};
+        }
+        const uint64_t at = s->published % s->piece_cap;
+        const uint64_t first = std::min<uint64_t>(npieces, s->piece_cap - at);
+        GS_CUDA(cudaMemcpyAsync(s->d_pieces + at, pcs.data(), first * sizeof(ServePiece), cudaMemcpyHostToDevice, st));
+        if (first < npieces)
+            GS_CUDA(cudaMemcpyAsync(s->d_pieces, pcs.data() + first, (npieces - first) * sizeof(ServePiece),
+                                    cudaMemcpyHostToDevice, st));
+        const unsigned long long newpub = s->published + npieces;
+        GS_CUDA(cudaMemcpyAsync(&s->d_ctl->published, &newpub, 8, cudaMemcpyHostToDevice, st));
+        GS_CUDA(cudaStreamSynchronize(st));
+        s->published = newpub;
+        r.npieces = npieces;
+        s->h_done[(size_t)r.slot] = 0;
+    } catch (CudaFail &f) {
+        status = fail_cuda(f.e);
+    } catch (std::invalid_argument &) {
+        status = GSOFA_ERR_INVALID_INPUT;
+    }
+    s->arena.release(st_off, st_units);
+    if (status != GSOFA_OK) {
+        server_release(s, r);
+        return status;
+    }
+    const int64_t rid = s->next_id++;
+    s->reqs.emplace(rid, r);
+    *id = rid;
+    return server_launch_if_idle(s);
+}
+
+gsofa_status gsofa_server_poll(gsofa_server *s, int64_t *ids, int32_t capacity, int32_t *count)
+{
+    if (!s || !count || (capacity > 0 && !ids)) return GSOFA_ERR_INVALID_INPUT;
+    *count = 0;
+    try {
+        GS_CUDA(cudaSetDevice(s->device));
+        unsigned long long tk = 0;
+        GS_CUDA(cudaMemcpyAsync(s->h_done.data(), s->d_done, s->h_done.size() * 4, cudaMemcpyDeviceToHost, s->io));
+        GS_CUDA(cudaMemcpyAsync(&tk, &s->d_ctl->taken, 8, cudaMemcpyDeviceToHost, s->io));
+        GS_CUDA(cudaStreamSynchronize(s->io));
+        s->taken_seen = tk;
+        bool pending = false;
+        for (auto &kv : s->reqs) {
+            ServerReq &r = kv.second;
+            if (r.done) continue;
+            if (r.slot >= 0 && s->h_done[(size_t)r.slot] >= r.npieces) {
+                r.done = true;
+                if (*count < capacity) ids[(*count)++] = kv.first;
+            } else {
+                pending = true;
+            }
+        }
+        if (pending) return server_launch_if_idle(s);
+    } catch (CudaFail &f) {
+        return fail_cuda(f.e);
+    }
+    return GSOFA_OK;
+}
+
+gsofa_status gsofa_server_result(gsofa_server *s, int64_t id, gsofa_result *out)
+{
+    if (!s || !out) return GSOFA_ERR_INVALID_INPUT;
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end() || !it->second.done) return GSOFA_ERR_INVALID_INPUT;
+    ServerReq &r = it->second;
+    std::memset(out, 0, sizeof(*out));
+    const int64_t n = r.n;
+    try {
+        GS_CUDA(cudaSetDevice(s->device));
+        out->n = r.n;
+        out->u_row_count = (int32_t *)std::malloc((size_t)n * 4);
+        out->l_col_count = (int32_t *)std::malloc((size_t)n * 4);
+        out->line_flags = (uint8_t *)std::malloc((size_t)n);
+        std::vector<uint8_t> lf((size_t)n);
+        if (!out->u_row_count || !out->l_col_count || !out->line_flags) throw std::bad_alloc();
+        GS_CUDA(cudaMemcpyAsync(out->u_row_count, s->d_cnt + r.lb, n * 4, cudaMemcpyDeviceToHost, s->io));
+        GS_CUDA(cudaMemcpyAsync(out->l_col_count, s->d_cnt + s->lmax + r.lb, n * 4, cudaMemcpyDeviceToHost, s->io));
+        GS_CUDA(cudaMemcpyAsync(out->line_flags, s->d_nxt + r.lb, n, cudaMemcpyDeviceToHost, s->io));
+        GS_CUDA(cudaMemcpyAsync(lf.data(), s->d_nxt + s->lmax + r.lb, n, cudaMemcpyDeviceToHost, s->io));
+        GS_CUDA(cudaStreamSynchronize(s->io));
+        uint64_t su = 0, sl = 0;
+        for (int64_t q = 0; q < n; q++) {
+            su += (uint64_t)out->u_row_count[q];
+            sl += (uint64_t)out->l_col_count[q];
+            out->line_flags[q] = (uint8_t)(out->line_flags[q] | (lf[(size_t)q] << 1));
+        }
+        out->nnz_u = su;
+        out->nnz_l = sl;
+        out->nnz_lu = su + sl + (uint64_t)n;
+        out->fill_count = su + sl - r.orig_up - r.orig_lo;
+        std::vector<int32_t> sn((size_t)std::max<int64_t>(n, 1));
+        const int32_t k = gsofa_supernodes_from_lines(r.n, out->u_row_count, out->line_flags, s->max_sn, sn.data());
+        out->n_supernodes = k;
+        out->sn_start = (int32_t *)std::malloc((size_t)std::max(k, 1) * 4);
+        if (!out->sn_start) throw std::bad_alloc();
+        std::memcpy(out->sn_start, sn.data(), (size_t)k * 4);
+        out->sources = 2 * (uint64_t)n;
+    } catch (CudaFail &f) {
+        free_result_arrays(out);
+        return fail_cuda(f.e);
+    } catch (std::bad_alloc &) {
+        free_result_arrays(out);
+        return GSOFA_ERR_OOM;
+    }
+    server_release(s, r);
+    s->reqs.erase(it);
+    return GSOFA_OK;
+}
+
+}  // extern "C"

@@ -178,6 +178,15 @@ __device__ __forceinline__ int64_t block_excl_max(int64_t v, int64_t *total,
     return max(pre, ex);
 }
 
+// Global load; CG = true reads through L2 only (no L1), for data that the
+// host may rewrite while a persistent kernel runs.
+template <bool CG>
+__device__ __forceinline__ int32_t ld(const int32_t *p)
+{
+    if (CG) return __ldcg(p);
+    return *p;
+}
+
 // Bit test-and-set in the shared-memory bitmap; true when this call set it.
 __device__ __forceinline__ bool test_and_set(uint32_t *bm, int32_t m)
 {
@@ -297,7 +306,7 @@ __device__ __forceinline__ int32_t chain_start(const PassGraph &g, int32_t x, in
 // With `reuse`, the bitmap still holds the finished traversal of s-1, which is
 // valid because s-1 in adj(s) implies X(s-1) u {s-1} is inside X(s) and
 // hi(s-1) minus (s-1, s] is inside hi(s).
-template <int GT>
+template <int GT, bool CG>
 __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                                int64_t line, int pass, int32_t s, uint32_t *bm,
                                const Frontier &f, SharedState &sh,
@@ -322,14 +331,14 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
 
     // seeding: every neighbour of s is structure of line s; level-0 items
     {
-        const int32_t b0 = g.ptr[s], e0 = g.ptr[s + 1];
+        const int32_t b0 = ld<CG>(g.ptr + s), e0 = ld<CG>(g.ptr + s + 1);
         if (tid == 0) {
             edges += (unsigned long long)(e0 - b0);
-            if (pass == 0) einsp += (unsigned long long)rawdeg[s];
+            if (pass == 0) einsp += (unsigned long long)ld<CG>(rawdeg + s);
         }
         int *tailp = &sh.tailc[0];
         const int end = 0, start = 0;
-        for (int32_t k = b0 + tid; k < e0; k += GT) GSOFA_VISIT(g.adj[k]);
+        for (int32_t k = b0 + tid; k < e0; k += GT) GSOFA_VISIT(ld<CG>(g.adj + k));
     }
 
     // level-synchronous expansion through vertices < s, one barrier a level
@@ -361,10 +370,10 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                 int32_t b = 0, d = 0;
                 if (it < end) {
                     const int32_t v = fr_get(f, it, wstart);
-                    b = g.ptr[v];
-                    d = g.ptr[v + 1] - b;
+                    b = ld<CG>(g.ptr + v);
+                    d = ld<CG>(g.ptr + v + 1) - b;
                     edges += (unsigned long long)d;
-                    if (pass == 0) { xcnt++; einsp += (unsigned long long)rawdeg[v]; }
+                    if (pass == 0) { xcnt++; einsp += (unsigned long long)ld<CG>(rawdeg + v); }
                 }
                 unsigned heavy = __ballot_sync(0xffffffffu, d > HEAVY_ROW);
                 while (heavy) {
@@ -374,7 +383,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                     const int32_t hd = __shfl_sync(0xffffffffu, d, src);
                     for (int32_t k0 = 0; k0 < hd; k0 += 32) {
                         const bool on = k0 + lane < hd;
-                        const int32_t m = on ? g.adj[hb + k0 + lane] : 0;
+                        const int32_t m = on ? ld<CG>(g.adj + hb + k0 + lane) : 0;
                         const bool fresh = on && test_and_set(bm, m);
                         if (fresh) { t_lo = min(t_lo, m); t_hi = max(t_hi, m); }
                         const bool low = fresh && m < s;
@@ -392,7 +401,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                 for (int k0 = 0; k0 < dmax; k0 += 8) {
                     int32_t buf[8];
 #pragma unroll
-                    for (int u = 0; u < 8; u++) buf[u] = (k0 + u < dl) ? g.adj[b + k0 + u] : -1;
+                    for (int u = 0; u < 8; u++) buf[u] = (k0 + u < dl) ? ld<CG>(g.adj + b + k0 + u) : -1;
 #pragma unroll
                     for (int u = 0; u < 8; u++) {
                         const int32_t m = buf[u];
@@ -420,12 +429,12 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                 it = __shfl_sync(gmask, it, 0, lanes) + start;
                 if (it >= end) break;
                 const int32_t v = fr_get(f, it, wstart);
-                const int32_t b = g.ptr[v], e = g.ptr[v + 1];
+                const int32_t b = ld<CG>(g.ptr + v), e = ld<CG>(g.ptr + v + 1);
                 if (lane_in_group == 0) {
                     edges += (unsigned long long)(e - b);
-                    if (pass == 0) { xcnt++; einsp += (unsigned long long)rawdeg[v]; }
+                    if (pass == 0) { xcnt++; einsp += (unsigned long long)ld<CG>(rawdeg + v); }
                 }
-                for (int32_t k = b + lane_in_group; k < e; k += lanes) GSOFA_VISIT(g.adj[k]);
+                for (int32_t k = b + lane_in_group; k < e; k += lanes) GSOFA_VISIT(ld<CG>(g.adj + k));
             }
         }
         wstart = start;
@@ -529,6 +538,61 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
 }
 #undef GSOFA_VISIT
 
+// Per-thread tallies of one CTA's traversals (summed over the CTA at the end).
+struct Tally {
+    unsigned long long edges = 0, nsrc = 0, xcnt = 0, einsp = 0, nreuse = 0;
+    unsigned long long prof[4] = {0, 0, 0, 0};  // levels, expansion, output, clearing cycles
+};
+
+// The sources s_lo, s_lo + stride, ... < s_hi of one work piece, in order,
+// each starting from the previous source's state whenever that is valid.
+template <int BLOCK, bool PAIRED, bool CG>
+__device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &g, int pass,
+                          int32_t s_lo, int32_t s_hi, int32_t stride, uint32_t *bm,
+                          const Frontier &fr, SharedState &sh, int (*pair_flag)[2], int half,
+                          int gtid, int bar, Tally &acc)
+{
+    constexpr int GT = PAIRED ? BLOCK / 2 : BLOCK;
+    const int tid = threadIdx.x;
+    int prev = -2;
+    int idx = 0;
+    for (int32_t s = s_lo; s < s_hi; s += stride, idx++) {
+        int reuse = 0;
+        if (a.reuse && prev == s - 1) {
+            if (PAIRED) {
+                reuse = pair_flag[(idx - 1) & 1][1 - half];
+            } else {
+                if (tid < 32) {
+                    const bool h = warp_has_prev(g, s);
+                    if (tid == 0) sh.flag = h ? 1 : 0;
+                }
+                __syncthreads();
+                reuse = sh.flag;
+            }
+        }
+        if (!reuse) {
+            const long long cc = clock64();
+            const int clo = sh.chain_lo, chi = sh.chain_hi;
+            clear_range<GT>(bm, clo, chi, gtid);
+            gsync<GT>(bar);
+            if (gtid == 0) {
+                sh.chain_lo = INT32_MAX; sh.chain_hi = -1;
+                acc.prof[3] += (unsigned long long)(clock64() - cc);
+            }
+        } else if (gtid == 0) {
+            acc.nreuse++;
+        }
+        process_source<GT, CG>(a, g, md.n, md.line_base + s, pass, s, bm, fr, sh, acc.edges,
+                           md.rawdeg, acc.xcnt, acc.einsp, acc.prof, gtid, bar);
+        if (PAIRED) {
+            if (gtid == 0) pair_flag[idx & 1][half] = sh.flag;
+            __syncthreads();
+        }
+        prev = s;
+        if (gtid == 0) acc.nsrc++;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // The persistent cooperative factorization kernel.
 //
@@ -562,8 +626,7 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
     if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
     const Frontier fr{ring, a.queue + ((int64_t)blockIdx.x * NS + half) * a.qcap, a.qcap, a.status,
                       a.ring_size};
-    unsigned long long edges = 0, nsrc = 0, xcnt = 0, einsp = 0, nreuse = 0;
-    unsigned long long prof[4] = {0, 0, 0, 0};  // levels, expansion, output, clearing cycles
+    Tally acc;
     __syncthreads();
     for (;;) {
         if (tid == 0) s_piece = (long long)atomicAdd(a.piece_counter, 1ull);
@@ -600,43 +663,8 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
             s_lo = sh.seg[0];
             s_hi = sh.seg[1];
         }
-        int prev = -2;
-        int idx = 0;
-        for (int32_t s = s_lo; s < s_hi; s += rg.stride, idx++) {
-            int reuse = 0;
-            if (a.reuse && prev == s - 1) {
-                if (PAIRED) {
-                    reuse = pair_flag[(idx - 1) & 1][1 - half];
-                } else {
-                    if (tid < 32) {
-                        const bool h = warp_has_prev(g, s);
-                        if (tid == 0) sh.flag = h ? 1 : 0;
-                    }
-                    __syncthreads();
-                    reuse = sh.flag;
-                }
-            }
-            if (!reuse) {
-                const long long cc = clock64();
-                const int clo = sh.chain_lo, chi = sh.chain_hi;
-                clear_range<GT>(bm, clo, chi, gtid);
-                gsync<GT>(bar);
-                if (gtid == 0) {
-                    sh.chain_lo = INT32_MAX; sh.chain_hi = -1;
-                    prof[3] += (unsigned long long)(clock64() - cc);
-                }
-            } else if (gtid == 0) {
-                nreuse++;
-            }
-            process_source<GT>(a, g, md.n, md.line_base + s, pass, s, bm, fr, sh, edges,
-                               md.rawdeg, xcnt, einsp, prof, gtid, bar);
-            if (PAIRED) {
-                if (gtid == 0) pair_flag[idx & 1][half] = sh.flag;
-                __syncthreads();
-            }
-            prev = s;
-            if (gtid == 0) nsrc++;
-        }
+        run_piece<BLOCK, PAIRED, false>(a, md, g, pass, s_lo, s_hi, rg.stride, bm, fr, sh, pair_flag,
+                                        half, gtid, bar, acc);
         // the next piece starts from an empty bitmap
         {
             const int clo = sh.chain_lo, chi = sh.chain_hi;
@@ -648,13 +676,13 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
     }
     {
         int64_t *wsum = shs[0].warp;
-        const int64_t e = block_sum<BLOCK>((int64_t)edges, wsum);
-        const int64_t x = block_sum<BLOCK>((int64_t)xcnt, wsum);
-        const int64_t ei = block_sum<BLOCK>((int64_t)einsp, wsum);
-        const int64_t ns = block_sum<BLOCK>((int64_t)nsrc, wsum);
-        const int64_t nr = block_sum<BLOCK>((int64_t)nreuse, wsum);
+        const int64_t e = block_sum<BLOCK>((int64_t)acc.edges, wsum);
+        const int64_t x = block_sum<BLOCK>((int64_t)acc.xcnt, wsum);
+        const int64_t ei = block_sum<BLOCK>((int64_t)acc.einsp, wsum);
+        const int64_t ns = block_sum<BLOCK>((int64_t)acc.nsrc, wsum);
+        const int64_t nr = block_sum<BLOCK>((int64_t)acc.nreuse, wsum);
         int64_t pv[4];
-        for (int q = 0; q < 4; q++) pv[q] = block_sum<BLOCK>((int64_t)prof[q], wsum);
+        for (int q = 0; q < 4; q++) pv[q] = block_sum<BLOCK>((int64_t)acc.prof[q], wsum);
         if (tid == 0) {
             atomicAdd(&a.counters[0], (unsigned long long)e);
             atomicAdd(&a.counters[1], (unsigned long long)ns);

@@ -1,15 +1,18 @@
-"""Serving loop: symbolic factorizations as a request stream on one GPU.
+"""Serving loops: symbolic factorizations as a request stream on one GPU.
 
-Requests (matrices) arrive over time.  The loop keeps every admitted
-request's CSR and scratch resident on the device and runs continuous
-batching at launch granularity: whenever the GPU finishes a persistent
-launch, every request that has arrived in the meantime and fits the memory
-budget is uploaded and joins the next launch, so the work of all of them
-overlaps on the device.  Admission is by predicted device bytes: the
-matrix's own storage plus the per-line state and the frontier queues of the
-launch (n x concurrent sources x per-source state, from
-gsofa_predict_scratch_bytes).  A request whose result is delivered releases
-its bytes.
+ContinuousServer (the serving path) drives the persistent kernel of
+StreamServer: each request is uploaded and published as soon as it arrives
+and fits, and its work pieces run on whichever CTAs free up, overlapping
+with every request already on the device.
+
+Server batches at launch granularity instead: whenever the GPU finishes a
+persistent launch, every request that has arrived in the meantime and fits
+the memory budget is uploaded and joins the next launch.  It is kept for
+comparison and for matrices larger than the serving kernel's limit.
+
+Admission is by predicted device bytes (the matrix's own storage plus the
+per-line state and frontier queues, n x concurrent sources x per-source
+state); a request whose result is delivered releases its bytes.
 
 Latency is measured per request from its arrival to the moment its result is
 on the host; the report gives p50/p99 and sustained factorizations/s, and
@@ -127,6 +130,79 @@ class Server:
             "requests": len(done),
             "launches": launches,
             "mean_batch": float(np.mean(batch_sizes)) if batch_sizes else 0.0,
+            "p50_ms": float(np.percentile(lat, 50) * 1000) if len(lat) else None,
+            "p99_ms": float(np.percentile(lat, 99) * 1000) if len(lat) else None,
+            "mean_ms": float(lat.mean() * 1000) if len(lat) else None,
+            "factorizations_per_s": len(done) / span if span > 0 else None,
+            "nnz_lu_per_s": sum(c.result.nnz_lu for c in done) / span if span > 0 else None,
+            "span_s": span,
+        }
+        return {"report": report, "completions": sorted(done, key=lambda c: c.rid)}
+
+
+class ContinuousServer:
+    """Serves a request stream on the persistent kernel (StreamServer):
+    every request is published as soon as it arrives and fits, and runs
+    alongside whatever is already on the device.  Requests that do not fit
+    wait (admission by device bytes) until finished ones are fetched."""
+
+    def __init__(self, server, poll_interval_s: float = 0.0005,
+                 oversize: Optional[Callable[[Graph], Result]] = None, max_n: Optional[int] = None):
+        self.server = server
+        self.poll_interval = poll_interval_s
+        self.oversize = oversize      # runs requests above max_n (after draining)
+        self.max_n = max_n
+
+    def run(self, requests: Sequence[Request], clock: Callable[[], float] = time.perf_counter,
+            on_result: Optional[Callable[[Completion], None]] = None) -> Dict:
+        reqs = sorted(requests, key=lambda r: r.arrival_s)
+        t0 = clock()
+        now = lambda: clock() - t0  # noqa: E731
+        pending = collections.deque(reqs)
+        waiting: collections.deque = collections.deque()
+        inflight: Dict[int, Request] = {}
+        started: Dict[int, float] = {}
+        done: List[Completion] = []
+        while pending or waiting or inflight:
+            t = now()
+            while pending and pending[0].arrival_s <= t:
+                waiting.append(pending.popleft())
+            # admit waiting requests in arrival order while they fit
+            while waiting:
+                r = waiting[0]
+                st = now()
+                if self.max_n is not None and r.graph.n > self.max_n:
+                    if inflight:
+                        break                      # finish what runs, then take it alone
+                    self.server.drain()
+                    res = self.oversize(r.graph)
+                    waiting.popleft()
+                    c = Completion(r.rid, r.arrival_s, st, now(), res)
+                    done.append(c)
+                    if on_result:
+                        on_result(c)
+                    continue
+                rid = self.server.submit(r.graph)
+                if rid is None:
+                    break
+                waiting.popleft()
+                inflight[rid] = r
+                started[rid] = st
+            for rid in self.server.poll():
+                res = self.server.result(rid)
+                r = inflight.pop(rid)
+                c = Completion(r.rid, r.arrival_s, started.pop(rid), now(), res)
+                done.append(c)
+                if on_result:
+                    on_result(c)
+            if not waiting and inflight:
+                time.sleep(self.poll_interval)
+            elif not inflight and not waiting and pending:
+                time.sleep(max(0.0, min(pending[0].arrival_s - now(), 0.05)))
+        lat = np.array([c.latency_s for c in done])
+        span = max(c.done_s for c in done) - min(c.arrival_s for c in done) if done else 0.0
+        report = {
+            "requests": len(done),
             "p50_ms": float(np.percentile(lat, 50) * 1000) if len(lat) else None,
             "p99_ms": float(np.percentile(lat, 99) * 1000) if len(lat) else None,
             "mean_ms": float(lat.mean() * 1000) if len(lat) else None,

@@ -53,7 +53,9 @@ typedef enum gsofa_status {
     GSOFA_ERR_TIMEOUT = 4,       /* a bounded device-side wait gave up     */
     GSOFA_ERR_CUDA = 5,          /* a CUDA runtime call failed             */
     GSOFA_ERR_IO = 6,            /* an input file could not be read        */
-    GSOFA_ERR_UNSUPPORTED = 7    /* no usable GPU or too large for it      */
+    GSOFA_ERR_UNSUPPORTED = 7,   /* no usable GPU or too large for it      */
+    GSOFA_ERR_BUSY = 8           /* no room for the request now: poll and
+                                    fetch results, then submit again        */
 } gsofa_status;
 
 typedef struct gsofa_ctx gsofa_ctx;       /* device, stream, scratch pools */
@@ -209,6 +211,50 @@ int32_t gsofa_supernodes_from_lines(int32_t n, const int32_t *u_row_count,
  * with these parameters, excluding the pattern pool (admission control). */
 size_t gsofa_predict_scratch_bytes(const gsofa_ctx *ctx, int32_t n, int64_t nnz,
                                    const gsofa_params *params);
+
+/* ---- serving: continuous batching over a persistent kernel ----------------
+ * A server keeps one persistent kernel running on its device.  Every
+ * submitted request (a matrix) is uploaded into device memory the server
+ * reserved at creation, cut into work pieces and published to the running
+ * kernel, whose CTAs take pieces of all live requests as they free up; a
+ * request that arrives while others are being factorized starts on the next
+ * free CTA.  Admission is by predicted device bytes (matrix, per-line state):
+ * a request that does not fit now returns GSOFA_ERR_BUSY.  Results are counts
+ * and supernodes (no pattern).  One host thread drives a server. */
+typedef struct gsofa_server gsofa_server;
+
+typedef struct gsofa_server_config {
+    int32_t device;
+    int32_t max_n;              /* largest request; 0: the largest the paired
+                                   kernel's shared memory holds             */
+    int64_t mem_budget_bytes;   /* device bytes the server may hold; 0: 90%
+                                   of the free memory                       */
+    int32_t max_supernode_size; /* as in gsofa_params                       */
+    int32_t src_chunk;          /* sources per work piece; 0: 32            */
+    int32_t max_requests;       /* requests in flight; 0: 4096             */
+    int32_t idle_exit_us;       /* idle time before the kernel's CTAs exit;
+                                   0: 20000                                 */
+    int32_t max_n_out;          /* set by gsofa_server_create: the limit    */
+} gsofa_server_config;
+
+gsofa_status gsofa_server_create(gsofa_server **srv, gsofa_server_config *cfg);
+void gsofa_server_destroy(gsofa_server *srv);
+/* Device bytes a request holds while it is in flight. */
+size_t gsofa_server_request_bytes(const gsofa_server *srv, int32_t n, int64_t nnz);
+/* Uploads and publishes one request (host arrays, copied); *id identifies it. */
+gsofa_status gsofa_server_submit(gsofa_server *srv, int32_t n, int64_t nnz,
+                                 const int32_t *beg, const int32_t *end,
+                                 const int32_t *adj, int64_t *id);
+/* Ids of requests finished since the last poll (up to `capacity`). */
+gsofa_status gsofa_server_poll(gsofa_server *srv, int64_t *ids, int32_t capacity,
+                               int32_t *count);
+/* Waits until every published request has finished and the kernel has
+ * exited, so other work (another library's kernels, gsofa_symbfact) gets the
+ * whole device; the next submit restarts the kernel. */
+gsofa_status gsofa_server_drain(gsofa_server *srv);
+/* The result of a finished request (counts, line flags, supernodes, totals);
+ * releases the request's device memory.  Free with gsofa_result_free. */
+gsofa_status gsofa_server_result(gsofa_server *srv, int64_t id, gsofa_result *out);
 
 /* ---- factorization without device allocation ------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc:
