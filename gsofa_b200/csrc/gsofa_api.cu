@@ -1337,8 +1337,11 @@ struct ServerReq {
     int64_t g_off = 0, g_units = 0; // graph region in the arena
     uint64_t npieces = 0;
     uint64_t orig_up = 0, orig_lo = 0;
+    int cls = 0;                    // priority class (ring) of its pieces
     bool done = false;
 };
+
+constexpr int32_t kSmallRequest = 65536;   // lines below which a request is class 0
 
 }  // namespace
 
@@ -1371,8 +1374,8 @@ struct gsofa_server {
     std::unordered_map<int64_t, ServerReq> reqs;
     std::vector<unsigned int> h_done;
     int64_t next_id = 1;
-    unsigned long long published = 0;
-    unsigned long long taken_seen = 0;
+    unsigned long long published[kServeClasses] = {0, 0};
+    unsigned long long taken_seen[kServeClasses] = {0, 0};
 };
 
 namespace {
@@ -1396,10 +1399,30 @@ int64_t server_staging_bytes(int32_t n, int64_t nnz)
            r(8 * 2 * scan_tiles) + r(64);
 }
 
+// Stops the running launch (its CTAs are idle or finish what they hold) and
+// clears the flag so the next launch runs.
+void server_stop_kernel(gsofa_server *s)
+{
+    const int32_t one = 1, zero = 0;
+    GS_CUDA(cudaMemcpyAsync(&s->d_ctl->stop, &one, 4, cudaMemcpyHostToDevice, s->io));
+    GS_CUDA(cudaStreamSynchronize(s->io));
+    GS_CUDA(cudaStreamSynchronize(s->run));
+    GS_CUDA(cudaMemcpyAsync(&s->d_ctl->stop, &zero, 4, cudaMemcpyHostToDevice, s->io));
+    GS_CUDA(cudaStreamSynchronize(s->io));
+}
+
 gsofa_status server_launch_if_idle(gsofa_server *s)
 {
-    const cudaError_t q = cudaStreamQuery(s->run);
-    if (q == cudaErrorNotReady) return GSOFA_OK;
+    cudaError_t q = cudaStreamQuery(s->run);
+    if (q == cudaErrorNotReady) {
+        // a launch is running: keep it unless CTAs have left (safety timeout)
+        int32_t live = 0;
+        GS_CUDA(cudaMemcpyAsync(&live, &s->d_ctl->live, 4, cudaMemcpyDeviceToHost, s->io));
+        GS_CUDA(cudaStreamSynchronize(s->io));
+        if (live >= s->grid) return GSOFA_OK;
+        server_stop_kernel(s);
+        q = cudaSuccess;
+    }
     if (q != cudaSuccess) return fail_cuda(q);
     ServeArgs sa{};
     JobArgs &a = sa.job;
@@ -1465,7 +1488,7 @@ gsofa_status gsofa_server_create(gsofa_server **out, gsofa_server_config *cfg)
         s->max_sn = cfg->max_supernode_size;
         s->chunk = cfg->src_chunk > 0 ? cfg->src_chunk : 32;
         s->max_slots = cfg->max_requests > 0 ? cfg->max_requests : 4096;
-        s->idle_spins = std::max(1, (cfg->idle_exit_us > 0 ? cfg->idle_exit_us : 20000) / 2);
+        s->idle_spins = std::max(1, (cfg->idle_exit_us > 0 ? cfg->idle_exit_us : 30000000) / 2);
         s->bitmap_words = ((s->max_n + 31) / 32 + 3) / 4 * 4;
         // frontier ring: the largest that fits beside the two bitmaps
         void *kfn = (void *)serve_kernel<512>;
@@ -1486,7 +1509,8 @@ gsofa_status gsofa_server_create(gsofa_server **out, gsofa_server_config *cfg)
         GS_CUDA(cudaMemGetInfo(&fr, &tot));
         const int64_t budget = cfg->mem_budget_bytes > 0 ? cfg->mem_budget_bytes : (int64_t)(0.9 * (double)fr);
         s->lmax = std::max<int64_t>(4 * (int64_t)s->max_n, 1 << 24);
-        const int64_t fixed = (int64_t)s->grid * 2 * s->max_n * 4 + (int64_t)s->piece_cap * sizeof(ServePiece) +
+        const int64_t fixed = (int64_t)s->grid * 2 * s->max_n * 4 +
+                              (int64_t)kServeClasses * s->piece_cap * sizeof(ServePiece) +
                               (int64_t)s->max_slots * (sizeof(MatDesc) + 4) + s->lmax * 10 + 4096;
         s->arena_units = (budget - fixed) / kArenaUnit;
         if (s->arena_units < units(server_graph_bytes(s->max_n, 8 * (int64_t)s->max_n))) {
@@ -1495,7 +1519,7 @@ gsofa_status gsofa_server_create(gsofa_server **out, gsofa_server_config *cfg)
         }
         GS_CUDA(cudaMalloc(&s->d_ctl, sizeof(ServeCtl) + 64));
         s->d_status = (uint32_t *)((char *)s->d_ctl + sizeof(ServeCtl));
-        GS_CUDA(cudaMalloc(&s->d_pieces, s->piece_cap * sizeof(ServePiece)));
+        GS_CUDA(cudaMalloc(&s->d_pieces, kServeClasses * s->piece_cap * sizeof(ServePiece)));
         GS_CUDA(cudaMalloc(&s->d_slots, (size_t)s->max_slots * sizeof(MatDesc)));
         GS_CUDA(cudaMalloc(&s->d_done, (size_t)s->max_slots * 4));
         GS_CUDA(cudaMalloc(&s->d_cnt, (size_t)2 * s->lmax * 4));
@@ -1576,8 +1600,10 @@ gsofa_status gsofa_server_submit(gsofa_server *s, int32_t n, int64_t nnz, const 
     r.n = n;
     r.nnz = nnz;
     const uint64_t npieces = ((uint64_t)n + s->chunk - 1) / s->chunk;
+    const int cls = n < kSmallRequest ? 0 : 1;
+    r.cls = cls;
     if (s->free_slots.empty()) return GSOFA_ERR_BUSY;
-    if (s->published + npieces - s->taken_seen > s->piece_cap) return GSOFA_ERR_BUSY;
+    if (s->published[cls] + npieces - s->taken_seen[cls] > s->piece_cap) return GSOFA_ERR_BUSY;
     int64_t st_off = 0;
     const int64_t st_units = units(server_staging_bytes(n, nnz));
     r.g_units = units(server_graph_bytes(n, nnz));
@@ -1681,16 +1707,17 @@ gsofa_status gsofa_server_submit(gsofa_server *s, int32_t n, int64_t nnz, const 
             const int64_t hi = (int64_t)n - (int64_t)k * s->chunk;
             pcs[k] = ServePiece{r.slot, (int32_t)std::max<int64_t>(0, hi - s->chunk), (int32_t)hi, 0};
         }
-        const uint64_t at = s->published % s->piece_cap;
+        ServePiece *ring = s->d_pieces + (size_t)cls * s->piece_cap;
+        const uint64_t at = s->published[cls] % s->piece_cap;
         const uint64_t first = std::min<uint64_t>(npieces, s->piece_cap - at);
-        GS_CUDA(cudaMemcpyAsync(s->d_pieces + at, pcs.data(), first * sizeof(ServePiece), cudaMemcpyHostToDevice, st));
+        GS_CUDA(cudaMemcpyAsync(ring + at, pcs.data(), first * sizeof(ServePiece), cudaMemcpyHostToDevice, st));
         if (first < npieces)
-            GS_CUDA(cudaMemcpyAsync(s->d_pieces, pcs.data() + first, (npieces - first) * sizeof(ServePiece),
+            GS_CUDA(cudaMemcpyAsync(ring, pcs.data() + first, (npieces - first) * sizeof(ServePiece),
                                     cudaMemcpyHostToDevice, st));
-        const unsigned long long newpub = s->published + npieces;
-        GS_CUDA(cudaMemcpyAsync(&s->d_ctl->published, &newpub, 8, cudaMemcpyHostToDevice, st));
+        const unsigned long long newpub = s->published[cls] + npieces;
+        GS_CUDA(cudaMemcpyAsync(&s->d_ctl->published[cls], &newpub, 8, cudaMemcpyHostToDevice, st));
         GS_CUDA(cudaStreamSynchronize(st));
-        s->published = newpub;
+        s->published[cls] = newpub;
         r.npieces = npieces;
         s->h_done[(size_t)r.slot] = 0;
     } catch (CudaFail &f) {
@@ -1715,11 +1742,11 @@ gsofa_status gsofa_server_poll(gsofa_server *s, int64_t *ids, int32_t capacity, 
     *count = 0;
     try {
         GS_CUDA(cudaSetDevice(s->device));
-        unsigned long long tk = 0;
+        unsigned long long tk[kServeClasses] = {0, 0};
         GS_CUDA(cudaMemcpyAsync(s->h_done.data(), s->d_done, s->h_done.size() * 4, cudaMemcpyDeviceToHost, s->io));
-        GS_CUDA(cudaMemcpyAsync(&tk, &s->d_ctl->taken, 8, cudaMemcpyDeviceToHost, s->io));
+        GS_CUDA(cudaMemcpyAsync(tk, s->d_ctl->taken, sizeof(tk), cudaMemcpyDeviceToHost, s->io));
         GS_CUDA(cudaStreamSynchronize(s->io));
-        s->taken_seen = tk;
+        for (int c = 0; c < kServeClasses; c++) s->taken_seen[c] = tk[c];
         bool pending = false;
         for (auto &kv : s->reqs) {
             ServerReq &r = kv.second;
@@ -1732,6 +1759,8 @@ gsofa_status gsofa_server_poll(gsofa_server *s, int64_t *ids, int32_t capacity, 
             }
         }
         if (pending) return server_launch_if_idle(s);
+        // nothing in flight: stop the launch so it restarts with every CTA
+        if (cudaStreamQuery(s->run) == cudaErrorNotReady) server_stop_kernel(s);
     } catch (CudaFail &f) {
         return fail_cuda(f.e);
     }

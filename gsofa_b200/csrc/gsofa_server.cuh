@@ -24,22 +24,28 @@ struct ServePiece {          // sources [s_lo, s_hi) of request slot `slot`
     int32_t slot, s_lo, s_hi, pad;
 };
 
+// Two rings: class 0 holds the pieces of small requests and is always served
+// first, so they are not queued behind the pieces of a large one.
+constexpr int kServeClasses = 2;
+
 struct ServeCtl {            // device memory shared by host and kernel
-    unsigned long long published;  // pieces the kernel may take (host)
-    unsigned long long taken;      // pieces claimed so far (kernel)
+    unsigned long long published[kServeClasses];  // pieces the kernel may take (host)
+    unsigned long long taken[kServeClasses];      // pieces claimed so far (kernel)
     int32_t stop;                  // host: exit as soon as idle
-    uint32_t status;
+    int32_t live;                  // CTAs of the running launch that have not exited
     unsigned long long pad[2];
 };
 
 struct ServeArgs {
     JobArgs job;                   // per-line arrays, queues, launch shape
     ServeCtl *ctl;
-    const ServePiece *pieces;      // ring of piece_cap entries
+    const ServePiece *pieces;      // kServeClasses rings of piece_cap entries
     unsigned long long piece_cap;
     const MatDesc *slots;          // matrix descriptor of every request slot
     unsigned int *slot_done;       // finished pieces per slot
-    int idle_spins;                // sleeps of ~2 us before an idle CTA exits
+    int idle_spins;                // sleeps of ~2 us before an idle CTA gives up
+                                   // (a safety bound: the host stops the kernel
+                                   // itself when nothing is in flight)
 };
 
 // Copies a POD through L2-only 8-byte loads.
@@ -76,27 +82,36 @@ __global__ void __launch_bounds__(BLOCK) serve_kernel(ServeArgs sa)
     const Frontier fr{ring, a.queue + ((int64_t)blockIdx.x * 2 + half) * a.qcap, a.qcap, a.status,
                       a.ring_size};
     Tally acc;
+    __shared__ int s_class;
+    if (tid == 0) atomicAdd(&sa.ctl->live, 1);
     __syncthreads();
     for (;;) {
         if (tid == 0) {
             long long got = -1;
+            int cls = 0;
             volatile ServeCtl *ctl = sa.ctl;
-            for (int it = 0; it < sa.idle_spins; it++) {
-                const unsigned long long pub = ctl->published;
-                const unsigned long long tk = ctl->taken;
-                if (tk < pub) {
-                    if (atomicCAS(&sa.ctl->taken, tk, tk + 1) == tk) { got = (long long)tk; break; }
-                    continue;
+            for (int it = 0; it < sa.idle_spins && got < 0; it++) {
+                bool seen = false;
+                for (int c = 0; c < kServeClasses && got < 0; c++) {
+                    const unsigned long long pub = ctl->published[c];
+                    const unsigned long long tk = ctl->taken[c];
+                    if (tk < pub) {
+                        seen = true;
+                        if (atomicCAS(&sa.ctl->taken[c], tk, tk + 1) == tk) { got = (long long)tk; cls = c; }
+                    }
                 }
+                if (got >= 0 || seen) continue;
                 if (ctl->stop) break;     // only once nothing is left to take
                 __nanosleep(2000);
             }
             s_piece = got;
+            s_class = cls;
         }
         __syncthreads();
         const long long pc = s_piece;
         if (pc < 0) break;
-        const ServePiece piece = load_cg(sa.pieces + (pc % (long long)sa.piece_cap));
+        const ServePiece piece =
+            load_cg(sa.pieces + (unsigned long long)s_class * sa.piece_cap + (pc % (long long)sa.piece_cap));
         const MatDesc md = load_cg(sa.slots + piece.slot);
         run_piece<BLOCK, true, true>(a, md, md.g[half], half, piece.s_lo, piece.s_hi, 1, bm, fr, sh,
                                      pair_flag, half, gtid, bar, acc);
@@ -112,6 +127,7 @@ __global__ void __launch_bounds__(BLOCK) serve_kernel(ServeArgs sa)
         }
         __syncthreads();
     }
+    if (tid == 0) atomicSub(&sa.ctl->live, 1);
 }
 
 }  // namespace dev

@@ -232,8 +232,10 @@ typedef struct gsofa_server_config {
     int32_t max_supernode_size; /* as in gsofa_params                       */
     int32_t src_chunk;          /* sources per work piece; 0: 32            */
     int32_t max_requests;       /* requests in flight; 0: 4096             */
-    int32_t idle_exit_us;       /* idle time before the kernel's CTAs exit;
-                                   0: 20000                                 */
+    int32_t idle_exit_us;       /* safety bound on how long an idle CTA
+                                   waits for work (the host stops the kernel
+                                   itself when nothing is in flight);
+                                   0: 30 s                                  */
     int32_t max_n_out;          /* set by gsofa_server_create: the limit    */
 } gsofa_server_config;
 
