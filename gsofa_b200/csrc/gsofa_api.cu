@@ -1411,7 +1411,18 @@ void server_stop_kernel(gsofa_server *s)
     GS_CUDA(cudaStreamSynchronize(s->io));
 }
 
+gsofa_status server_launch_if_idle_impl(gsofa_server *s);
+
 gsofa_status server_launch_if_idle(gsofa_server *s)
+{
+    try {
+        return server_launch_if_idle_impl(s);
+    } catch (CudaFail &f) {
+        return fail_cuda(f.e);
+    }
+}
+
+gsofa_status server_launch_if_idle_impl(gsofa_server *s)
 {
     cudaError_t q = cudaStreamQuery(s->run);
     if (q == cudaErrorNotReady) {
