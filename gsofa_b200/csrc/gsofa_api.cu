@@ -1426,15 +1426,18 @@ gsofa_status server_launch_if_idle_impl(gsofa_server *s)
 {
     cudaError_t q = cudaStreamQuery(s->run);
     if (q == cudaErrorNotReady) {
-        // a launch is running: keep it unless CTAs have left (safety timeout)
-        int32_t live = 0;
-        GS_CUDA(cudaMemcpyAsync(&live, &s->d_ctl->live, 4, cudaMemcpyDeviceToHost, s->io));
+        // a launch is running: keep it unless some of its CTAs have left
+        // (their safety timeout); then let it finish and start a full one
+        int32_t exited = 0;
+        GS_CUDA(cudaMemcpyAsync(&exited, &s->d_ctl->exited, 4, cudaMemcpyDeviceToHost, s->io));
         GS_CUDA(cudaStreamSynchronize(s->io));
-        if (live >= s->grid) return GSOFA_OK;
+        if (exited == 0) return GSOFA_OK;
         server_stop_kernel(s);
         q = cudaSuccess;
     }
     if (q != cudaSuccess) return fail_cuda(q);
+    GS_CUDA(cudaMemsetAsync(&s->d_ctl->exited, 0, 4, s->io));
+    GS_CUDA(cudaStreamSynchronize(s->io));
     ServeArgs sa{};
     JobArgs &a = sa.job;
     a.queue = s->d_queue;

@@ -32,7 +32,7 @@ struct ServeCtl {            // device memory shared by host and kernel
     unsigned long long published[kServeClasses];  // pieces the kernel may take (host)
     unsigned long long taken[kServeClasses];      // pieces claimed so far (kernel)
     int32_t stop;                  // host: exit as soon as idle
-    int32_t live;                  // CTAs of the running launch that have not exited
+    int32_t exited;                // CTAs of the current launch that have left
     unsigned long long pad[2];
 };
 
@@ -83,7 +83,6 @@ __global__ void __launch_bounds__(BLOCK) serve_kernel(ServeArgs sa)
                       a.ring_size};
     Tally acc;
     __shared__ int s_class;
-    if (tid == 0) atomicAdd(&sa.ctl->live, 1);
     __syncthreads();
     for (;;) {
         if (tid == 0) {
@@ -127,7 +126,7 @@ __global__ void __launch_bounds__(BLOCK) serve_kernel(ServeArgs sa)
         }
         __syncthreads();
     }
-    if (tid == 0) atomicSub(&sa.ctl->live, 1);
+    if (tid == 0) atomicAdd(&sa.ctl->exited, 1);
 }
 
 }  // namespace dev

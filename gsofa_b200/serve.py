@@ -147,11 +147,13 @@ class ContinuousServer:
     wait (admission by device bytes) until finished ones are fetched."""
 
     def __init__(self, server, poll_interval_s: float = 0.0005,
-                 oversize: Optional[Callable[[Graph], Result]] = None, max_n: Optional[int] = None):
+                 oversize: Optional[Callable[[Graph], Result]] = None, max_n: Optional[int] = None,
+                 stall_s: float = 300.0):
         self.server = server
         self.poll_interval = poll_interval_s
         self.oversize = oversize      # runs requests above max_n (after draining)
         self.max_n = max_n
+        self.stall_s = stall_s        # no completion for this long while work is in flight: error
 
     def run(self, requests: Sequence[Request], clock: Callable[[], float] = time.perf_counter,
             on_result: Optional[Callable[[Completion], None]] = None) -> Dict:
@@ -163,8 +165,12 @@ class ContinuousServer:
         inflight: Dict[int, Request] = {}
         started: Dict[int, float] = {}
         done: List[Completion] = []
+        last_progress = now()
         while pending or waiting or inflight:
             t = now()
+            if inflight and t - last_progress > self.stall_s:
+                raise RuntimeError(f"serving stalled: {len(inflight)} requests in flight, "
+                                   f"no completion for {self.stall_s:.0f} s")
             while pending and pending[0].arrival_s <= t:
                 waiting.append(pending.popleft())
             # admit waiting requests in arrival order while they fit
@@ -189,6 +195,7 @@ class ContinuousServer:
                 inflight[rid] = r
                 started[rid] = st
             for rid in self.server.poll():
+                last_progress = now()
                 res = self.server.result(rid)
                 r = inflight.pop(rid)
                 c = Completion(r.rid, r.arrival_s, started.pop(rid), now(), res)
