@@ -1494,7 +1494,11 @@ gsofa_status gsofa_server_create(gsofa_server **out, gsofa_server_config *cfg)
         if (prop.major < 10) { delete s; return GSOFA_ERR_UNSUPPORTED; }
         s->sms = prop.multiProcessorCount;
         s->optin = prop.sharedMemPerBlockOptin;
-        const size_t static_smem = 2 * sizeof(SharedState) + 1024;
+        // Shared memory left free on each SM so the upload kernels (and the
+        // runtime's memset kernels) of new requests run beside the serving
+        // kernel instead of waiting for it to exit.
+        const size_t reserve = 12 * 1024;
+        const size_t static_smem = 2 * sizeof(SharedState) + 1024 + reserve;
         const int32_t limit_n =
             (int32_t)std::min<int64_t>(((int64_t)(s->optin - static_smem) / 2 - 1024 * 4) / 4 / 4 * 4 * 32, INT32_MAX);
         s->max_n = cfg->max_n > 0 ? cfg->max_n : limit_n;
