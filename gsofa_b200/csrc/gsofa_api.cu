@@ -243,9 +243,12 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     if (L == 0) return GSOFA_OK;
 
     // parameters
-    const int32_t words_needed = ((max_n + 31) / 32 + 3) / 4 * 4;
+    // bitmap words rounded to 128 so its summary (one bit per word) is a
+    // whole number of 16-byte groups
+    const int32_t words_needed = ((max_n + 31) / 32 + 127) / 128 * 128;
+    const int32_t state_needed = words_needed + words_needed / 32;
     const bool paired = reuse && p.reuse != 2 &&
-                        (size_t)2 * words_needed * 4 + 2 * 1024 * 4 + sizeof(SharedState) * 2 + 1024 <=
+                        (size_t)2 * state_needed * 4 + 2 * 1024 * 4 + sizeof(SharedState) * 2 + 1024 <=
                             ctx->smem_optin;
     int block = p.block_size ? p.block_size : pick_block(max_n) * (paired ? 2 : 1);
     void *kfn = factor_kernel_for(block, paired);
@@ -257,8 +260,9 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     int chunk = p.src_chunk > 0 ? p.src_chunk : (reuse ? 32 : 1);
 
     const int32_t bitmap_words = words_needed;
+    const int32_t state_words = state_needed;
     const size_t static_smem = sizeof(SharedState) * NS + 1024;
-    if ((size_t)NS * (bitmap_words * 4 + 1024 * 4) + static_smem > ctx->smem_optin) return GSOFA_ERR_UNSUPPORTED;
+    if ((size_t)NS * (state_words * 4 + 1024 * 4) + static_smem > ctx->smem_optin) return GSOFA_ERR_UNSUPPORTED;
     // frontier ring: the largest of 8K/4K/2K/1K entries that keeps the most
     // CTAs (each with its own bitmap) resident on an SM; sized once per shape
     int ring = 0, occ = 0;
@@ -269,10 +273,10 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
             ring = sh.ring; occ = sh.occ; cached = true;
         }
     if (cached) {
-        smem = (size_t)NS * ((size_t)bitmap_words * 4 + (size_t)ring * 4);
+        smem = (size_t)NS * ((size_t)state_words * 4 + (size_t)ring * 4);
     } else {
         for (int cand = 8192; cand >= 1024; cand >>= 1) {
-            const size_t sm = (size_t)NS * ((size_t)bitmap_words * 4 + (size_t)cand * 4);
+            const size_t sm = (size_t)NS * ((size_t)state_words * 4 + (size_t)cand * 4);
             if (sm + static_smem > ctx->smem_optin) continue;
             GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
             int o = 0;
@@ -372,6 +376,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         a.queue = d_queue;
         a.qcap = qcap;
         a.bitmap_words = bitmap_words;
+        a.state_words = state_words;
         a.ring_size = ring;
         a.lanes = lanes;
         a.reuse = reuse;
@@ -1133,9 +1138,10 @@ extern "C" gsofa_status gsofa_symbfact_counts_noalloc(int device, void *cuda_str
         // launch shape: 256 threads, one CTA per SM (its queue slice is n ints)
         constexpr int BLOCK = 256;
         void *kfn = factor_kernel_for(BLOCK, false);
-        const int32_t bitmap_words = ((n + 31) / 32 + 3) / 4 * 4;
+        const int32_t bitmap_words = ((n + 31) / 32 + 127) / 128 * 128;
+        const int32_t state_words = bitmap_words + bitmap_words / 32;
         const int ring = 4096;
-        const size_t smem = (size_t)bitmap_words * 4 + (size_t)ring * 4;
+        const size_t smem = (size_t)state_words * 4 + (size_t)ring * 4;
         GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int occ = 0;
         GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, BLOCK, smem));
@@ -1241,6 +1247,7 @@ extern "C" gsofa_status gsofa_symbfact_counts_noalloc(int device, void *cuda_str
         a.queue = queue;
         a.qcap = n;
         a.bitmap_words = bitmap_words;
+        a.state_words = state_words;
         a.ring_size = ring;
         a.lanes = 1;
         a.reuse = 1;
@@ -1354,7 +1361,7 @@ struct gsofa_server {
     int32_t max_slots = 4096;
     int idle_spins = 10000;
     int block = 512, ring = 1024, grid = 0;
-    int32_t bitmap_words = 0;
+    int32_t bitmap_words = 0, state_words = 0;
     size_t smem = 0;
     cudaStream_t run = nullptr, io = nullptr;
     ServeCtl *d_ctl = nullptr;
@@ -1443,6 +1450,7 @@ gsofa_status server_launch_if_idle_impl(gsofa_server *s)
     a.queue = s->d_queue;
     a.qcap = s->max_n;
     a.bitmap_words = s->bitmap_words;
+    a.state_words = s->state_words;
     a.ring_size = s->ring;
     a.lanes = 1;
     a.reuse = 1;
@@ -1499,20 +1507,22 @@ gsofa_status gsofa_server_create(gsofa_server **out, gsofa_server_config *cfg)
         // kernel instead of waiting for it to exit.
         const size_t reserve = 12 * 1024;
         const size_t static_smem = 2 * sizeof(SharedState) + 1024 + reserve;
+        const int64_t per_half_words = ((int64_t)(s->optin - static_smem) / 2 - 1024 * 4) / 4;
         const int32_t limit_n =
-            (int32_t)std::min<int64_t>(((int64_t)(s->optin - static_smem) / 2 - 1024 * 4) / 4 / 4 * 4 * 32, INT32_MAX);
+            (int32_t)std::min<int64_t>(per_half_words * 32 / 33 / 128 * 128 * 32, INT32_MAX);
         s->max_n = cfg->max_n > 0 ? cfg->max_n : limit_n;
         if (s->max_n > limit_n || s->max_n <= 0) { delete s; return GSOFA_ERR_UNSUPPORTED; }
         s->max_sn = cfg->max_supernode_size;
         s->chunk = cfg->src_chunk > 0 ? cfg->src_chunk : 32;
         s->max_slots = cfg->max_requests > 0 ? cfg->max_requests : 4096;
         s->idle_spins = std::max(1, (cfg->idle_exit_us > 0 ? cfg->idle_exit_us : 30000000) / 2);
-        s->bitmap_words = ((s->max_n + 31) / 32 + 3) / 4 * 4;
+        s->bitmap_words = ((s->max_n + 31) / 32 + 127) / 128 * 128;
+        s->state_words = s->bitmap_words + s->bitmap_words / 32;
         // frontier ring: the largest that fits beside the two bitmaps
         void *kfn = (void *)serve_kernel<512>;
         s->ring = 0;
         for (int cand = 8192; cand >= 1024; cand >>= 1) {
-            const size_t sm = 2 * ((size_t)s->bitmap_words * 4 + (size_t)cand * 4);
+            const size_t sm = 2 * ((size_t)s->state_words * 4 + (size_t)cand * 4);
             if (sm + static_smem <= s->optin) { s->ring = cand; s->smem = sm; break; }
         }
         if (!s->ring) { delete s; return GSOFA_ERR_UNSUPPORTED; }

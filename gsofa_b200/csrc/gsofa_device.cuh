@@ -67,7 +67,8 @@ struct JobArgs {
     unsigned long long *piece_counter; // dynamic fetch of work pieces
     int32_t *queue;            // gridDim.x * qcap
     int64_t qcap;
-    int32_t bitmap_words;      // shared-memory bitmap size (>= max n / 32, multiple of 4)
+    int32_t bitmap_words;      // shared-memory bitmap size (>= max n / 32, multiple of 128)
+    int32_t state_words;       // bitmap + its summary (bitmap_words / 32 words)
     int32_t ring_size;         // shared-memory frontier ring entries (power of two)
     int32_t lanes;             // lanes per frontier vertex: 1 (thread per vertex,
                                // warp for long rows) or 4..32
@@ -188,12 +189,17 @@ __device__ __forceinline__ int32_t ld(const int32_t *p)
 }
 
 // Bit test-and-set in the shared-memory bitmap; true when this call set it.
-__device__ __forceinline__ bool test_and_set(uint32_t *bm, int32_t m)
+// summ holds one bit per bitmap word, set when that word first becomes
+// nonzero, so output scans can skip empty stretches 32 words at a time.
+__device__ __forceinline__ bool test_and_set(uint32_t *bm, uint32_t *summ, int32_t m)
 {
     const uint32_t bit = 1u << (m & 31);
-    uint32_t *w = bm + (m >> 5);
+    const int wi = m >> 5;
+    uint32_t *w = bm + wi;
     if (*reinterpret_cast<volatile uint32_t *>(w) & bit) return false;
-    return !(atomicOr(w, bit) & bit);
+    const uint32_t old = atomicOr(w, bit);
+    if (old == 0u) atomicOr(summ + (wi >> 5), 1u << (wi & 31));
+    return !(old & bit);
 }
 
 // Frontier queue of one source: absolute positions 0, 1, 2, ... in BFS order.
@@ -250,10 +256,11 @@ struct SharedState {
 // Clears the bitmap words covering vertices [lo, hi]; gtid/GT: the calling
 // thread's index and the size of the thread group that shares the bitmap.
 template <int GT>
-__device__ __forceinline__ void clear_range(uint32_t *bm, int lo, int hi, int gtid)
+__device__ __forceinline__ void clear_range(uint32_t *bm, uint32_t *summ, int lo, int hi, int gtid)
 {
     if (hi < lo) return;
     for (int w = (lo >> 5) + gtid; w <= (hi >> 5); w += GT) bm[w] = 0u;
+    for (int w = (lo >> 10) + gtid; w <= (hi >> 10); w += GT) summ[w] = 0u;
 }
 
 // Barrier of the GT threads that work on one traversal: the whole CTA
@@ -294,7 +301,7 @@ __device__ __forceinline__ int32_t chain_start(const PassGraph &g, int32_t x, in
 #define GSOFA_VISIT(m)                                                          \
     do {                                                                        \
         const int32_t _m = (m);                                                 \
-        if (test_and_set(bm, _m)) {                                             \
+        if (test_and_set(bm, summ, _m)) {                                             \
             t_lo = min(t_lo, _m);                                               \
             t_hi = max(t_hi, _m);                                               \
             if (_m < s) push(f, tailp, end, start, _m);                         \
@@ -308,7 +315,7 @@ __device__ __forceinline__ int32_t chain_start(const PassGraph &g, int32_t x, in
 // hi(s-1) minus (s-1, s] is inside hi(s).
 template <int GT, bool CG>
 __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
-                               int64_t line, int pass, int32_t s, uint32_t *bm,
+                               int64_t line, int pass, int32_t s, uint32_t *bm, uint32_t *summ,
                                const Frontier &f, SharedState &sh,
                                unsigned long long &edges, const int32_t *rawdeg,
                                unsigned long long &xcnt, unsigned long long &einsp,
@@ -325,7 +332,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         c0 = clock64();
         sh.tailc[0] = sh.tailc[1] = sh.tailc[2] = 0;
         sh.fetch[0] = sh.fetch[1] = sh.fetch[2] = 0;
-        if (test_and_set(bm, s)) { t_lo = s; t_hi = s; }
+        if (test_and_set(bm, summ, s)) { t_lo = s; t_hi = s; }
     }
     gsync<GT>(bar);
 
@@ -384,7 +391,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                     for (int32_t k0 = 0; k0 < hd; k0 += 32) {
                         const bool on = k0 + lane < hd;
                         const int32_t m = on ? ld<CG>(g.adj + hb + k0 + lane) : 0;
-                        const bool fresh = on && test_and_set(bm, m);
+                        const bool fresh = on && test_and_set(bm, summ, m);
                         if (fresh) { t_lo = min(t_lo, m); t_hi = max(t_hi, m); }
                         const bool low = fresh && m < s;
                         const unsigned bal = __ballot_sync(0xffffffffu, low);
@@ -405,7 +412,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
 #pragma unroll
                     for (int u = 0; u < 8; u++) {
                         const int32_t m = buf[u];
-                        const bool fresh = m >= 0 && test_and_set(bm, m);
+                        const bool fresh = m >= 0 && test_and_set(bm, summ, m);
                         if (fresh) { t_lo = min(t_lo, m); t_hi = max(t_hi, m); }
                         const bool low = fresh && m < s;
                         const unsigned bal = __ballot_sync(0xffffffffu, low);
@@ -462,15 +469,20 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
     const int wid = tid >> 5;
     const int w0 = (s + 1) >> 5;
     const int w1 = (chain_hi > s) ? (chain_hi >> 5) : (w0 - 1);
-    const int nchunks = (w1 - w0 + 1 + 31) >> 5;      // <= 0 when empty
+    // chunks are aligned groups of 32 words: one summary word each
+    const int cfirst = w0 >> 5;
+    const int nchunks = (w1 >= w0) ? (w1 >> 5) - cfirst + 1 : 0;
     const int per = nchunks > 0 ? (nchunks + NWARP - 1) / NWARP : 0;
     const int ch0 = wid * per;
     const int ch1 = min(ch0 + per, max(nchunks, 0));
     const uint32_t first_mask = ~0u << ((s + 1) & 31);
     int wcount = 0;
     for (int c = ch0; c < ch1; c++) {
-        const int w = w0 + (c << 5) + lane;
-        uint32_t x = (w <= w1) ? bm[w] : 0u;
+        const uint32_t sc = summ[cfirst + c];
+        if (!sc) continue;                              // warp-uniform
+        const int w = ((cfirst + c) << 5) + lane;
+        uint32_t x = ((sc >> lane) & 1u) ? bm[w] : 0u;
+        if (w < w0 || w > w1) x = 0u;
         if (w == w0) x &= first_mask;
         wcount += __popc(x);
     }
@@ -513,8 +525,11 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         if (base >= 0 && wcount > 0) {
             int64_t run = base + wpre;
             for (int c = ch0; c < ch1; c++) {
-                const int w = w0 + (c << 5) + lane;
-                uint32_t x = (w <= w1) ? bm[w] : 0u;
+                const uint32_t sc = summ[cfirst + c];
+                if (!sc) continue;
+                const int w = ((cfirst + c) << 5) + lane;
+                uint32_t x = ((sc >> lane) & 1u) ? bm[w] : 0u;
+                if (w < w0 || w > w1) x = 0u;
                 if (w == w0) x &= first_mask;
                 const int pc = __popc(x);
                 int incl = pc;
@@ -548,7 +563,7 @@ struct Tally {
 // each starting from the previous source's state whenever that is valid.
 template <int BLOCK, bool PAIRED, bool CG>
 __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &g, int pass,
-                          int32_t s_lo, int32_t s_hi, int32_t stride, uint32_t *bm,
+                          int32_t s_lo, int32_t s_hi, int32_t stride, uint32_t *bm, uint32_t *summ,
                           const Frontier &fr, SharedState &sh, int (*pair_flag)[2], int half,
                           int gtid, int bar, Tally &acc)
 {
@@ -573,7 +588,7 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
         if (!reuse) {
             const long long cc = clock64();
             const int clo = sh.chain_lo, chi = sh.chain_hi;
-            clear_range<GT>(bm, clo, chi, gtid);
+            clear_range<GT>(bm, summ, clo, chi, gtid);
             gsync<GT>(bar);
             if (gtid == 0) {
                 sh.chain_lo = INT32_MAX; sh.chain_hi = -1;
@@ -582,7 +597,7 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
         } else if (gtid == 0) {
             acc.nreuse++;
         }
-        process_source<GT, CG>(a, g, md.n, md.line_base + s, pass, s, bm, fr, sh, acc.edges,
+        process_source<GT, CG>(a, g, md.n, md.line_base + s, pass, s, bm, summ, fr, sh, acc.edges,
                            md.rawdeg, acc.xcnt, acc.einsp, acc.prof, gtid, bar);
         if (PAIRED) {
             if (gtid == 0) pair_flag[idx & 1][half] = sh.flag;
@@ -618,11 +633,12 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
     const int gtid = PAIRED ? tid % GT : tid;
     const int bar = PAIRED ? 1 + half : 0;
     SharedState &sh = shs[half];
-    uint32_t *bm = smem_dyn + (size_t)half * a.bitmap_words;
-    int32_t *ring = (int32_t *)(smem_dyn + (size_t)NS * a.bitmap_words) + (size_t)half * a.ring_size;
+    uint32_t *bm = smem_dyn + (size_t)half * a.state_words;
+    uint32_t *summ = bm + a.bitmap_words;
+    int32_t *ring = (int32_t *)(smem_dyn + (size_t)NS * a.state_words) + (size_t)half * a.ring_size;
 
     // ---- phase 1: traversals ------------------------------------------------
-    for (int w = tid; w < NS * a.bitmap_words; w += BLOCK) smem_dyn[w] = 0u;
+    for (int w = tid; w < NS * a.state_words; w += BLOCK) smem_dyn[w] = 0u;
     if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
     const Frontier fr{ring, a.queue + ((int64_t)blockIdx.x * NS + half) * a.qcap, a.qcap, a.status,
                       a.ring_size};
@@ -663,12 +679,12 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
             s_lo = sh.seg[0];
             s_hi = sh.seg[1];
         }
-        run_piece<BLOCK, PAIRED, false>(a, md, g, pass, s_lo, s_hi, rg.stride, bm, fr, sh, pair_flag,
+        run_piece<BLOCK, PAIRED, false>(a, md, g, pass, s_lo, s_hi, rg.stride, bm, summ, fr, sh, pair_flag,
                                         half, gtid, bar, acc);
         // the next piece starts from an empty bitmap
         {
             const int clo = sh.chain_lo, chi = sh.chain_hi;
-            clear_range<GT>(bm, clo, chi, gtid);
+            clear_range<GT>(bm, summ, clo, chi, gtid);
             __syncthreads();
             if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
             __syncthreads();

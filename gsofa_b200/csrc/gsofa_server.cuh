@@ -75,9 +75,10 @@ __global__ void __launch_bounds__(BLOCK) serve_kernel(ServeArgs sa)
     const int gtid = tid % GT;
     const int bar = 1 + half;
     SharedState &sh = shs[half];
-    uint32_t *bm = smem_dyn + (size_t)half * a.bitmap_words;
-    int32_t *ring = (int32_t *)(smem_dyn + (size_t)2 * a.bitmap_words) + (size_t)half * a.ring_size;
-    for (int w = tid; w < 2 * a.bitmap_words; w += BLOCK) smem_dyn[w] = 0u;
+    uint32_t *bm = smem_dyn + (size_t)half * a.state_words;
+    uint32_t *summ = bm + a.bitmap_words;
+    int32_t *ring = (int32_t *)(smem_dyn + (size_t)2 * a.state_words) + (size_t)half * a.ring_size;
+    for (int w = tid; w < 2 * a.state_words; w += BLOCK) smem_dyn[w] = 0u;
     if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
     const Frontier fr{ring, a.queue + ((int64_t)blockIdx.x * 2 + half) * a.qcap, a.qcap, a.status,
                       a.ring_size};
@@ -112,11 +113,11 @@ __global__ void __launch_bounds__(BLOCK) serve_kernel(ServeArgs sa)
         const ServePiece piece =
             load_cg(sa.pieces + (unsigned long long)s_class * sa.piece_cap + (pc % (long long)sa.piece_cap));
         const MatDesc md = load_cg(sa.slots + piece.slot);
-        run_piece<BLOCK, true, true>(a, md, md.g[half], half, piece.s_lo, piece.s_hi, 1, bm, fr, sh,
+        run_piece<BLOCK, true, true>(a, md, md.g[half], half, piece.s_lo, piece.s_hi, 1, bm, summ, fr, sh,
                                      pair_flag, half, gtid, bar, acc);
         {
             const int clo = sh.chain_lo, chi = sh.chain_hi;
-            clear_range<GT>(bm, clo, chi, gtid);
+            clear_range<GT>(bm, summ, clo, chi, gtid);
             __syncthreads();
             if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
         }
