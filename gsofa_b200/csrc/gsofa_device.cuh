@@ -250,8 +250,14 @@ struct SharedState {
     int chain_hi;     // highest vertex set since the last clear
     int seg[2];       // piece boundaries after chain alignment
     int64_t pool_base;
+    int64_t pool_cur;  // this traversal's private slice of the pattern pool:
+    int64_t pool_end;  // [pool_cur, pool_end), refilled POOL_CHUNK entries at a time
     int64_t warp[32];
 };
+
+// Pattern pool entries a traversal takes from the shared pool at a time (one
+// global atomic per chunk instead of one per source).
+constexpr int64_t POOL_CHUNK = 1 << 16;
 
 // Clears the bitmap words covering vertices [lo, hi]; gtid/GT: the calling
 // thread's index and the size of the thread group that shares the bitmap.
@@ -509,12 +515,22 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         a.nxt[slot] = (uint8_t)nx;
         sh.flag = nx;
         if (a.want_pattern) {
-            const unsigned long long o = atomicAdd(a.pool_tail, (unsigned long long)total);
-            if ((int64_t)o + total > a.pool_cap) {
+            if (sh.pool_cur + total > sh.pool_end) {
+                const int64_t want = max(total, POOL_CHUNK);
+                const unsigned long long o = atomicAdd(a.pool_tail, (unsigned long long)want);
+                if ((int64_t)o + want > a.pool_cap) {
+                    sh.pool_cur = sh.pool_end = 0;
+                } else {
+                    sh.pool_cur = (int64_t)o;
+                    sh.pool_end = (int64_t)o + want;
+                }
+            }
+            if (sh.pool_cur + total > sh.pool_end) {
                 atomicOr(a.status, ERR_POOL_OVERFLOW);
                 sh.pool_base = -1;
             } else {
-                sh.pool_base = (int64_t)o;
+                sh.pool_base = sh.pool_cur;
+                sh.pool_cur += total;
             }
             a.poff[slot] = sh.pool_base;
         }
@@ -523,7 +539,19 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         gsync<GT>(bar);
         const int64_t base = sh.pool_base;
         if (base >= 0 && wcount > 0) {
-            int64_t run = base + wpre;
+            // Entries go through this warp's slice of the frontier ring (idle
+            // once the traversal is done) and leave in coalesced runs.
+            const int slice = f.ring_size / NWARP;
+            int32_t *stage = f.ring + wid * slice;
+            int64_t run = base + wpre;   // global position of stage[0]
+            int fill = 0;
+            auto flush = [&]() {
+                __syncwarp();
+                for (int i = lane; i < fill; i += 32) a.pool[run + i] = stage[i];
+                __syncwarp();
+                run += fill;
+                fill = 0;
+            };
             for (int c = ch0; c < ch1; c++) {
                 const uint32_t sc = summ[cfirst + c];
                 if (!sc) continue;
@@ -538,14 +566,18 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                     const int y = __shfl_up_sync(0xffffffffu, incl, o);
                     if (lane >= o) incl += y;
                 }
-                int32_t *dst = a.pool + run + (incl - pc);
+                const int tot = __shfl_sync(0xffffffffu, incl, 31);
+                if (fill + tot > slice) flush();
+                int32_t *dst = (tot > slice) ? a.pool + run + (incl - pc) : stage + fill + (incl - pc);
                 while (x) {
                     const int bit = __ffs(x) - 1;
                     x &= x - 1u;
                     *dst++ = (w << 5) + bit;
                 }
-                run += __shfl_sync(0xffffffffu, incl, 31);
+                if (tot > slice) run += tot;
+                else fill += tot;
             }
+            flush();
         }
     }
     gsync<GT>(bar);
@@ -639,7 +671,7 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
 
     // ---- phase 1: traversals ------------------------------------------------
     for (int w = tid; w < NS * a.state_words; w += BLOCK) smem_dyn[w] = 0u;
-    if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
+    if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.pool_cur = sh.pool_end = 0; }
     const Frontier fr{ring, a.queue + ((int64_t)blockIdx.x * NS + half) * a.qcap, a.qcap, a.status,
                       a.ring_size};
     Tally acc;
