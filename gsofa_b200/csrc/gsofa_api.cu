@@ -319,6 +319,9 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     // pool sizing: the last run's exact need (plus the traversals' unused
     // chunk ends), else a share of the budget
     const int64_t pool_slack = (int64_t)grid * NS * POOL_CHUNK;
+    // entries plus what chunked allocation may leave unused: under 1/7 of the
+    // entries at refills and one chunk per traversal at the end
+    auto pool_need = [&](int64_t entries) { return std::max<int64_t>(entries, 1) * 8 / 7 + 1 + pool_slack; };
     int64_t pool_cap = 0;
     if (want_pattern) {
         if (p.pool_capacity > 0) {
@@ -331,7 +334,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
                 else known += mats[i]->last_pattern_total;
             }
             if (all_known) {
-                pool_cap = std::max<int64_t>(known, 1) + pool_slack;
+                pool_cap = pool_need(known);
             } else {
                 size_t freeb = ctx->budget > ctx->held ? ctx->budget - ctx->held : 0;
                 pool_cap = std::max<int64_t>((int64_t)(freeb / 4 / (2 * sizeof(int32_t))), 1 << 20);
@@ -488,7 +491,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         if (status & ERR_QUEUE_OVERFLOW) return GSOFA_ERR_QUEUE_OVERFLOW;
         if (want_pattern && (status & ERR_POOL_OVERFLOW)) {
             if (attempt == 0) {
-                pool_cap = std::max<int64_t>(tot[0] + tot[1], 1) + pool_slack;
+                pool_cap = pool_need(tot[0] + tot[1]);
                 continue;   // rerun with the pool the counts ask for
             }
             return GSOFA_ERR_QUEUE_OVERFLOW;

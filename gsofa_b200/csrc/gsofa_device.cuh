@@ -515,24 +515,31 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         a.nxt[slot] = (uint8_t)nx;
         sh.flag = nx;
         if (a.want_pattern) {
-            if (sh.pool_cur + total > sh.pool_end) {
-                const int64_t want = max(total, POOL_CHUNK);
-                const unsigned long long o = atomicAdd(a.pool_tail, (unsigned long long)want);
-                if ((int64_t)o + want > a.pool_cap) {
-                    sh.pool_cur = sh.pool_end = 0;
-                } else {
-                    sh.pool_cur = (int64_t)o;
-                    sh.pool_end = (int64_t)o + want;
+            // Lists up to POOL_CHUNK / 8 come from this traversal's chunk (a
+            // refill abandons less than one such list, so under 1/7 of the
+            // entries are lost); longer lists take an exact range.
+            int64_t b = -1;
+            if (total > POOL_CHUNK / 8) {
+                const unsigned long long o = atomicAdd(a.pool_tail, (unsigned long long)total);
+                if ((int64_t)o + total <= a.pool_cap) b = (int64_t)o;
+            } else {
+                if (sh.pool_cur + total > sh.pool_end) {
+                    const unsigned long long o = atomicAdd(a.pool_tail, (unsigned long long)POOL_CHUNK);
+                    if ((int64_t)o + POOL_CHUNK > a.pool_cap) {
+                        sh.pool_cur = sh.pool_end = 0;
+                    } else {
+                        sh.pool_cur = (int64_t)o;
+                        sh.pool_end = (int64_t)o + POOL_CHUNK;
+                    }
+                }
+                if (sh.pool_cur + total <= sh.pool_end) {
+                    b = sh.pool_cur;
+                    sh.pool_cur += total;
                 }
             }
-            if (sh.pool_cur + total > sh.pool_end) {
-                atomicOr(a.status, ERR_POOL_OVERFLOW);
-                sh.pool_base = -1;
-            } else {
-                sh.pool_base = sh.pool_cur;
-                sh.pool_cur += total;
-            }
-            a.poff[slot] = sh.pool_base;
+            if (b < 0) atomicOr(a.status, ERR_POOL_OVERFLOW);
+            sh.pool_base = b;
+            a.poff[slot] = b;
         }
     }
     if (a.want_pattern) {
