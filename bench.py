@@ -524,7 +524,8 @@ def main():
             "edges_inspected_without_reuse": ideal.edges_inspected,
             "work_ratio": res.edges_inspected / max(ideal.edges_inspected, 1),
             "levels": res.levels, "reused_sources": res.reused_sources, "sources": res.sources,
-            "cycles_expand_output_clear": list(res.cycles), "ctas": res.ctas}
+            "cycles": dict(zip(("seed", "levels", "fold", "out_count", "out_write", "clear", "pair_wait"),
+                               res.cycles)), "ctas": res.ctas}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -111,7 +111,7 @@ class _CResult(ctypes.Structure):
         ("e_insp", ctypes.c_uint64),
         ("levels", ctypes.c_uint64),
         ("reused_sources", ctypes.c_uint64),
-        ("cycles", ctypes.c_uint64 * 3),
+        ("cycles", ctypes.c_uint64 * 7),
         ("ctas", ctypes.c_uint64),
         ("kernel_ms", ctypes.c_double),
         ("u_row_count", _i32p),
@@ -148,7 +148,7 @@ class Result:
     kernel_ms: float
     levels: int = 0
     reused_sources: int = 0
-    cycles: tuple = (0, 0, 0)
+    cycles: tuple = (0, 0, 0, 0, 0, 0, 0)
     ctas: int = 0
     u_row_count: Optional[np.ndarray] = None
     l_col_count: Optional[np.ndarray] = None

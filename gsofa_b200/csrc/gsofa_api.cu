@@ -359,8 +359,8 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         char *d_misc = (char *)ctx->grow(ctx->misc, 256);
         unsigned long long *d_piece = (unsigned long long *)d_misc;
         unsigned long long *d_tail = (unsigned long long *)(d_misc + 8);
-        unsigned long long *d_counters = (unsigned long long *)(d_misc + 16);   // 12 counters
-        uint32_t *d_status = (uint32_t *)(d_misc + 128);
+        unsigned long long *d_counters = (unsigned long long *)(d_misc + 16);   // 16 counters
+        uint32_t *d_status = (uint32_t *)(d_misc + 192);
         int32_t *d_pool = nullptr, *d_out = nullptr;
         if (want_pattern) {
             d_pool = (int32_t *)ctx->grow(ctx->pool, (size_t)pool_cap * sizeof(int32_t));
@@ -474,8 +474,8 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         else issue(args);
         GS_CUDA(cudaEventRecord(ctx->ev1, st));
 
-        unsigned long long h_misc[17];
-        GS_CUDA(cudaMemcpyAsync(h_misc, d_misc, 136, cudaMemcpyDeviceToHost, st));
+        unsigned long long h_misc[25];
+        GS_CUDA(cudaMemcpyAsync(h_misc, d_misc, sizeof(h_misc), cudaMemcpyDeviceToHost, st));
         int64_t tot[2];
         GS_CUDA(cudaMemcpyAsync(&tot[0], d_gptr + L, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
         GS_CUDA(cudaMemcpyAsync(&tot[1], d_gptr + (L + 1) + L, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
@@ -483,7 +483,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         const double t_done = now_ms();
         float ms = 0.f;
         GS_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-        const uint32_t status = (uint32_t)(h_misc[16] & 0xffffffffu);
+        const uint32_t status = (uint32_t)(h_misc[24] & 0xffffffffu);
         const unsigned long long edges = h_misc[2], nsrc = h_misc[3], nsn = h_misc[4];
         const unsigned long long xtot = h_misc[5], einsp = h_misc[6];
         const unsigned long long levels = h_misc[7], reused = h_misc[8];
@@ -533,7 +533,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
             r.e_insp = einsp;
             r.levels = levels;
             r.reused_sources = reused;
-            for (int q = 0; q < 3; q++) r.cycles[q] = h_misc[9 + q];
+            for (int q = 0; q < 7; q++) r.cycles[q] = h_misc[9 + q];
             r.ctas = (uint64_t)grid;
             if (part_count == 1) {
                 r.fill_count = r.nnz_u - mats[i]->orig_up + r.nnz_l - mats[i]->orig_lo;
@@ -1275,18 +1275,18 @@ extern "C" gsofa_status gsofa_symbfact_counts_noalloc(int device, void *cuda_str
         a.tile_last = tiles + 2 * ntiles;
         a.tile_sn = tiles + 3 * ntiles;
         a.counters = (unsigned long long *)(misc + 16);
-        a.status = (uint32_t *)(misc + 128);
+        a.status = (uint32_t *)(misc + 192);
         void *args[] = {&a};
         GS_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(BLOCK), args, smem, st));
         GS_CUDA(cudaMemcpyAsync(d_u_row_count, cnt, (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
         GS_CUDA(cudaMemcpyAsync(d_l_col_count, cnt + L, (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
-        unsigned long long hm[17];
+        unsigned long long hm[25];
         int64_t tot[2];
         GS_CUDA(cudaMemcpyAsync(hm, misc, sizeof(hm), cudaMemcpyDeviceToHost, st));
         GS_CUDA(cudaMemcpyAsync(&tot[0], gp + L, 8, cudaMemcpyDeviceToHost, st));
         GS_CUDA(cudaMemcpyAsync(&tot[1], gp + (L + 1) + L, 8, cudaMemcpyDeviceToHost, st));
         GS_CUDA(cudaStreamSynchronize(st));
-        if ((uint32_t)(hm[16] & 0xffffffffu) & ERR_QUEUE_OVERFLOW) return GSOFA_ERR_QUEUE_OVERFLOW;
+        if ((uint32_t)(hm[24] & 0xffffffffu) & ERR_QUEUE_OVERFLOW) return GSOFA_ERR_QUEUE_OVERFLOW;
         summary[0] = (uint64_t)(tot[0] + tot[1]) - hc[0] - hc[1];
         summary[1] = (uint64_t)(tot[0] + tot[1] + n);
         summary[2] = hm[4];

@@ -96,7 +96,8 @@ struct JobArgs {
     unsigned long long *counters; // [0] edges inspected, [1] sources, [2] sn total,
                                   // [3] pass-G expansions, [4] pass-G input degrees,
                                   // [5] levels, [6] sources that reused state,
-                                  // [7..9] cycles: expansion, output, clearing
+                                  // [7..13] cycles: seeding, levels, fold, output
+                                  // count, output write, clearing, pair wait
     uint32_t *status;
 };
 
@@ -353,6 +354,8 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         const int end = 0, start = 0;
         for (int32_t k = b0 + tid; k < e0; k += GT) GSOFA_VISIT(ld<CG>(g.adj + k));
     }
+    long long cs = 0;
+    if (tid == 0) { cs = clock64(); prof[1] += (unsigned long long)(cs - c0); }
 
     // level-synchronous expansion through vertices < s, one barrier a level
     int start = 0, wstart = 0;
@@ -453,6 +456,8 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         wstart = start;
         start = end;
     }
+    long long ce = 0;
+    if (tid == 0) { ce = clock64(); prof[2] += (unsigned long long)(ce - cs); }
 
     // fold the touched range into the chain range (warp reduce + shared atomics)
     {
@@ -466,7 +471,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
     }
     const int chain_hi = sh.chain_hi;
     long long c1 = 0;
-    if (tid == 0) { c1 = clock64(); prof[1] += (unsigned long long)(c1 - c0); }
+    if (tid == 0) { c1 = clock64(); prof[3] += (unsigned long long)(c1 - ce); }
 
     // hi(s) = set bits in (s, chain_hi].  Each warp owns a run of 32-word
     // chunks: it counts them, one cross-warp prefix gives its output offset,
@@ -507,6 +512,8 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         total = __shfl_sync(0xffffffffu, x, 31);
         wpre = __shfl_sync(0xffffffffu, x - v, wid);
     }
+    long long c2 = 0;
+    if (tid == 0) { c2 = clock64(); prof[4] += (unsigned long long)(c2 - c1); }
 
     const int64_t slot = (int64_t)pass * a.L + line;
     if (tid == 0) {
@@ -588,14 +595,16 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         }
     }
     gsync<GT>(bar);
-    if (tid == 0) prof[2] += (unsigned long long)(clock64() - c1);
+    if (tid == 0) prof[5] += (unsigned long long)(clock64() - c2);
 }
 #undef GSOFA_VISIT
 
 // Per-thread tallies of one CTA's traversals (summed over the CTA at the end).
 struct Tally {
     unsigned long long edges = 0, nsrc = 0, xcnt = 0, einsp = 0, nreuse = 0;
-    unsigned long long prof[4] = {0, 0, 0, 0};  // levels, expansion, output, clearing cycles
+    // levels, then cycles of: seeding, level loop, range fold, output count,
+    // output write, bitmap clearing, wait for the other pass (paired mode)
+    unsigned long long prof[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 // The sources s_lo, s_lo + stride, ... < s_hi of one work piece, in order,
@@ -640,7 +649,9 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
                            md.rawdeg, acc.xcnt, acc.einsp, acc.prof, gtid, bar);
         if (PAIRED) {
             if (gtid == 0) pair_flag[idx & 1][half] = sh.flag;
+            const long long cw = clock64();
             __syncthreads();
+            if (gtid == 0) acc.prof[7] += (unsigned long long)(clock64() - cw);
         }
         prev = s;
         if (gtid == 0) acc.nsrc++;
@@ -736,8 +747,8 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
         const int64_t ei = block_sum<BLOCK>((int64_t)acc.einsp, wsum);
         const int64_t ns = block_sum<BLOCK>((int64_t)acc.nsrc, wsum);
         const int64_t nr = block_sum<BLOCK>((int64_t)acc.nreuse, wsum);
-        int64_t pv[4];
-        for (int q = 0; q < 4; q++) pv[q] = block_sum<BLOCK>((int64_t)acc.prof[q], wsum);
+        int64_t pv[8];
+        for (int q = 0; q < 8; q++) pv[q] = block_sum<BLOCK>((int64_t)acc.prof[q], wsum);
         if (tid == 0) {
             atomicAdd(&a.counters[0], (unsigned long long)e);
             atomicAdd(&a.counters[1], (unsigned long long)ns);
@@ -745,9 +756,7 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
             atomicAdd(&a.counters[4], (unsigned long long)ei);
             atomicAdd(&a.counters[5], (unsigned long long)pv[0]);
             atomicAdd(&a.counters[6], (unsigned long long)nr);
-            atomicAdd(&a.counters[7], (unsigned long long)pv[1]);
-            atomicAdd(&a.counters[8], (unsigned long long)pv[2]);
-            atomicAdd(&a.counters[9], (unsigned long long)pv[3]);
+            for (int q = 1; q < 8; q++) atomicAdd(&a.counters[6 + q], (unsigned long long)pv[q]);
         }
     }
     grid.sync();

@@ -113,8 +113,10 @@ typedef struct gsofa_result {
                                 duplicates included)                      */
     uint64_t levels;         /* frontier levels summed over the traversals  */
     uint64_t reused_sources; /* traversals that started from s-1's state    */
-    uint64_t cycles[3];      /* SM cycles summed over CTAs: expansion,
-                                output (count + pattern), bitmap clearing  */
+    uint64_t cycles[7];      /* SM cycles summed over traversals: seeding,
+                                level loop, range fold, output count,
+                                output write, bitmap clearing, waiting
+                                for the other pass                          */
     uint64_t ctas;           /* CTAs of the persistent launch               */
     double kernel_ms;        /* factorization kernel time on the device     */
     /* per-line arrays (host, library-owned; NULL with NO_DOWNLOAD) */
