@@ -246,7 +246,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     // bitmap words rounded to 128 so its summary (one bit per word) is a
     // whole number of 16-byte groups
     const int32_t words_needed = ((max_n + 31) / 32 + 127) / 128 * 128;
-    const int32_t state_needed = words_needed + words_needed / 32;
+    const int32_t state_needed = words_needed + words_needed / 32 + ((words_needed / 32 + 31) / 32 + 3) / 4 * 4;
     const bool paired = reuse && p.reuse != 2 &&
                         (size_t)2 * state_needed * 4 + 2 * 1024 * 4 + sizeof(SharedState) * 2 + 1024 <=
                             ctx->smem_optin;
@@ -1144,7 +1144,7 @@ extern "C" gsofa_status gsofa_symbfact_counts_noalloc(int device, void *cuda_str
         constexpr int BLOCK = 256;
         void *kfn = factor_kernel_for(BLOCK, false);
         const int32_t bitmap_words = ((n + 31) / 32 + 127) / 128 * 128;
-        const int32_t state_words = bitmap_words + bitmap_words / 32;
+        const int32_t state_words = bitmap_words + bitmap_words / 32 + ((bitmap_words / 32 + 31) / 32 + 3) / 4 * 4;
         const int ring = 4096;
         const size_t smem = (size_t)state_words * 4 + (size_t)ring * 4;
         GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1514,7 +1514,7 @@ gsofa_status gsofa_server_create(gsofa_server **out, gsofa_server_config *cfg)
         const size_t static_smem = 2 * sizeof(SharedState) + 1024 + reserve;
         const int64_t per_half_words = ((int64_t)(s->optin - static_smem) / 2 - 1024 * 4) / 4;
         const int32_t limit_n =
-            (int32_t)std::min<int64_t>(per_half_words * 32 / 33 / 128 * 128 * 32, INT32_MAX);
+            (int32_t)std::min<int64_t>((per_half_words - 64) * 32 / 33 / 128 * 128 * 32, INT32_MAX);
         s->max_n = cfg->max_n > 0 ? cfg->max_n : limit_n;
         if (s->max_n > limit_n || s->max_n <= 0) { delete s; return GSOFA_ERR_UNSUPPORTED; }
         s->max_sn = cfg->max_supernode_size;
@@ -1522,7 +1522,7 @@ gsofa_status gsofa_server_create(gsofa_server **out, gsofa_server_config *cfg)
         s->max_slots = cfg->max_requests > 0 ? cfg->max_requests : 4096;
         s->idle_spins = std::max(1, (cfg->idle_exit_us > 0 ? cfg->idle_exit_us : 30000000) / 2);
         s->bitmap_words = ((s->max_n + 31) / 32 + 127) / 128 * 128;
-        s->state_words = s->bitmap_words + s->bitmap_words / 32;
+        s->state_words = s->bitmap_words + s->bitmap_words / 32 + ((s->bitmap_words / 32 + 31) / 32 + 3) / 4 * 4;
         // frontier ring: the largest that fits beside the two bitmaps
         void *kfn = (void *)serve_kernel<512>;
         s->ring = 0;

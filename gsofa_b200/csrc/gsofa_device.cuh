@@ -68,7 +68,7 @@ struct JobArgs {
     int32_t *queue;            // gridDim.x * qcap
     int64_t qcap;
     int32_t bitmap_words;      // shared-memory bitmap size (>= max n / 32, multiple of 128)
-    int32_t state_words;       // bitmap + its summary (bitmap_words / 32 words)
+    int32_t state_words;       // bitmap + its two summary levels
     int32_t ring_size;         // shared-memory frontier ring entries (power of two)
     int32_t lanes;             // lanes per frontier vertex: 1 (thread per vertex,
                                // warp for long rows) or 4..32
@@ -189,9 +189,18 @@ __device__ __forceinline__ int32_t ld(const int32_t *p)
     return *p;
 }
 
+// Words of a bitmap's first summary level (the bitmap is followed directly by
+// its summary, so their distance is the bitmap size).
+__device__ __forceinline__ int bm_summary_words(const uint32_t *bm, const uint32_t *summ)
+{
+    return (int)(summ - bm) >> 5;
+}
+
 // Bit test-and-set in the shared-memory bitmap; true when this call set it.
 // summ holds one bit per bitmap word, set when that word first becomes
 // nonzero, so output scans can skip empty stretches 32 words at a time.
+// summ is followed by a second level (one bit per summary word, i.e. per
+// 32K vertices) at summ + summary_words; SUMM2_OFF gives that offset.
 __device__ __forceinline__ bool test_and_set(uint32_t *bm, uint32_t *summ, int32_t m)
 {
     const uint32_t bit = 1u << (m & 31);
@@ -199,7 +208,11 @@ __device__ __forceinline__ bool test_and_set(uint32_t *bm, uint32_t *summ, int32
     uint32_t *w = bm + wi;
     if (*reinterpret_cast<volatile uint32_t *>(w) & bit) return false;
     const uint32_t old = atomicOr(w, bit);
-    if (old == 0u) atomicOr(summ + (wi >> 5), 1u << (wi & 31));
+    if (old == 0u) {
+        const int si = wi >> 5;
+        const uint32_t olds = atomicOr(summ + si, 1u << (wi & 31));
+        if (olds == 0u) atomicOr(summ + (bm_summary_words(bm, summ)) + (si >> 5), 1u << (si & 31));
+    }
     return !(old & bit);
 }
 
@@ -268,6 +281,28 @@ __device__ __forceinline__ void clear_range(uint32_t *bm, uint32_t *summ, int lo
     if (hi < lo) return;
     for (int w = (lo >> 5) + gtid; w <= (hi >> 5); w += GT) bm[w] = 0u;
     for (int w = (lo >> 10) + gtid; w <= (hi >> 10); w += GT) summ[w] = 0u;
+    uint32_t *summ2 = summ + bm_summary_words(bm, summ);
+    for (int w = (lo >> 15) + gtid; w <= (hi >> 15); w += GT) summ2[w] = 0u;
+}
+
+// Visits the nonzero chunks c in [c0, c1) (chunk = 32 bitmap words = one
+// summary word) in increasing order, using the second summary level to skip
+// empty stretches; fn(c) runs warp-uniformly.
+template <class F>
+__device__ __forceinline__ void for_nonzero_chunks(const uint32_t *summ2, int c0, int c1, F fn)
+{
+    int c = c0;
+    while (c < c1) {
+        const int wb = c & ~31;
+        uint32_t m = summ2[wb >> 5] & (~0u << (c & 31));
+        if (c1 - wb < 32) m &= (1u << (c1 - wb)) - 1u;
+        while (m) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1u;
+            fn(wb + b);
+        }
+        c = wb + 32;
+    }
 }
 
 // Barrier of the GT threads that work on one traversal: the whole CTA
@@ -487,16 +522,16 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
     const int ch0 = wid * per;
     const int ch1 = min(ch0 + per, max(nchunks, 0));
     const uint32_t first_mask = ~0u << ((s + 1) & 31);
+    const uint32_t *summ2 = summ + bm_summary_words(bm, summ);
     int wcount = 0;
-    for (int c = ch0; c < ch1; c++) {
-        const uint32_t sc = summ[cfirst + c];
-        if (!sc) continue;                              // warp-uniform
-        const int w = ((cfirst + c) << 5) + lane;
+    for_nonzero_chunks(summ2, cfirst + ch0, cfirst + ch1, [&](int cc) {
+        const uint32_t sc = summ[cc];
+        const int w = (cc << 5) + lane;
         uint32_t x = ((sc >> lane) & 1u) ? bm[w] : 0u;
         if (w < w0 || w > w1) x = 0u;
         if (w == w0) x &= first_mask;
         wcount += __popc(x);
-    }
+    });
     wcount = __reduce_add_sync(0xffffffffu, wcount);
     if (lane == 0) sh.warp[wid] = wcount;
     gsync<GT>(bar);
@@ -566,10 +601,9 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                 run += fill;
                 fill = 0;
             };
-            for (int c = ch0; c < ch1; c++) {
-                const uint32_t sc = summ[cfirst + c];
-                if (!sc) continue;
-                const int w = ((cfirst + c) << 5) + lane;
+            for_nonzero_chunks(summ2, cfirst + ch0, cfirst + ch1, [&](int cc) {
+                const uint32_t sc = summ[cc];
+                const int w = (cc << 5) + lane;
                 uint32_t x = ((sc >> lane) & 1u) ? bm[w] : 0u;
                 if (w < w0 || w > w1) x = 0u;
                 if (w == w0) x &= first_mask;
@@ -590,7 +624,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                 }
                 if (tot > slice) run += tot;
                 else fill += tot;
-            }
+            });
             flush();
         }
     }
