@@ -453,19 +453,34 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                     int32_t buf[8];
 #pragma unroll
                     for (int u = 0; u < 8; u++) buf[u] = (k0 + u < dl) ? ld<CG>(g.adj + b + k0 + u) : -1;
+                    // independent bit tests and sets first, then one enqueue
+                    // (warp scan + one shared atomic) for all new low vertices
+                    unsigned fresh = 0u;
 #pragma unroll
-                    for (int u = 0; u < 8; u++) {
-                        const int32_t m = buf[u];
-                        const bool fresh = m >= 0 && test_and_set(bm, summ, m);
-                        if (fresh) { t_lo = min(t_lo, m); t_hi = max(t_hi, m); }
-                        const bool low = fresh && m < s;
-                        const unsigned bal = __ballot_sync(0xffffffffu, low);
-                        if (bal) {
-                            int pb = 0;
-                            if (lane == 0) pb = atomicAdd(tailp, __popc(bal));
-                            pb = __shfl_sync(0xffffffffu, pb, 0);
-                            if (low) fr_put(f, end + pb + __popc(bal & ((1u << lane) - 1u)), start, m);
+                    for (int u = 0; u < 8; u++)
+                        if (buf[u] >= 0 && test_and_set(bm, summ, buf[u])) fresh |= 1u << u;
+                    int nlow = 0;
+#pragma unroll
+                    for (int u = 0; u < 8; u++)
+                        if ((fresh >> u) & 1u) {
+                            t_lo = min(t_lo, buf[u]);
+                            t_hi = max(t_hi, buf[u]);
+                            nlow += buf[u] < s;
                         }
+                    int incl = nlow;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                        if (lane >= o) incl += y;
+                    }
+                    const int wtot = __shfl_sync(0xffffffffu, incl, 31);
+                    if (wtot) {
+                        int pb = 0;
+                        if (lane == 0) pb = atomicAdd(tailp, wtot);
+                        pb = __shfl_sync(0xffffffffu, pb, 0) + (incl - nlow);
+#pragma unroll
+                        for (int u = 0; u < 8; u++)
+                            if (((fresh >> u) & 1u) && buf[u] < s) fr_put(f, end + pb++, start, buf[u]);
                     }
                 }
             }
