@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--lanes", type=int, default=0)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
+    ap.add_argument("--chunk", type=int, default=0, help="sources per work piece (0: library default)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -400,7 +401,7 @@ def main():
     ctx.set_stream(stream.cuda_stream)
     m = ctx.upload(g)
     params = gsofa_b200.Params.default(want_pattern=want_pattern, flags=gsofa_b200.FLAG_NO_DOWNLOAD,
-                                       reuse=args.reuse, block_size=args.block,
+                                       reuse=args.reuse, block_size=args.block, src_chunk=args.chunk,
                                        threads_per_source=args.lanes, ctas_per_sm=args.ctas_per_sm)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
@@ -447,7 +448,8 @@ def main():
         pe = torch.from_numpy(g.end).pin_memory()
         pa = torch.from_numpy(g.adj).pin_memory()
         pe2e = gsofa_b200.Params.default(want_pattern=want_pattern, reuse=args.reuse, block_size=args.block,
-                                         threads_per_source=args.lanes, ctas_per_sm=args.ctas_per_sm)
+                                         src_chunk=args.chunk, threads_per_source=args.lanes,
+                                         ctas_per_sm=args.ctas_per_sm)
         # page-locked result buffers, sized from the warm-up result, reused
         n1 = g.n + 1
 
