@@ -17,7 +17,7 @@ from . import Context, Matrix, Params
 
 DEFAULT_CANDIDATES: Tuple[Tuple[int, int, int], ...] = (
     # (block_size, threads_per_source, src_chunk)
-    (512, 1, 32), (1024, 1, 32), (256, 1, 32), (512, 1, 64), (512, 1, 16), (512, 8, 32),
+    (0, 1, 0), (1024, 1, 128), (1024, 1, 512), (512, 1, 0), (256, 1, 0), (1024, 8, 0),
 )
 
 _CACHE_ENV = "GSOFA_AUTOTUNE_CACHE"

@@ -257,7 +257,6 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     int lanes = p.threads_per_source ? p.threads_per_source : 1;
     if (lanes != 1 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
         return GSOFA_ERR_INVALID_INPUT;
-    int chunk = p.src_chunk > 0 ? p.src_chunk : (reuse ? 32 : 1);
 
     const int32_t bitmap_words = words_needed;
     const int32_t state_words = state_needed;
@@ -290,6 +289,15 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = p.ctas_per_sm > 0 ? std::min(p.ctas_per_sm, occ) : occ;
     const int grid = per_sm * ctx->sm_count;
+    // sources per work piece: a piece's first source cannot reuse state, so
+    // pieces are long (up to 512 sources) while there are still about eight
+    // per concurrent traversal -- the last pieces handed out are the light,
+    // low-numbered sources, so the launch's tail stays short
+    int chunk = p.src_chunk;
+    if (chunk <= 0) {
+        const int64_t per = (int64_t)(paired ? 1 : 2) * L / ((int64_t)8 * grid);
+        chunk = reuse ? (int)std::min<int64_t>(512, std::max<int64_t>(32, per)) : 1;
+    }
 
     // work ranges: biggest matrices first
     std::vector<int> order(count);
@@ -489,6 +497,9 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         const unsigned long long levels = h_misc[7], reused = h_misc[8];
 
         if (status & ERR_QUEUE_OVERFLOW) return GSOFA_ERR_QUEUE_OVERFLOW;
+        // a list's count and its pattern disagree: an internal fault, never
+        // a property of the input
+        if (status & ERR_COUNT_MISMATCH) return GSOFA_ERR_CUDA;
         if (want_pattern && (status & ERR_POOL_OVERFLOW)) {
             if (attempt == 0) {
                 pool_cap = pool_need(tot[0] + tot[1]);
@@ -1362,7 +1373,7 @@ struct gsofa_server {
     size_t optin = 0;
     int32_t max_n = 0;
     int32_t max_sn = 0;
-    int32_t chunk = 32;
+    int32_t chunk = 0;              // sources per piece; 0: from the request's n
     int32_t max_slots = 4096;
     int idle_spins = 10000;
     int block = 512, ring = 1024, grid = 0;
@@ -1518,7 +1529,7 @@ gsofa_status gsofa_server_create(gsofa_server **out, gsofa_server_config *cfg)
         s->max_n = cfg->max_n > 0 ? cfg->max_n : limit_n;
         if (s->max_n > limit_n || s->max_n <= 0) { delete s; return GSOFA_ERR_UNSUPPORTED; }
         s->max_sn = cfg->max_supernode_size;
-        s->chunk = cfg->src_chunk > 0 ? cfg->src_chunk : 32;
+        s->chunk = cfg->src_chunk > 0 ? cfg->src_chunk : 0;
         s->max_slots = cfg->max_requests > 0 ? cfg->max_requests : 4096;
         s->idle_spins = std::max(1, (cfg->idle_exit_us > 0 ? cfg->idle_exit_us : 30000000) / 2);
         s->bitmap_words = ((s->max_n + 31) / 32 + 127) / 128 * 128;
@@ -1632,7 +1643,12 @@ gsofa_status gsofa_server_submit(gsofa_server *s, int32_t n, int64_t nnz, const 
     ServerReq r;
     r.n = n;
     r.nnz = nnz;
-    const uint64_t npieces = ((uint64_t)n + s->chunk - 1) / s->chunk;
+    // long pieces for long requests (a piece's first source cannot reuse
+    // state), while keeping about eight pieces per resident CTA
+    const int32_t chunk = s->chunk > 0 ? s->chunk
+                                       : (int32_t)std::min<int64_t>(
+                                             512, std::max<int64_t>(32, (int64_t)n / (8 * std::max(s->grid, 1))));
+    const uint64_t npieces = ((uint64_t)n + chunk - 1) / chunk;
     const int cls = n < kSmallRequest ? 0 : 1;
     r.cls = cls;
     if (s->free_slots.empty()) return GSOFA_ERR_BUSY;
@@ -1737,8 +1753,8 @@ gsofa_status gsofa_server_submit(gsofa_server *s, int32_t n, int64_t nnz, const 
         std::vector<ServePiece> pcs((size_t)npieces);
         for (uint64_t k = 0; k < npieces; k++) {
             // highest sources first: they carry the largest traversals
-            const int64_t hi = (int64_t)n - (int64_t)k * s->chunk;
-            pcs[k] = ServePiece{r.slot, (int32_t)std::max<int64_t>(0, hi - s->chunk), (int32_t)hi, 0};
+            const int64_t hi = (int64_t)n - (int64_t)k * chunk;
+            pcs[k] = ServePiece{r.slot, (int32_t)std::max<int64_t>(0, hi - chunk), (int32_t)hi, 0};
         }
         ServePiece *ring = s->d_pieces + (size_t)cls * s->piece_cap;
         const uint64_t at = s->published[cls] % s->piece_cap;

@@ -56,6 +56,7 @@ struct Range {
 enum : uint32_t {
     ERR_POOL_OVERFLOW = 1u,
     ERR_QUEUE_OVERFLOW = 2u,
+    ERR_COUNT_MISMATCH = 4u,   // a list's running count and its bitmap disagree
 };
 
 struct JobArgs {
@@ -267,6 +268,12 @@ struct SharedState {
     int64_t pool_cur;  // this traversal's private slice of the pattern pool:
     int64_t pool_end;  // [pool_cur, pool_end), refilled POOL_CHUNK entries at a time
     int64_t warp[32];
+    // tallies kept by the half's first thread only: levels, then cycles of
+    // seeding, level loop, range fold and clearing, output count, output
+    // write, (unused), wait for the other pass; sources; reused sources
+    unsigned long long prof[8];
+    unsigned long long nsrc, nreuse;
+    int hcount;        // set bits above the current source (|hi(s)| once done)
 };
 
 // Pattern pool entries a traversal takes from the shared pool at a time (one
@@ -305,6 +312,42 @@ __device__ __forceinline__ void for_nonzero_chunks(const uint32_t *summ2, int c0
     }
 }
 
+// for_nonzero_chunks limited to the first `count` nonzero chunks.
+template <class F>
+__device__ __forceinline__ void for_nonzero_chunks_n(const uint32_t *summ2, int c0, int c1, int count, F fn)
+{
+    int c = c0;
+    while (c < c1 && count > 0) {
+        const int wb = c & ~31;
+        uint32_t m = summ2[wb >> 5] & (~0u << (c & 31));
+        if (c1 - wb < 32) m &= (1u << (c1 - wb)) - 1u;
+        while (m && count > 0) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1u;
+            fn(wb + b);
+            count--;
+        }
+        c = wb + 32;
+    }
+}
+
+// Position of the r-th (from 0) set bit of m, which must hold more than r
+// set bits: a binary search on popcounts of the low halves.
+__device__ __forceinline__ int select_bit(uint32_t m, int r)
+{
+    int pos = 0;
+#pragma unroll
+    for (int w = 16; w >= 1; w >>= 1) {
+        const int low = __popc(m & ((1u << w) - 1u));
+        if (r >= low) {
+            r -= low;
+            m >>= w;
+            pos += w;
+        }
+    }
+    return pos;
+}
+
 // Barrier of the GT threads that work on one traversal: the whole CTA
 // (bar == 0) or one half of it (named barrier `bar`).
 template <int GT>
@@ -339,7 +382,8 @@ __device__ __forceinline__ int32_t chain_start(const PassGraph &g, int32_t x, in
 }
 
 // Visits neighbour m of a frontier vertex: marks it, and queues it for the
-// next level when it lies below the source.
+// next level when it lies below the source, else counts it in nh (new
+// vertices above the source).
 #define GSOFA_VISIT(m)                                                          \
     do {                                                                        \
         const int32_t _m = (m);                                                 \
@@ -347,6 +391,7 @@ __device__ __forceinline__ int32_t chain_start(const PassGraph &g, int32_t x, in
             t_lo = min(t_lo, _m);                                               \
             t_hi = max(t_hi, _m);                                               \
             if (_m < s) push(f, tailp, end, start, _m);                         \
+            else nh++;                                                          \
         }                                                                       \
     } while (0)
 
@@ -375,6 +420,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         sh.tailc[0] = sh.tailc[1] = sh.tailc[2] = 0;
         sh.fetch[0] = sh.fetch[1] = sh.fetch[2] = 0;
         if (test_and_set(bm, summ, s)) { t_lo = s; t_hi = s; }
+        else sh.hcount--;   // s was in hi(s-1): counted, but not above s
     }
     gsync<GT>(bar);
 
@@ -387,7 +433,10 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         }
         int *tailp = &sh.tailc[0];
         const int end = 0, start = 0;
+        int nh = 0;
         for (int32_t k = b0 + tid; k < e0; k += GT) GSOFA_VISIT(ld<CG>(g.adj + k));
+        nh = (int)__reduce_add_sync(0xffffffffu, (unsigned)nh);
+        if (lane == 0 && nh) atomicAdd(&sh.hcount, nh);
     }
     long long cs = 0;
     if (tid == 0) { cs = clock64(); prof[1] += (unsigned long long)(cs - c0); }
@@ -439,6 +488,8 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                         if (fresh) { t_lo = min(t_lo, m); t_hi = max(t_hi, m); }
                         const bool low = fresh && m < s;
                         const unsigned bal = __ballot_sync(0xffffffffu, low);
+                        const unsigned bhi = __ballot_sync(0xffffffffu, fresh) & ~bal;
+                        if (lane == 0 && bhi) atomicAdd(&sh.hcount, __popc(bhi));
                         if (bal) {
                             int pb = 0;
                             if (lane == 0) pb = atomicAdd(tailp, __popc(bal));
@@ -459,25 +510,29 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
 #pragma unroll
                     for (int u = 0; u < 8; u++)
                         if (buf[u] >= 0 && test_and_set(bm, summ, buf[u])) fresh |= 1u << u;
-                    int nlow = 0;
+                    // new vertices below s in the low 16 bits, above s in
+                    // the high ones (a warp step finds at most 256)
+                    int nlh = 0;
 #pragma unroll
                     for (int u = 0; u < 8; u++)
                         if ((fresh >> u) & 1u) {
                             t_lo = min(t_lo, buf[u]);
                             t_hi = max(t_hi, buf[u]);
-                            nlow += buf[u] < s;
+                            nlh += buf[u] < s ? 1 : 0x10000;
                         }
-                    int incl = nlow;
+                    int incl = nlh;
 #pragma unroll
                     for (int o = 1; o < 32; o <<= 1) {
                         const int y = __shfl_up_sync(0xffffffffu, incl, o);
                         if (lane >= o) incl += y;
                     }
-                    const int wtot = __shfl_sync(0xffffffffu, incl, 31);
+                    const int wsum = __shfl_sync(0xffffffffu, incl, 31);
+                    const int wtot = wsum & 0xffff;
+                    if (lane == 0 && (wsum >> 16)) atomicAdd(&sh.hcount, wsum >> 16);
                     if (wtot) {
                         int pb = 0;
                         if (lane == 0) pb = atomicAdd(tailp, wtot);
-                        pb = __shfl_sync(0xffffffffu, pb, 0) + (incl - nlow);
+                        pb = __shfl_sync(0xffffffffu, pb, 0) + ((incl - nlh) & 0xffff);
 #pragma unroll
                         for (int u = 0; u < 8; u++)
                             if (((fresh >> u) & 1u) && buf[u] < s) fr_put(f, end + pb++, start, buf[u]);
@@ -489,6 +544,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
             const unsigned gmask = (lanes == 32)
                                        ? 0xffffffffu
                                        : (((1u << lanes) - 1u) << (lane & ~(lanes - 1)));
+            int nh = 0;
             for (;;) {
                 int it = 0;
                 if (lane_in_group == 0) it = atomicAdd(fetchp, 1);
@@ -502,6 +558,8 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                 }
                 for (int32_t k = b + lane_in_group; k < e; k += lanes) GSOFA_VISIT(ld<CG>(g.adj + k));
             }
+            nh = (int)__reduce_add_sync(0xffffffffu, (unsigned)nh);
+            if (lane == 0 && nh) atomicAdd(&sh.hcount, nh);
         }
         wstart = start;
         start = end;
@@ -509,7 +567,9 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
     long long ce = 0;
     if (tid == 0) { ce = clock64(); prof[2] += (unsigned long long)(ce - cs); }
 
-    // fold the touched range into the chain range (warp reduce + shared atomics)
+    // fold the touched range into the chain range (warp reduce + shared
+    // atomics; it is read only when the bitmap is cleared, after later
+    // barriers)
     {
         const int wl = __reduce_min_sync(0xffffffffu, t_lo);
         const int wh = __reduce_max_sync(0xffffffffu, t_hi);
@@ -517,54 +577,13 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
             if (wl != INT32_MAX) atomicMin(&sh.chain_lo, wl);
             if (wh >= 0) atomicMax(&sh.chain_hi, wh);
         }
-        gsync<GT>(bar);
     }
-    const int chain_hi = sh.chain_hi;
     long long c1 = 0;
     if (tid == 0) { c1 = clock64(); prof[3] += (unsigned long long)(c1 - ce); }
 
-    // hi(s) = set bits in (s, chain_hi].  Each warp owns a run of 32-word
-    // chunks: it counts them, one cross-warp prefix gives its output offset,
-    // then per chunk a warp scan places every lane's bits in sorted order.
-    constexpr int NWARP = GT / 32;
-    const int wid = tid >> 5;
-    const int w0 = (s + 1) >> 5;
-    const int w1 = (chain_hi > s) ? (chain_hi >> 5) : (w0 - 1);
-    // chunks are aligned groups of 32 words: one summary word each
-    const int cfirst = w0 >> 5;
-    const int nchunks = (w1 >= w0) ? (w1 >> 5) - cfirst + 1 : 0;
-    const int per = nchunks > 0 ? (nchunks + NWARP - 1) / NWARP : 0;
-    const int ch0 = wid * per;
-    const int ch1 = min(ch0 + per, max(nchunks, 0));
-    const uint32_t first_mask = ~0u << ((s + 1) & 31);
-    const uint32_t *summ2 = summ + bm_summary_words(bm, summ);
-    int wcount = 0;
-    for_nonzero_chunks(summ2, cfirst + ch0, cfirst + ch1, [&](int cc) {
-        const uint32_t sc = summ[cc];
-        const int w = (cc << 5) + lane;
-        uint32_t x = ((sc >> lane) & 1u) ? bm[w] : 0u;
-        if (w < w0 || w > w1) x = 0u;
-        if (w == w0) x &= first_mask;
-        wcount += __popc(x);
-    });
-    wcount = __reduce_add_sync(0xffffffffu, wcount);
-    if (lane == 0) sh.warp[wid] = wcount;
-    gsync<GT>(bar);
-    int64_t wpre = 0, total = 0;
-    {
-        const int64_t v = lane < NWARP ? sh.warp[lane] : 0;
-        int64_t x = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        total = __shfl_sync(0xffffffffu, x, 31);
-        wpre = __shfl_sync(0xffffffffu, x - v, wid);
-    }
-    long long c2 = 0;
-    if (tid == 0) { c2 = clock64(); prof[4] += (unsigned long long)(c2 - c1); }
-
+    // |hi(s)| = the bits above s: the traversal's running count, complete
+    // since the level loop's last barrier
+    const int total = sh.hcount;
     const int64_t slot = (int64_t)pass * a.L + line;
     if (tid == 0) {
         a.cnt[slot] = (int32_t)total;
@@ -599,29 +618,97 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
             a.poff[slot] = b;
         }
     }
+    long long c2 = 0;
     if (a.want_pattern) {
-        gsync<GT>(bar);
-        const int64_t base = sh.pool_base;
-        if (base >= 0 && wcount > 0) {
-            // Entries go through this warp's slice of the frontier ring (idle
-            // once the traversal is done) and leave in coalesced runs.
-            const int slice = f.ring_size / NWARP;
-            int32_t *stage = f.ring + wid * slice;
-            int64_t run = base + wpre;   // global position of stage[0]
-            int fill = 0;
-            auto flush = [&]() {
-                __syncwarp();
-                for (int i = lane; i < fill; i += 32) a.pool[run + i] = stage[i];
-                __syncwarp();
-                run += fill;
-                fill = 0;
+        // hi(s) = set bits above s, read in chunks of 32 bitmap words (one
+        // summary word each).  The nonzero chunks -- the set bits of the
+        // second summary level -- are split into NWARP runs of equal count,
+        // one per warp in increasing order, so a list whose bits crowd into a
+        // few chunks still spreads over several warps, and each warp walks
+        // only its own chunks.  Bits above the chain's highest vertex are
+        // clear at every level, so the runs end there by themselves.
+        constexpr int NWARP = GT / 32;
+        const int wid = tid >> 5;
+        const int w0 = (s + 1) >> 5;
+        const int cfirst = w0 >> 5;
+        const int cend = a.bitmap_words >> 5;   // chunks [cfirst, cend)
+        const uint32_t first_mask = ~0u << ((s + 1) & 31);
+        const uint32_t *summ2 = summ + bm_summary_words(bm, summ);
+        // this lane's word of chunk cc, without the bits up to s
+        auto chunk_word = [&](int cc) -> uint32_t {
+            const int w = (cc << 5) + lane;
+            uint32_t x = ((summ[cc] >> lane) & 1u) ? bm[w] : 0u;
+            if (w < w0) x = 0u;
+            if (w == w0) x &= first_mask;
+            return x;
+        };
+        int c_run = cend, n_run = 0;   // this warp's run: n_run nonzero chunks from c_run
+        if (cend > cfirst) {
+            const int sw0 = cfirst >> 5, sw1 = (cend - 1) >> 5;
+            auto sword = [&](int w) -> uint32_t {
+                uint32_t m = summ2[w];
+                if (w == sw0) m &= ~0u << (cfirst & 31);
+                return m;
             };
-            for_nonzero_chunks(summ2, cfirst + ch0, cfirst + ch1, [&](int cc) {
-                const uint32_t sc = summ[cc];
-                const int w = (cc << 5) + lane;
-                uint32_t x = ((sc >> lane) & 1u) ? bm[w] : 0u;
-                if (w < w0 || w > w1) x = 0u;
-                if (w == w0) x &= first_mask;
+            int z = 0;
+            for (int w = sw0 + lane; w <= sw1; w += 32) z += __popc(sword(w));
+            z = (int)__reduce_add_sync(0xffffffffu, (unsigned)z);
+            const int k0 = (int)((int64_t)wid * z / NWARP);
+            n_run = (int)((int64_t)(wid + 1) * z / NWARP) - k0;
+            if (n_run > 0) {
+                int carry = 0;
+                for (int wb = sw0; wb <= sw1; wb += 32) {
+                    const int w = wb + lane;
+                    const uint32_t m = w <= sw1 ? sword(w) : 0u;
+                    const int pc = __popc(m);
+                    int incl = pc;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                        if (lane >= o) incl += y;
+                    }
+                    const int excl = carry + incl - pc;
+                    const unsigned hit = __ballot_sync(0xffffffffu, excl <= k0 && k0 < excl + pc);
+                    if (hit) {
+                        const int src = __ffs(hit) - 1;
+                        const int c = (w << 5) + select_bit(m, k0 - excl);
+                        c_run = __shfl_sync(0xffffffffu, c, src);
+                        break;
+                    }
+                    carry += __shfl_sync(0xffffffffu, incl, 31);
+                }
+            }
+        }
+        int wcount = 0;
+        for_nonzero_chunks_n(summ2, c_run, cend, n_run, [&](int cc) { wcount += __popc(chunk_word(cc)); });
+        wcount = (int)__reduce_add_sync(0xffffffffu, (unsigned)wcount);
+        if (lane == 0) sh.warp[wid] = wcount;
+        gsync<GT>(bar);
+        if (tid == 0) { c2 = clock64(); prof[4] += (unsigned long long)(c2 - c1); }
+        int wpre = 0, all = 0;   // entries of the warps before this one; of all
+        {
+            const int v = lane < NWARP ? (int)sh.warp[lane] : 0;
+            int x = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            wpre = __shfl_sync(0xffffffffu, x - v, wid);
+            all = __shfl_sync(0xffffffffu, x, 31);
+        }
+        // the pool range holds `total` entries: write nothing if the bitmap
+        // says otherwise
+        if (tid == 0 && all != total) atomicOr(a.status, ERR_COUNT_MISMATCH);
+        const int64_t base = sh.pool_base;
+        if (base >= 0 && wcount > 0 && all == total) {
+            // A chunk whose words hold at most two entries each is written a
+            // word per lane; denser chunks a word at a time across the warp,
+            // lane = bit, so every store is one coalesced run.
+            int32_t *out = a.pool + base + wpre;
+            int pos = 0;
+            for_nonzero_chunks_n(summ2, c_run, cend, n_run, [&](int cc) {
+                uint32_t x = chunk_word(cc);
                 const int pc = __popc(x);
                 int incl = pc;
 #pragma unroll
@@ -629,31 +716,41 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                     const int y = __shfl_up_sync(0xffffffffu, incl, o);
                     if (lane >= o) incl += y;
                 }
-                const int tot = __shfl_sync(0xffffffffu, incl, 31);
-                if (fill + tot > slice) flush();
-                int32_t *dst = (tot > slice) ? a.pool + run + (incl - pc) : stage + fill + (incl - pc);
-                while (x) {
-                    const int bit = __ffs(x) - 1;
-                    x &= x - 1u;
-                    *dst++ = (w << 5) + bit;
+                const int excl = incl - pc;
+                const int wbase = (cc << 5);
+                if (__reduce_max_sync(0xffffffffu, (unsigned)pc) <= 2u) {
+                    int32_t *dst = out + pos + excl;
+                    while (x) {
+                        const int bit = __ffs(x) - 1;
+                        x &= x - 1u;
+                        *dst++ = ((wbase + lane) << 5) + bit;
+                    }
+                } else {
+                    unsigned nzw = __ballot_sync(0xffffffffu, x != 0u);
+                    const uint32_t below = (1u << lane) - 1u;
+                    while (nzw) {
+                        const int j = __ffs(nzw) - 1;
+                        nzw &= nzw - 1u;
+                        const uint32_t xj = __shfl_sync(0xffffffffu, x, j);
+                        const int pj = __shfl_sync(0xffffffffu, excl, j);
+                        if ((xj >> lane) & 1u) out[pos + pj + __popc(xj & below)] = ((wbase + j) << 5) + lane;
+                    }
                 }
-                if (tot > slice) run += tot;
-                else fill += tot;
+                pos += __shfl_sync(0xffffffffu, incl, 31);
             });
-            flush();
         }
+    } else if (tid == 0) {
+        c2 = c1;
     }
     gsync<GT>(bar);
     if (tid == 0) prof[5] += (unsigned long long)(clock64() - c2);
 }
 #undef GSOFA_VISIT
 
-// Per-thread tallies of one CTA's traversals (summed over the CTA at the end).
+// Per-thread tallies of one CTA's traversals (summed over the CTA at the
+// end); the per-source ones live in SharedState, kept by one thread.
 struct Tally {
-    unsigned long long edges = 0, nsrc = 0, xcnt = 0, einsp = 0, nreuse = 0;
-    // levels, then cycles of: seeding, level loop, range fold, output count,
-    // output write, bitmap clearing, wait for the other pass (paired mode)
-    unsigned long long prof[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned long long edges = 0, xcnt = 0, einsp = 0;
 };
 
 // The sources s_lo, s_lo + stride, ... < s_hi of one work piece, in order,
@@ -688,22 +785,22 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
             clear_range<GT>(bm, summ, clo, chi, gtid);
             gsync<GT>(bar);
             if (gtid == 0) {
-                sh.chain_lo = INT32_MAX; sh.chain_hi = -1;
-                acc.prof[3] += (unsigned long long)(clock64() - cc);
+                sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0;
+                sh.prof[3] += (unsigned long long)(clock64() - cc);
             }
         } else if (gtid == 0) {
-            acc.nreuse++;
+            sh.nreuse++;
         }
         process_source<GT, CG>(a, g, md.n, md.line_base + s, pass, s, bm, summ, fr, sh, acc.edges,
-                           md.rawdeg, acc.xcnt, acc.einsp, acc.prof, gtid, bar);
+                           md.rawdeg, acc.xcnt, acc.einsp, sh.prof, gtid, bar);
         if (PAIRED) {
             if (gtid == 0) pair_flag[idx & 1][half] = sh.flag;
             const long long cw = clock64();
             __syncthreads();
-            if (gtid == 0) acc.prof[7] += (unsigned long long)(clock64() - cw);
+            if (gtid == 0) sh.prof[7] += (unsigned long long)(clock64() - cw);
         }
         prev = s;
-        if (gtid == 0) acc.nsrc++;
+        if (gtid == 0) sh.nsrc++;
     }
 }
 
@@ -738,7 +835,11 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
 
     // ---- phase 1: traversals ------------------------------------------------
     for (int w = tid; w < NS * a.state_words; w += BLOCK) smem_dyn[w] = 0u;
-    if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.pool_cur = sh.pool_end = 0; }
+    if (gtid == 0) {
+        sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0; sh.pool_cur = sh.pool_end = 0;
+        for (int q = 0; q < 8; q++) sh.prof[q] = 0;
+        sh.nsrc = sh.nreuse = 0;
+    }
     const Frontier fr{ring, a.queue + ((int64_t)blockIdx.x * NS + half) * a.qcap, a.qcap, a.status,
                       a.ring_size};
     Tally acc;
@@ -770,8 +871,9 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
             // cut pieces where adjacency chains start, so a piece's first
             // source rarely has a predecessor it could have reused
             if (tid < 32) {
-                const int32_t lo = (j0 == 0) ? s_lo : chain_start(g, s_lo, rg.chunk);
-                const int32_t hi = (j1 == rg.nj) ? s_hi : chain_start(g, s_hi, rg.chunk);
+                const int32_t lim = min(rg.chunk, 64);
+                const int32_t lo = (j0 == 0) ? s_lo : chain_start(g, s_lo, lim);
+                const int32_t hi = (j1 == rg.nj) ? s_hi : chain_start(g, s_hi, lim);
                 if (tid == 0) { sh.seg[0] = lo; sh.seg[1] = hi; }
             }
             __syncthreads();
@@ -785,7 +887,7 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
             const int clo = sh.chain_lo, chi = sh.chain_hi;
             clear_range<GT>(bm, summ, clo, chi, gtid);
             __syncthreads();
-            if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
+            if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0; }
             __syncthreads();
         }
     }
@@ -794,11 +896,13 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
         const int64_t e = block_sum<BLOCK>((int64_t)acc.edges, wsum);
         const int64_t x = block_sum<BLOCK>((int64_t)acc.xcnt, wsum);
         const int64_t ei = block_sum<BLOCK>((int64_t)acc.einsp, wsum);
-        const int64_t ns = block_sum<BLOCK>((int64_t)acc.nsrc, wsum);
-        const int64_t nr = block_sum<BLOCK>((int64_t)acc.nreuse, wsum);
-        int64_t pv[8];
-        for (int q = 0; q < 8; q++) pv[q] = block_sum<BLOCK>((int64_t)acc.prof[q], wsum);
         if (tid == 0) {
+            unsigned long long ns = 0, nr = 0, pv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (int h = 0; h < NS; h++) {
+                ns += shs[h].nsrc;
+                nr += shs[h].nreuse;
+                for (int q = 0; q < 8; q++) pv[q] += shs[h].prof[q];
+            }
             atomicAdd(&a.counters[0], (unsigned long long)e);
             atomicAdd(&a.counters[1], (unsigned long long)ns);
             atomicAdd(&a.counters[3], (unsigned long long)x);
@@ -822,7 +926,8 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
         }
         return lo;
     };
-    // supernode run boundary before line l (SURVEY a11 definition)
+    // supernode run boundary before line l: lines l-1 and l join when each
+    // is in the other's line and line l's upper count is one less
     auto sn_flag = [&](int64_t l) -> bool {
         const MatDesc &md = a.mats[mat_of(l)];
         const int64_t s = l - md.line_base;

@@ -79,7 +79,11 @@ __global__ void __launch_bounds__(BLOCK) serve_kernel(ServeArgs sa)
     uint32_t *summ = bm + a.bitmap_words;
     int32_t *ring = (int32_t *)(smem_dyn + (size_t)2 * a.state_words) + (size_t)half * a.ring_size;
     for (int w = tid; w < 2 * a.state_words; w += BLOCK) smem_dyn[w] = 0u;
-    if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
+    if (gtid == 0) {
+        sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0;
+        for (int q = 0; q < 8; q++) sh.prof[q] = 0;
+        sh.nsrc = sh.nreuse = 0;
+    }
     const Frontier fr{ring, a.queue + ((int64_t)blockIdx.x * 2 + half) * a.qcap, a.qcap, a.status,
                       a.ring_size};
     Tally acc;
@@ -119,7 +123,7 @@ __global__ void __launch_bounds__(BLOCK) serve_kernel(ServeArgs sa)
             const int clo = sh.chain_lo, chi = sh.chain_hi;
             clear_range<GT>(bm, summ, clo, chi, gtid);
             __syncthreads();
-            if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; }
+            if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0; }
         }
         if (tid == 0) {
             __threadfence();

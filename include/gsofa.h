@@ -63,7 +63,8 @@ typedef struct gsofa_matrix gsofa_matrix; /* device-resident G and G^T     */
 
 /* Tuning and output parameters; zero means "choose automatically". */
 typedef struct gsofa_params {
-    int32_t src_chunk;          /* consecutive sources per work item          */
+    int32_t src_chunk;          /* consecutive sources per work item; 0: 32 to
+                                   512, about eight pieces per resident CTA  */
     int32_t block_size;         /* threads per CTA: 128, 256, 512 or 1024     */
     int32_t threads_per_source; /* lanes expanding one frontier vertex:
                                    1 (default: one thread per vertex, a warp
@@ -232,7 +233,8 @@ typedef struct gsofa_server_config {
     int64_t mem_budget_bytes;   /* device bytes the server may hold; 0: 90%
                                    of the free memory                       */
     int32_t max_supernode_size; /* as in gsofa_params                       */
-    int32_t src_chunk;          /* sources per work piece; 0: 32            */
+    int32_t src_chunk;          /* sources per work piece; 0: 32 to 512 from
+                                   each request's n                         */
     int32_t max_requests;       /* requests in flight; 0: 4096             */
     int32_t idle_exit_us;       /* safety bound on how long an idle CTA
                                    waits for work (the host stops the kernel
