@@ -406,7 +406,11 @@ def main():
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     res = None
-    for _ in range(max(args.warmup, 0)):
+    # warm-up steps are timed steps untimed: the L2 flush runs too, so its
+    # kernel is loaded before the timed region starts
+    for i in range(max(args.warmup, 0)):
+        if i:
+            flush.fill_(i & 0xff)
         res = ctx.symbfact(m, params)
     if res is None:
         res = ctx.symbfact(m, params)
@@ -462,7 +466,8 @@ def main():
             bufs.update(u_ptr=pinned(n1, torch.int64), l_ptr=pinned(n1, torch.int64),
                         u_idx=pinned(res.nnz_u, torch.int32), l_idx=pinned(res.nnz_l, torch.int32))
         out = None
-        for _ in range(1):   # warm the host-side allocations
+        for _ in range(2):   # warm the host-side allocations
+            flush.fill_(1)
             mm = ctx.upload(pb.numpy(), pe.numpy(), pa.numpy())
             out = ctx.symbfact_into(mm, pe2e, bufs)
             mm.free()

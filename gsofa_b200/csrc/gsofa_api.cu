@@ -79,7 +79,7 @@ struct gsofa_ctx {
     cudaStream_t own_stream = nullptr;  // the context's own stream
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // job scratch
-    DevBuf queue, cnt, nxt, poff, gptr, lrow, snind, snlist, tiles, misc, pool, out, mats, ranges;
+    DevBuf queue, cnt, nxt, poff, gptr, lrow, snind, snlist, tiles, misc, pool, out, mats, ranges, stamp;
     // upload staging
     DevBuf st_beg, st_end, st_adj, st_tmp;
     std::vector<gsofa_matrix *> matrices;
@@ -370,9 +370,14 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         unsigned long long *d_counters = (unsigned long long *)(d_misc + 16);   // 16 counters
         uint32_t *d_status = (uint32_t *)(d_misc + 192);
         int32_t *d_pool = nullptr, *d_out = nullptr;
+        uint16_t *d_stamp = nullptr;
+        // a 16-bit chain index per vertex for every traversal: its lists are
+        // read off the bitmap when the chain ends
+        const int64_t stamp_stride = (int64_t)bitmap_words * 32;
         if (want_pattern) {
             d_pool = (int32_t *)ctx->grow(ctx->pool, (size_t)pool_cap * sizeof(int32_t));
             d_out = (int32_t *)ctx->grow(ctx->out, (size_t)pool_cap * sizeof(int32_t));
+            d_stamp = (uint16_t *)ctx->grow(ctx->stamp, (size_t)grid * NS * stamp_stride * sizeof(uint16_t));
         }
         MatDesc *d_mats = (MatDesc *)ctx->grow(ctx->mats, md.size() * sizeof(MatDesc));
         int64_t *d_minfo = (int64_t *)ctx->grow(ctx->matinfo, (size_t)3 * count * sizeof(int64_t));
@@ -414,6 +419,8 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         a.tile_sn = d_tiles + 3 * ntiles;
         a.counters = d_counters;
         a.status = d_status;
+        a.stamp = d_stamp;
+        a.stamp_stride = stamp_stride;
 
         // The job: descriptor copies, clears and the cooperative launch.  With
         // GSOFA_FLAG_GRAPH it is captured once into a CUDA graph and replayed
@@ -716,7 +723,7 @@ void gsofa_destroy(gsofa_ctx *c)
     while (!c->matrices.empty()) gsofa_matrix_free(c->matrices.back());
     DevBuf *bufs[] = {&c->queue, &c->cnt, &c->nxt, &c->poff, &c->gptr, &c->lrow, &c->snind,
                       &c->snlist, &c->tiles, &c->misc, &c->pool, &c->out, &c->mats, &c->ranges,
-                      &c->st_beg, &c->st_end, &c->st_adj, &c->st_tmp, &c->matinfo};
+                      &c->st_beg, &c->st_end, &c->st_adj, &c->st_tmp, &c->matinfo, &c->stamp};
     for (DevBuf *b : bufs) c->release(*b);
     if (c->graph.exec) cudaGraphExecDestroy(c->graph.exec);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1017,6 +1024,8 @@ size_t gsofa_predict_scratch_bytes(const gsofa_ctx *c, int32_t n, int64_t nnz,
     b += L * (2 * 4 + 2 + 2 * 8 + 4 + 1 + 4);   // cnt, nxt, poff, lrow, snind, sn list
     b += 2 * (L + 1) * 8;                       // gptr
     b += (size_t)(n + 1) * 8 + (size_t)nnz * 8; // G and G^T
+    if (p.want_pattern)                         // chain stamps, two traversals a CTA
+        b += grid * 2 * ((size_t)(n + 4095) / 4096 * 4096) * 2;
     return b;
 }
 

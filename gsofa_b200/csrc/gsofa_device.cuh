@@ -100,6 +100,8 @@ struct JobArgs {
                                   // [7..13] cycles: seeding, levels, fold, output
                                   // count, output write, clearing, pair wait
     uint32_t *status;
+    uint16_t *stamp;           // pattern mode: per traversal, stamp_stride entries:
+    int64_t stamp_stride;      // the chain index at which each vertex was first set
 };
 
 constexpr int TILE = 2048;     // lines per tile in the post-traversal phases
@@ -274,7 +276,22 @@ struct SharedState {
     unsigned long long prof[8];
     unsigned long long nsrc, nreuse;
     int hcount;        // set bits above the current source (|hi(s)| once done)
+    // the current chain -- consecutive sources sharing one bitmap -- whose
+    // lists are written when it ends (pattern mode)
+    uint16_t *stamp;   // this traversal's stamp row, or null (counts only)
+    int chain_s0;      // its first source
+    int chain_len;     // its sources so far (the current one included)
+    int chain_idx;     // index of the current source in it
+    int64_t chain_total;  // entries of its lists
 };
+
+// Records that v was first set while the chain's source chain_idx ran.
+// Only vertices above the chain's first source can appear in its lists.
+__device__ __forceinline__ void stamp_set(const SharedState &sh, int32_t v)
+{
+    uint16_t *st = sh.stamp;
+    if (st != nullptr && v > sh.chain_s0) st[v] = (uint16_t)sh.chain_idx;
+}
 
 // Pattern pool entries a traversal takes from the shared pool at a time (one
 // global atomic per chunk instead of one per source).
@@ -310,42 +327,6 @@ __device__ __forceinline__ void for_nonzero_chunks(const uint32_t *summ2, int c0
         }
         c = wb + 32;
     }
-}
-
-// for_nonzero_chunks limited to the first `count` nonzero chunks.
-template <class F>
-__device__ __forceinline__ void for_nonzero_chunks_n(const uint32_t *summ2, int c0, int c1, int count, F fn)
-{
-    int c = c0;
-    while (c < c1 && count > 0) {
-        const int wb = c & ~31;
-        uint32_t m = summ2[wb >> 5] & (~0u << (c & 31));
-        if (c1 - wb < 32) m &= (1u << (c1 - wb)) - 1u;
-        while (m && count > 0) {
-            const int b = __ffs(m) - 1;
-            m &= m - 1u;
-            fn(wb + b);
-            count--;
-        }
-        c = wb + 32;
-    }
-}
-
-// Position of the r-th (from 0) set bit of m, which must hold more than r
-// set bits: a binary search on popcounts of the low halves.
-__device__ __forceinline__ int select_bit(uint32_t m, int r)
-{
-    int pos = 0;
-#pragma unroll
-    for (int w = 16; w >= 1; w >>= 1) {
-        const int low = __popc(m & ((1u << w) - 1u));
-        if (r >= low) {
-            r -= low;
-            m >>= w;
-            pos += w;
-        }
-    }
-    return pos;
 }
 
 // Barrier of the GT threads that work on one traversal: the whole CTA
@@ -390,6 +371,7 @@ __device__ __forceinline__ int32_t chain_start(const PassGraph &g, int32_t x, in
         if (test_and_set(bm, summ, _m)) {                                             \
             t_lo = min(t_lo, _m);                                               \
             t_hi = max(t_hi, _m);                                               \
+            stamp_set(sh, _m);                                                  \
             if (_m < s) push(f, tailp, end, start, _m);                         \
             else nh++;                                                          \
         }                                                                       \
@@ -419,7 +401,9 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         c0 = clock64();
         sh.tailc[0] = sh.tailc[1] = sh.tailc[2] = 0;
         sh.fetch[0] = sh.fetch[1] = sh.fetch[2] = 0;
-        if (test_and_set(bm, summ, s)) { t_lo = s; t_hi = s; }
+        sh.chain_idx = sh.chain_len;
+        sh.chain_len = sh.chain_idx + 1;
+        if (test_and_set(bm, summ, s)) { t_lo = s; t_hi = s; stamp_set(sh, s); }
         else sh.hcount--;   // s was in hi(s-1): counted, but not above s
     }
     gsync<GT>(bar);
@@ -485,7 +469,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                         const bool on = k0 + lane < hd;
                         const int32_t m = on ? ld<CG>(g.adj + hb + k0 + lane) : 0;
                         const bool fresh = on && test_and_set(bm, summ, m);
-                        if (fresh) { t_lo = min(t_lo, m); t_hi = max(t_hi, m); }
+                        if (fresh) { t_lo = min(t_lo, m); t_hi = max(t_hi, m); stamp_set(sh, m); }
                         const bool low = fresh && m < s;
                         const unsigned bal = __ballot_sync(0xffffffffu, low);
                         const unsigned bhi = __ballot_sync(0xffffffffu, fresh) & ~bal;
@@ -520,6 +504,11 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                             t_hi = max(t_hi, buf[u]);
                             nlh += buf[u] < s ? 1 : 0x10000;
                         }
+                    if (fresh && sh.stamp != nullptr) {
+#pragma unroll
+                        for (int u = 0; u < 8; u++)
+                            if ((fresh >> u) & 1u) stamp_set(sh, buf[u]);
+                    }
                     int incl = nlh;
 #pragma unroll
                     for (int o = 1; o < 32; o <<= 1) {
@@ -582,22 +571,49 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
     if (tid == 0) { c1 = clock64(); prof[3] += (unsigned long long)(c1 - ce); }
 
     // |hi(s)| = the bits above s: the traversal's running count, complete
-    // since the level loop's last barrier
-    const int total = sh.hcount;
-    const int64_t slot = (int64_t)pass * a.L + line;
+    // since the level loop's last barrier.  The lists themselves are written
+    // when the chain ends (output_chain); here only the count and the link
+    // flag.
     if (tid == 0) {
+        const int total = sh.hcount;
+        const int64_t slot = (int64_t)pass * a.L + line;
         a.cnt[slot] = (int32_t)total;
         const int nx = (s + 1 < n) && ((bm[(s + 1) >> 5] >> ((s + 1) & 31)) & 1u);
         a.nxt[slot] = (uint8_t)nx;
         sh.flag = nx;
-        if (a.want_pattern) {
-            // Lists up to POOL_CHUNK / 8 come from this traversal's chunk (a
-            // refill abandons less than one such list, so under 1/7 of the
-            // entries are lost); longer lists take an exact range.
-            int64_t b = -1;
+        sh.chain_total += total;
+    }
+    gsync<GT>(bar);
+    if (tid == 0) prof[4] += (unsigned long long)(clock64() - c1);
+}
+#undef GSOFA_VISIT
+
+// Writes the lists of the chain that just ended -- sources chain_s0 ..
+// chain_s0 + chain_len - 1, which shared one bitmap -- while the bitmap still
+// holds the last source's traversal.  Bits are only ever added along a chain,
+// so the bits above source i of the chain that were set by the time it
+// finished are its list: hi(s_i) = { v > s_i : v set, stamp(v) <= i }.  One
+// pool range holds all of the chain's lists; each warp then writes whole
+// lists on its own, in increasing order, with no barrier per source.
+template <int GT>
+__device__ void output_chain(const JobArgs &a, int64_t line0, int pass, const uint32_t *bm,
+                             const uint32_t *summ, SharedState &sh, int gtid, int bar)
+{
+    constexpr int NWARP = GT / 32;
+    const int lane = gtid & 31, wid = gtid >> 5;
+    const int s0 = sh.chain_s0, len = sh.chain_len;
+    const int64_t row0 = (int64_t)pass * a.L + line0;   // cnt / poff entry of s0
+    // warp 0: one pool range for the chain, then every list's offset
+    if (wid == 0) {
+        long long base = -1;
+        if (lane == 0) {
+            // Ranges up to POOL_CHUNK / 8 come from this traversal's chunk (a
+            // refill abandons less than one such range, so under 1/7 of the
+            // entries are lost); longer ones take an exact range.
+            const int64_t total = sh.chain_total;
             if (total > POOL_CHUNK / 8) {
                 const unsigned long long o = atomicAdd(a.pool_tail, (unsigned long long)total);
-                if ((int64_t)o + total <= a.pool_cap) b = (int64_t)o;
+                if ((int64_t)o + total <= a.pool_cap) base = (long long)o;
             } else {
                 if (sh.pool_cur + total > sh.pool_end) {
                     const unsigned long long o = atomicAdd(a.pool_tail, (unsigned long long)POOL_CHUNK);
@@ -609,143 +625,103 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                     }
                 }
                 if (sh.pool_cur + total <= sh.pool_end) {
-                    b = sh.pool_cur;
+                    base = sh.pool_cur;
                     sh.pool_cur += total;
                 }
             }
-            if (b < 0) atomicOr(a.status, ERR_POOL_OVERFLOW);
-            sh.pool_base = b;
-            a.poff[slot] = b;
+            if (base < 0) atomicOr(a.status, ERR_POOL_OVERFLOW);
+        }
+        base = __shfl_sync(0xffffffffu, base, 0);
+        long long carry = 0;
+        for (int i0 = 0; i0 < len; i0 += 32) {
+            const int i = i0 + lane;
+            const long long c = i < len ? (long long)a.cnt[row0 + i] : 0;
+            long long incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const long long y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (i < len) a.poff[row0 + i] = base >= 0 ? base + carry + incl - c : -1;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
         }
     }
-    long long c2 = 0;
-    if (a.want_pattern) {
-        // hi(s) = set bits above s, read in chunks of 32 bitmap words (one
-        // summary word each).  The nonzero chunks -- the set bits of the
-        // second summary level -- are split into NWARP runs of equal count,
-        // one per warp in increasing order, so a list whose bits crowd into a
-        // few chunks still spreads over several warps, and each warp walks
-        // only its own chunks.  Bits above the chain's highest vertex are
-        // clear at every level, so the runs end there by themselves.
-        constexpr int NWARP = GT / 32;
-        const int wid = tid >> 5;
+    gsync<GT>(bar);
+
+    const uint32_t *summ2 = summ + bm_summary_words(bm, summ);
+    const int cend = sh.chain_hi >= 0 ? (sh.chain_hi >> 10) + 1 : 0;   // chunks holding set bits
+    const uint16_t *stamp = sh.stamp;
+    for (int i = wid; i < len; i += NWARP) {
+        const int s = s0 + i;
+        const int64_t off = a.poff[row0 + i];
+        const int cnt = a.cnt[row0 + i];
+        if (off < 0 || cnt == 0) continue;
+        int32_t *out = a.pool + off;
         const int w0 = (s + 1) >> 5;
-        const int cfirst = w0 >> 5;
-        const int cend = a.bitmap_words >> 5;   // chunks [cfirst, cend)
         const uint32_t first_mask = ~0u << ((s + 1) & 31);
-        const uint32_t *summ2 = summ + bm_summary_words(bm, summ);
-        // this lane's word of chunk cc, without the bits up to s
-        auto chunk_word = [&](int cc) -> uint32_t {
+        const bool last = (i == len - 1);   // every set bit was set by then
+        int pos = 0;
+        for_nonzero_chunks(summ2, w0 >> 5, cend, [&](int cc) {
             const int w = (cc << 5) + lane;
             uint32_t x = ((summ[cc] >> lane) & 1u) ? bm[w] : 0u;
             if (w < w0) x = 0u;
             if (w == w0) x &= first_mask;
-            return x;
-        };
-        int c_run = cend, n_run = 0;   // this warp's run: n_run nonzero chunks from c_run
-        if (cend > cfirst) {
-            const int sw0 = cfirst >> 5, sw1 = (cend - 1) >> 5;
-            auto sword = [&](int w) -> uint32_t {
-                uint32_t m = summ2[w];
-                if (w == sw0) m &= ~0u << (cfirst & 31);
-                return m;
-            };
-            int z = 0;
-            for (int w = sw0 + lane; w <= sw1; w += 32) z += __popc(sword(w));
-            z = (int)__reduce_add_sync(0xffffffffu, (unsigned)z);
-            const int k0 = (int)((int64_t)wid * z / NWARP);
-            n_run = (int)((int64_t)(wid + 1) * z / NWARP) - k0;
-            if (n_run > 0) {
-                int carry = 0;
-                for (int wb = sw0; wb <= sw1; wb += 32) {
-                    const int w = wb + lane;
-                    const uint32_t m = w <= sw1 ? sword(w) : 0u;
-                    const int pc = __popc(m);
-                    int incl = pc;
+            if (x != 0u && !last) {
+                // stamps of this word's 32 vertices: four 16-byte loads
+                const uint4 *sp = reinterpret_cast<const uint4 *>(stamp + ((int64_t)w << 5));
+                uint32_t keep = 0u;
 #pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                        if (lane >= o) incl += y;
+                for (int q = 0; q < 4; q++) {
+                    if ((x >> (8 * q)) & 0xffu) {
+                        const uint4 v = sp[q];
+                        const uint32_t h[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                        for (int e = 0; e < 4; e++) {
+                            keep |= (uint32_t)((int)(h[e] & 0xffffu) <= i) << (8 * q + 2 * e);
+                            keep |= (uint32_t)((int)(h[e] >> 16) <= i) << (8 * q + 2 * e + 1);
+                        }
                     }
-                    const int excl = carry + incl - pc;
-                    const unsigned hit = __ballot_sync(0xffffffffu, excl <= k0 && k0 < excl + pc);
-                    if (hit) {
-                        const int src = __ffs(hit) - 1;
-                        const int c = (w << 5) + select_bit(m, k0 - excl);
-                        c_run = __shfl_sync(0xffffffffu, c, src);
-                        break;
-                    }
-                    carry += __shfl_sync(0xffffffffu, incl, 31);
                 }
+                x &= keep;
             }
-        }
-        int wcount = 0;
-        for_nonzero_chunks_n(summ2, c_run, cend, n_run, [&](int cc) { wcount += __popc(chunk_word(cc)); });
-        wcount = (int)__reduce_add_sync(0xffffffffu, (unsigned)wcount);
-        if (lane == 0) sh.warp[wid] = wcount;
-        gsync<GT>(bar);
-        if (tid == 0) { c2 = clock64(); prof[4] += (unsigned long long)(c2 - c1); }
-        int wpre = 0, all = 0;   // entries of the warps before this one; of all
-        {
-            const int v = lane < NWARP ? (int)sh.warp[lane] : 0;
-            int x = v;
+            const int pc = __popc(x);
+            int incl = pc;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x += y;
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
             }
-            wpre = __shfl_sync(0xffffffffu, x - v, wid);
-            all = __shfl_sync(0xffffffffu, x, 31);
-        }
-        // the pool range holds `total` entries: write nothing if the bitmap
-        // says otherwise
-        if (tid == 0 && all != total) atomicOr(a.status, ERR_COUNT_MISMATCH);
-        const int64_t base = sh.pool_base;
-        if (base >= 0 && wcount > 0 && all == total) {
-            // A chunk whose words hold at most two entries each is written a
-            // word per lane; denser chunks a word at a time across the warp,
-            // lane = bit, so every store is one coalesced run.
-            int32_t *out = a.pool + base + wpre;
-            int pos = 0;
-            for_nonzero_chunks_n(summ2, c_run, cend, n_run, [&](int cc) {
-                uint32_t x = chunk_word(cc);
-                const int pc = __popc(x);
-                int incl = pc;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += y;
+            const int excl = incl - pc;
+            const int wbase = cc << 5;
+            // at most two entries a word: a word per lane; denser chunks a
+            // word at a time across the warp (lane = bit), one coalesced run
+            // per store.  Nothing lands past the list's own `cnt` entries.
+            if (__reduce_max_sync(0xffffffffu, (unsigned)pc) <= 2u) {
+                int at = pos + excl;
+                while (x) {
+                    const int bit = __ffs(x) - 1;
+                    x &= x - 1u;
+                    if (at < cnt) out[at] = ((wbase + lane) << 5) + bit;
+                    at++;
                 }
-                const int excl = incl - pc;
-                const int wbase = (cc << 5);
-                if (__reduce_max_sync(0xffffffffu, (unsigned)pc) <= 2u) {
-                    int32_t *dst = out + pos + excl;
-                    while (x) {
-                        const int bit = __ffs(x) - 1;
-                        x &= x - 1u;
-                        *dst++ = ((wbase + lane) << 5) + bit;
-                    }
-                } else {
-                    unsigned nzw = __ballot_sync(0xffffffffu, x != 0u);
-                    const uint32_t below = (1u << lane) - 1u;
-                    while (nzw) {
-                        const int j = __ffs(nzw) - 1;
-                        nzw &= nzw - 1u;
-                        const uint32_t xj = __shfl_sync(0xffffffffu, x, j);
-                        const int pj = __shfl_sync(0xffffffffu, excl, j);
-                        if ((xj >> lane) & 1u) out[pos + pj + __popc(xj & below)] = ((wbase + j) << 5) + lane;
-                    }
+            } else {
+                unsigned nzw = __ballot_sync(0xffffffffu, x != 0u);
+                const uint32_t below = (1u << lane) - 1u;
+                while (nzw) {
+                    const int j = __ffs(nzw) - 1;
+                    nzw &= nzw - 1u;
+                    const uint32_t xj = __shfl_sync(0xffffffffu, x, j);
+                    const int pj = __shfl_sync(0xffffffffu, excl, j);
+                    const int at = pos + pj + __popc(xj & below);
+                    if (((xj >> lane) & 1u) && at < cnt) out[at] = ((wbase + j) << 5) + lane;
                 }
-                pos += __shfl_sync(0xffffffffu, incl, 31);
-            });
-        }
-    } else if (tid == 0) {
-        c2 = c1;
+            }
+            pos += __shfl_sync(0xffffffffu, incl, 31);
+        });
+        if (lane == 0 && pos != cnt) atomicOr(a.status, ERR_COUNT_MISMATCH);
     }
     gsync<GT>(bar);
-    if (tid == 0) prof[5] += (unsigned long long)(clock64() - c2);
 }
-#undef GSOFA_VISIT
 
 // Per-thread tallies of one CTA's traversals (summed over the CTA at the
 // end); the per-source ones live in SharedState, kept by one thread.
@@ -767,7 +743,8 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
     int idx = 0;
     for (int32_t s = s_lo; s < s_hi; s += stride, idx++) {
         int reuse = 0;
-        if (a.reuse && prev == s - 1) {
+        // chain indices are 16-bit stamps: a chain ends after 65535 sources
+        if (a.reuse && prev == s - 1 && !(a.want_pattern && sh.chain_len >= 65535)) {
             if (PAIRED) {
                 reuse = pair_flag[(idx - 1) & 1][1 - half];
             } else {
@@ -780,12 +757,18 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
             }
         }
         if (!reuse) {
+            if (a.want_pattern && sh.chain_len > 0) {
+                const long long co = clock64();
+                output_chain<GT>(a, md.line_base + sh.chain_s0, pass, bm, summ, sh, gtid, bar);
+                if (gtid == 0) sh.prof[5] += (unsigned long long)(clock64() - co);
+            }
             const long long cc = clock64();
             const int clo = sh.chain_lo, chi = sh.chain_hi;
             clear_range<GT>(bm, summ, clo, chi, gtid);
             gsync<GT>(bar);
             if (gtid == 0) {
                 sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0;
+                sh.chain_s0 = s; sh.chain_len = 0; sh.chain_total = 0;
                 sh.prof[3] += (unsigned long long)(clock64() - cc);
             }
         } else if (gtid == 0) {
@@ -801,6 +784,15 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
         }
         prev = s;
         if (gtid == 0) sh.nsrc++;
+    }
+    // the piece's last chain
+    if (a.want_pattern && sh.chain_len > 0) {
+        const long long co = clock64();
+        output_chain<GT>(a, md.line_base + sh.chain_s0, pass, bm, summ, sh, gtid, bar);
+        if (gtid == 0) {
+            sh.prof[5] += (unsigned long long)(clock64() - co);
+            sh.chain_len = 0;
+        }
     }
 }
 
@@ -837,6 +829,8 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
     for (int w = tid; w < NS * a.state_words; w += BLOCK) smem_dyn[w] = 0u;
     if (gtid == 0) {
         sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0; sh.pool_cur = sh.pool_end = 0;
+        sh.stamp = a.want_pattern ? a.stamp + ((int64_t)blockIdx.x * NS + half) * a.stamp_stride : nullptr;
+        sh.chain_s0 = 0; sh.chain_len = 0; sh.chain_idx = 0; sh.chain_total = 0;
         for (int q = 0; q < 8; q++) sh.prof[q] = 0;
         sh.nsrc = sh.nreuse = 0;
     }

@@ -81,6 +81,8 @@ __global__ void __launch_bounds__(BLOCK) serve_kernel(ServeArgs sa)
     for (int w = tid; w < 2 * a.state_words; w += BLOCK) smem_dyn[w] = 0u;
     if (gtid == 0) {
         sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0;
+        sh.stamp = nullptr;   // counts only: no lists, no stamps
+        sh.chain_s0 = 0; sh.chain_len = 0; sh.chain_idx = 0; sh.chain_total = 0;
         for (int q = 0; q < 8; q++) sh.prof[q] = 0;
         sh.nsrc = sh.nreuse = 0;
     }
