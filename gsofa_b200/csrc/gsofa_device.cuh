@@ -98,7 +98,8 @@ struct JobArgs {
                                   // [3] pass-G expansions, [4] pass-G input degrees,
                                   // [5] levels, [6] sources that reused state,
                                   // [7..13] cycles: seeding, levels, fold, output
-                                  // count, output write, clearing, pair wait
+                                  // count, output write, clearing, pair wait;
+                                  // [14] ns until the traversals ended
     uint32_t *status;
     uint16_t *stamp;           // pattern mode: per traversal, stamp_stride entries:
     int64_t stamp_stride;      // the chain index at which each vertex was first set
@@ -594,11 +595,15 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
 // so the bits above source i of the chain that were set by the time it
 // finished are its list: hi(s_i) = { v > s_i : v set, stamp(v) <= i }.  One
 // pool range holds all of the chain's lists; each warp then writes whole
-// lists on its own, in increasing order, with no barrier per source.
+// lists on its own, in increasing order, with no barrier per source.  Lists
+// of pass G^T (columns of L) also count their entries into the L row
+// histogram (fire-and-forget reductions that overlap other traversals).
 template <int GT>
-__device__ void output_chain(const JobArgs &a, int64_t line0, int pass, const uint32_t *bm,
+__device__ void output_chain(const JobArgs &a, int64_t line_base, int pass, const uint32_t *bm,
                              const uint32_t *summ, SharedState &sh, int gtid, int bar)
 {
+    const int64_t line0 = line_base + sh.chain_s0;
+    int32_t *const lrow = pass ? a.lrow + line_base : nullptr;
     constexpr int NWARP = GT / 32;
     const int lane = gtid & 31, wid = gtid >> 5;
     const int s0 = sh.chain_s0, len = sh.chain_len;
@@ -701,7 +706,11 @@ __device__ void output_chain(const JobArgs &a, int64_t line0, int pass, const ui
                 while (x) {
                     const int bit = __ffs(x) - 1;
                     x &= x - 1u;
-                    if (at < cnt) out[at] = ((wbase + lane) << 5) + bit;
+                    const int32_t v = ((wbase + lane) << 5) + bit;
+                    if (at < cnt) {
+                        out[at] = v;
+                        if (lrow) atomicAdd(lrow + v, 1);
+                    }
                     at++;
                 }
             } else {
@@ -713,7 +722,11 @@ __device__ void output_chain(const JobArgs &a, int64_t line0, int pass, const ui
                     const uint32_t xj = __shfl_sync(0xffffffffu, x, j);
                     const int pj = __shfl_sync(0xffffffffu, excl, j);
                     const int at = pos + pj + __popc(xj & below);
-                    if (((xj >> lane) & 1u) && at < cnt) out[at] = ((wbase + j) << 5) + lane;
+                    if (((xj >> lane) & 1u) && at < cnt) {
+                        const int32_t v = ((wbase + j) << 5) + lane;
+                        out[at] = v;
+                        if (lrow) atomicAdd(lrow + v, 1);
+                    }
                 }
             }
             pos += __shfl_sync(0xffffffffu, incl, 31);
@@ -759,7 +772,7 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
         if (!reuse) {
             if (a.want_pattern && sh.chain_len > 0) {
                 const long long co = clock64();
-                output_chain<GT>(a, md.line_base + sh.chain_s0, pass, bm, summ, sh, gtid, bar);
+                output_chain<GT>(a, md.line_base, pass, bm, summ, sh, gtid, bar);
                 if (gtid == 0) sh.prof[5] += (unsigned long long)(clock64() - co);
             }
             const long long cc = clock64();
@@ -788,7 +801,7 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
     // the piece's last chain
     if (a.want_pattern && sh.chain_len > 0) {
         const long long co = clock64();
-        output_chain<GT>(a, md.line_base + sh.chain_s0, pass, bm, summ, sh, gtid, bar);
+        output_chain<GT>(a, md.line_base, pass, bm, summ, sh, gtid, bar);
         if (gtid == 0) {
             sh.prof[5] += (unsigned long long)(clock64() - co);
             sh.chain_len = 0;
@@ -826,6 +839,8 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
     int32_t *ring = (int32_t *)(smem_dyn + (size_t)NS * a.state_words) + (size_t)half * a.ring_size;
 
     // ---- phase 1: traversals ------------------------------------------------
+    unsigned long long t_start = 0;
+    if (blockIdx.x == 0 && tid == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_start));
     for (int w = tid; w < NS * a.state_words; w += BLOCK) smem_dyn[w] = 0u;
     if (gtid == 0) {
         sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0; sh.pool_cur = sh.pool_end = 0;
@@ -907,6 +922,11 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
         }
     }
     grid.sync();
+    if (blockIdx.x == 0 && tid == 0) {   // nanoseconds from launch to the end of the traversals
+        unsigned long long t_now;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_now));
+        a.counters[14] = t_now - t_start;
+    }
 
     const int64_t L = a.L;
     const int64_t ntiles = a.ntiles;
@@ -1022,7 +1042,7 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
     }
     grid.sync();
 
-    // ---- phase 6: supernode list, pattern compaction, L row histogram ---------
+    // ---- phase 6: supernode list, pattern compaction ---------------------------
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         int64_t c = a.tile_sn[t];
         for (int64_t base = t * TILE; base < min(L, (t + 1) * TILE); base += BLOCK) {
@@ -1055,12 +1075,21 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
             if (c == 0) continue;
             const int64_t src = a.poff[pl];
             const int64_t dst = (pass ? tot0 : 0) + a.gptr[pass * (L + 1) + l];
-            int64_t lb = 0;
-            if (pass) lb = a.mats[mat_of(l)].line_base;
-            for (int32_t k = lane; k < c; k += 32) {
-                const int32_t m = a.pool[src + k];
-                a.out[dst + k] = m;
-                if (pass) atomicAdd(&a.lrow[lb + m], 1);
+            // four loads in flight per lane before their stores
+            const int32_t *from = a.pool + src;
+            int32_t *to = a.out + dst;
+            for (int32_t k0 = 0; k0 < c; k0 += 128) {
+                int32_t v[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int32_t k = k0 + 32 * u + lane;
+                    v[u] = k < c ? __ldcs(from + k) : 0;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int32_t k = k0 + 32 * u + lane;
+                    if (k < c) __stcs(to + k, v[u]);
+                }
             }
         }
     }
