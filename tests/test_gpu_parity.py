@@ -85,6 +85,19 @@ def test_parameters_do_not_change_results(ctx, block, lanes, reuse, chunk, per_s
     assert_same(r, ref, where=f"params {block},{lanes},{reuse},{chunk},{per_sm}")
 
 
+def test_chain_longer_than_stamp_range(ctx):
+    """A path in natural order lets every source reuse its predecessor's
+    traversal, so one piece of 65,600 sources is one chain of reuse.  List
+    output keys each vertex by a 16-bit chain index, so the chain has to end
+    after 65,535 sources; the lists must stay exact across that break."""
+    n = 65_600
+    g = matgen.grid2d(n, 1)
+    ref = _oracle(g)
+    r = ctx.symbfact(ctx.upload(g), src_chunk=n)
+    assert r.reused_sources >= 2 * (n - 2)   # one chain per pass, but for the break
+    assert_same(r, ref, where="path, one 65,600-source piece")
+
+
 def test_counts_only_and_pool_retry(ctx):
     g = matgen.powerlaw(2000, seed=9)
     ref = _oracle(g)
