@@ -115,6 +115,43 @@ struct gsofa_ctx {
         b.p = nullptr;
         b.bytes = 0;
     }
+
+    // Device slabs of freed matrices, kept for later uploads so that a caller
+    // who uploads, factorizes and frees matrix after matrix pays no
+    // cudaMalloc / cudaFree (each of which synchronises the device) once the
+    // cache is warm.  At most kSlabs slabs and budget / 8 bytes are kept.
+    static constexpr size_t kSlabs = 8;
+    std::vector<DevBuf> slabs;
+    size_t slab_bytes = 0;
+    void *slab_take(size_t bytes, size_t *got)
+    {
+        int best = -1;
+        for (size_t i = 0; i < slabs.size(); i++)
+            if (slabs[i].bytes >= bytes && slabs[i].bytes <= 2 * bytes &&
+                (best < 0 || slabs[i].bytes < slabs[(size_t)best].bytes))
+                best = (int)i;
+        if (best >= 0) {
+            DevBuf b = slabs[(size_t)best];
+            slabs.erase(slabs.begin() + best);
+            slab_bytes -= b.bytes;
+            *got = b.bytes;
+            return b.p;
+        }
+        void *p = nullptr;
+        GS_CUDA(cudaMalloc(&p, bytes));
+        *got = bytes;
+        return p;
+    }
+    void slab_give(void *p, size_t bytes)
+    {
+        if (!p) return;
+        if (slabs.size() < kSlabs && slab_bytes + bytes <= budget / 8) {
+            slabs.push_back(DevBuf{p, bytes});
+            slab_bytes += bytes;
+        } else {
+            cudaFree(p);
+        }
+    }
 };
 
 struct gsofa_matrix {
@@ -125,6 +162,8 @@ struct gsofa_matrix {
     int32_t *d_gptr = nullptr, *d_gadj = nullptr;
     int32_t *d_tptr = nullptr, *d_tadj = nullptr;
     int32_t *d_orig_up = nullptr, *d_orig_lo = nullptr, *d_rawdeg = nullptr;
+    void *slab = nullptr;          // one device allocation holding all of the above
+    size_t slab_bytes = 0;
     uint64_t orig_up = 0, orig_lo = 0;
     int64_t last_pattern_total = -1;  // pool size the last run needed
 };
@@ -708,13 +747,8 @@ void gsofa_matrix_free(gsofa_matrix *m)
         auto &v = c->matrices;
         v.erase(std::remove(v.begin(), v.end(), m), v.end());
     }
-    cudaFree(m->d_gptr);
-    cudaFree(m->d_gadj);
-    cudaFree(m->d_tptr);
-    cudaFree(m->d_tadj);
-    cudaFree(m->d_orig_up);
-    cudaFree(m->d_orig_lo);
-    cudaFree(m->d_rawdeg);
+    if (c) c->slab_give(m->slab, m->slab_bytes);
+    else cudaFree(m->slab);
     delete m;
 }
 
@@ -727,6 +761,8 @@ void gsofa_destroy(gsofa_ctx *c)
                       &c->snlist, &c->tiles, &c->misc, &c->pool, &c->out, &c->mats, &c->ranges,
                       &c->st_beg, &c->st_end, &c->st_adj, &c->st_tmp, &c->matinfo, &c->stamp};
     for (DevBuf *b : bufs) c->release(*b);
+    for (DevBuf &b : c->slabs) cudaFree(b.p);
+    c->slabs.clear();
     if (c->graph.exec) cudaGraphExecDestroy(c->graph.exec);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -830,11 +866,24 @@ gsofa_status gsofa_upload(gsofa_ctx *c, int32_t n, int64_t nnz, const int32_t *b
         unsigned long long *d_counts = (unsigned long long *)(d_tsum + 2 * scan_tiles);
         uint32_t *d_status = (uint32_t *)(d_counts + 4);
 
-        GS_CUDA(cudaMalloc(&m->d_gptr, (size_t)(n + 1) * 4));
-        GS_CUDA(cudaMalloc(&m->d_tptr, (size_t)(n + 1) * 4));
-        GS_CUDA(cudaMalloc(&m->d_orig_up, nb));
-        GS_CUDA(cudaMalloc(&m->d_orig_lo, nb));
-        GS_CUDA(cudaMalloc(&m->d_rawdeg, nb));
+        // one slab: G and G^T offsets, per-line counts, and both adjacency
+        // arrays (at most nnz entries each: the input minus diagonal and
+        // duplicates)
+        {
+            auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+            const size_t pb = al((size_t)(n + 1) * 4), lb = al(nb);
+            const size_t ab = al((size_t)std::max<int64_t>(nnz, 1) * 4);
+            const size_t total = 2 * pb + 3 * lb + 2 * ab;
+            char *q = (char *)c->slab_take(total, &m->slab_bytes);
+            m->slab = q;
+            m->d_gptr = (int32_t *)q; q += pb;
+            m->d_tptr = (int32_t *)q; q += pb;
+            m->d_orig_up = (int32_t *)q; q += lb;
+            m->d_orig_lo = (int32_t *)q; q += lb;
+            m->d_rawdeg = (int32_t *)q; q += lb;
+            m->d_gadj = (int32_t *)q; q += ab;
+            m->d_tadj = (int32_t *)q;
+        }
         c->matrices.push_back(m);
 
         if (n > 0) {
@@ -894,8 +943,8 @@ gsofa_status gsofa_upload(gsofa_ctx *c, int32_t n, int64_t nnz, const int32_t *b
         m->orig_up = hc[0];
         m->orig_lo = hc[1];
         m->nnz_g = tot[0];
-        GS_CUDA(cudaMalloc(&m->d_gadj, (size_t)std::max<int64_t>(tot[0], 1) * 4));
-        GS_CUDA(cudaMalloc(&m->d_tadj, (size_t)std::max<int64_t>(tot[1], 1) * 4));
+        if (tot[0] > std::max<int64_t>(nnz, 1) || tot[1] > std::max<int64_t>(nnz, 1))
+            throw CudaFail{cudaErrorInvalidValue};   // cannot happen: kept entries <= input entries
         GS_CUDA(cudaMemcpyAsync(d_tcur, m->d_tptr, (size_t)(n + 1) * 4, cudaMemcpyDeviceToDevice, st));
         if (n > 0) {
             upload_fill_kernel<<<ugrid, ub, 0, st>>>(u, m->d_gptr, m->d_gadj, d_tcur, m->d_tadj);
