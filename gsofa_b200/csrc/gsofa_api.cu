@@ -1425,6 +1425,10 @@ struct ServerReq {
 };
 
 constexpr int32_t kSmallRequest = 65536;   // lines below which a request is class 0
+// Threads of a serving CTA (12 warps per pass).  With the kernel's 64
+// registers a thread, 768 threads leave 16K registers and 1280 thread slots
+// per SM: two 256-thread upload blocks still run beside the persistent kernel.
+constexpr int kServeBlock = 768;
 
 }  // namespace
 
@@ -1436,7 +1440,7 @@ struct gsofa_server {
     int32_t chunk = 0;              // sources per piece; 0: from the request's n
     int32_t max_slots = 4096;
     int idle_spins = 10000;
-    int block = 512, ring = 1024, grid = 0;
+    int block = kServeBlock, ring = 1024, grid = 0;
     int32_t bitmap_words = 0, state_words = 0;
     size_t smem = 0;
     cudaStream_t run = nullptr, io = nullptr;
@@ -1541,7 +1545,7 @@ gsofa_status server_launch_if_idle_impl(gsofa_server *s)
     sa.slots = s->d_slots;
     sa.slot_done = s->d_done;
     sa.idle_spins = s->idle_spins;
-    serve_kernel<512><<<s->grid, 512, s->smem, s->run>>>(sa);
+    serve_kernel<kServeBlock><<<s->grid, kServeBlock, s->smem, s->run>>>(sa);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? GSOFA_OK : fail_cuda(e);
 }
@@ -1595,7 +1599,7 @@ gsofa_status gsofa_server_create(gsofa_server **out, gsofa_server_config *cfg)
         s->bitmap_words = ((s->max_n + 31) / 32 + 127) / 128 * 128;
         s->state_words = s->bitmap_words + s->bitmap_words / 32 + ((s->bitmap_words / 32 + 31) / 32 + 3) / 4 * 4;
         // frontier ring: the largest that fits beside the two bitmaps
-        void *kfn = (void *)serve_kernel<512>;
+        void *kfn = (void *)serve_kernel<kServeBlock>;
         s->ring = 0;
         for (int cand = 8192; cand >= 1024; cand >>= 1) {
             const size_t sm = 2 * ((size_t)s->state_words * 4 + (size_t)cand * 4);
@@ -1604,7 +1608,7 @@ gsofa_status gsofa_server_create(gsofa_server **out, gsofa_server_config *cfg)
         if (!s->ring) { delete s; return GSOFA_ERR_UNSUPPORTED; }
         GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem));
         int occ = 0;
-        GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, 512, s->smem));
+        GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, kServeBlock, s->smem));
         if (occ <= 0) { delete s; return GSOFA_ERR_UNSUPPORTED; }
         s->grid = s->sms;   // one CTA per SM leaves room for the upload kernels
         GS_CUDA(cudaStreamCreateWithFlags(&s->run, cudaStreamNonBlocking));

@@ -61,8 +61,11 @@ __device__ __forceinline__ T load_cg(const T *p)
     return out;
 }
 
+// At most 64 registers a thread: with 768 threads that leaves a quarter of
+// the SM's registers (and 1280 thread slots) to the upload kernels, which
+// must run beside this kernel while it holds every SM.
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) serve_kernel(ServeArgs sa)
+__global__ void __maxnreg__(64) serve_kernel(ServeArgs sa)
 {
     constexpr int GT = BLOCK / 2;
     const JobArgs &a = sa.job;
