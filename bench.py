@@ -536,7 +536,7 @@ def main():
             "edges_inspected_without_reuse": ideal.edges_inspected,
             "work_ratio": res.edges_inspected / max(ideal.edges_inspected, 1),
             "levels": res.levels, "reused_sources": res.reused_sources, "sources": res.sources,
-            "cycles": dict(zip(("seed", "levels", "fold", "out_count", "out_write", "clear", "pair_wait"),
+            "cycles": dict(zip(("seed", "levels", "fold", "count", "lists", "clear", "pair_wait"),
                                res.cycles)), "ctas": res.ctas}
 
     cpu = None

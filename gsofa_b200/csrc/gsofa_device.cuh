@@ -97,8 +97,8 @@ struct JobArgs {
     unsigned long long *counters; // [0] edges inspected, [1] sources, [2] sn total,
                                   // [3] pass-G expansions, [4] pass-G input degrees,
                                   // [5] levels, [6] sources that reused state,
-                                  // [7..13] cycles: seeding, levels, fold, output
-                                  // count, output write, clearing, pair wait;
+                                  // [7..13] cycles: seeding, levels, fold, count,
+                                  // list output, clearing, pair wait;
                                   // [14] ns until the traversals ended
     uint32_t *status;
     uint16_t *stamp;           // pattern mode: per traversal, stamp_stride entries:
@@ -272,8 +272,9 @@ struct SharedState {
     int64_t pool_end;  // [pool_cur, pool_end), refilled POOL_CHUNK entries at a time
     int64_t warp[32];
     // tallies kept by the half's first thread only: levels, then cycles of
-    // seeding, level loop, range fold and clearing, output count, output
-    // write, (unused), wait for the other pass; sources; reused sources
+    // seeding, level loop, range fold, count and link flag, list output (per
+    // chain), bitmap clearing, wait for the other pass; sources; reused
+    // sources
     unsigned long long prof[8];
     unsigned long long nsrc, nreuse;
     int hcount;        // set bits above the current source (|hi(s)| once done)
@@ -782,7 +783,7 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
             if (gtid == 0) {
                 sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0;
                 sh.chain_s0 = s; sh.chain_len = 0; sh.chain_total = 0;
-                sh.prof[3] += (unsigned long long)(clock64() - cc);
+                sh.prof[6] += (unsigned long long)(clock64() - cc);
             }
         } else if (gtid == 0) {
             sh.nreuse++;

@@ -115,9 +115,10 @@ typedef struct gsofa_result {
     uint64_t levels;         /* frontier levels summed over the traversals  */
     uint64_t reused_sources; /* traversals that started from s-1's state    */
     uint64_t cycles[7];      /* SM cycles summed over traversals: seeding,
-                                level loop, range fold, output count,
-                                output write, bitmap clearing, waiting
-                                for the other pass                          */
+                                level loop, range fold, count and link
+                                flag, list output (once per chain of
+                                sources), bitmap clearing, waiting for the
+                                other pass                                  */
     uint64_t ctas;           /* CTAs of the persistent launch               */
     double kernel_ms;        /* factorization kernel time on the device     */
     /* per-line arrays (host, library-owned; NULL with NO_DOWNLOAD) */
