@@ -384,7 +384,9 @@ __device__ __forceinline__ int32_t chain_start(const PassGraph &g, int32_t x, in
 // With `reuse`, the bitmap still holds the finished traversal of s-1, which is
 // valid because s-1 in adj(s) implies X(s-1) u {s-1} is inside X(s) and
 // hi(s-1) minus (s-1, s] is inside hi(s).
-template <int GT, bool CG>
+// END_SYNC: finish with a barrier of the traversal's threads (not needed when
+// the caller's next step is a barrier of the whole CTA).
+template <int GT, bool CG, bool END_SYNC>
 __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                                int64_t line, int pass, int32_t s, uint32_t *bm, uint32_t *summ,
                                const Frontier &f, SharedState &sh,
@@ -585,7 +587,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         sh.flag = nx;
         sh.chain_total += total;
     }
-    gsync<GT>(bar);
+    if (END_SYNC) gsync<GT>(bar);
     if (tid == 0) prof[4] += (unsigned long long)(clock64() - c1);
 }
 #undef GSOFA_VISIT
@@ -788,7 +790,8 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
         } else if (gtid == 0) {
             sh.nreuse++;
         }
-        process_source<GT, CG>(a, g, md.n, md.line_base + s, pass, s, bm, summ, fr, sh, acc.edges,
+        // paired: the pass-flag exchange below is a barrier of the whole CTA
+        process_source<GT, CG, !PAIRED>(a, g, md.n, md.line_base + s, pass, s, bm, summ, fr, sh, acc.edges,
                            md.rawdeg, acc.xcnt, acc.einsp, sh.prof, gtid, bar);
         if (PAIRED) {
             if (gtid == 0) pair_flag[idx & 1][half] = sh.flag;

@@ -98,6 +98,22 @@ def test_chain_longer_than_stamp_range(ctx):
     assert_same(r, ref, where="path, one 65,600-source piece")
 
 
+def test_reused_device_slab_gives_exact_results(ctx):
+    """A freed matrix leaves its device slab in the context; the next upload
+    of similar size takes it over with the old contents still in it."""
+    big = matgen.grid3d(16, ordering="nd", drop_frac=0.1, seed=3)
+    small = matgen.grid3d(14, ordering="nd", drop_frac=0.1, seed=4)
+    m = ctx.upload(big)
+    assert_same(ctx.symbfact(m), _oracle(big), where="first slab")
+    m.free()
+    m2 = ctx.upload(small)      # fits the cached slab (within a factor of two)
+    assert_same(ctx.symbfact(m2), _oracle(small), where="reused slab")
+    m2.free()
+    m3 = ctx.upload(big)
+    assert_same(ctx.symbfact(m3), _oracle(big), where="slab reused again")
+    m3.free()
+
+
 def test_counts_only_and_pool_retry(ctx):
     g = matgen.powerlaw(2000, seed=9)
     ref = _oracle(g)
