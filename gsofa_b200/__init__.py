@@ -188,6 +188,9 @@ def lib():
                                   _i32p, _i64p, ctypes.POINTER(_i32p), ctypes.POINTER(_i32p),
                                   ctypes.POINTER(_i32p)]
     L.gsofa_read_text.restype = ctypes.c_int
+    L.gsofa_write_binary.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32,
+                                     ctypes.c_int64, _i32p, _i32p, _i32p]
+    L.gsofa_write_binary.restype = ctypes.c_int
     L.gsofa_free.argtypes = [vp]
     L.gsofa_free.restype = None
     L.gsofa_upload.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, _i32p, _i32p, _i32p,
@@ -471,7 +474,8 @@ class StreamServer:
 
 
 def read_text(beg_file: str, end_file: str, csr_file: str) -> Graph:
-    """Reads the reference's colbeg/colend/csr text files through the library."""
+    """Reads the reference's colbeg/colend/csr text files (or their binary
+    form, see write_binary) through the library."""
     n = ctypes.c_int32()
     nnz = ctypes.c_int64()
     b, e, a = _i32p(), _i32p(), _i32p()
@@ -485,6 +489,17 @@ def read_text(beg_file: str, end_file: str, csr_file: str) -> Graph:
         for p in (b, e, a):
             lib().gsofa_free(ctypes.cast(p, ctypes.c_void_p))
     return g
+
+
+def write_binary(g: Graph, beg_file: str, end_file: str, csr_file: str) -> None:
+    """Writes g as the three input files in the library's binary form, which
+    read_text (and the argv entry) load without text parsing."""
+    b = np.ascontiguousarray(g.beg, dtype=np.int32)
+    e = np.ascontiguousarray(g.end, dtype=np.int32)
+    a = np.ascontiguousarray(g.adj, dtype=np.int32)
+    _check(lib().gsofa_write_binary(beg_file.encode(), end_file.encode(), csr_file.encode(), int(g.n),
+                                    int(a.shape[0]), b.ctypes.data_as(_i32p), e.ctypes.data_as(_i32p),
+                                    a.ctypes.data_as(_i32p)), "gsofa_write_binary")
 
 
 def symbfact_min_id(argv: Sequence[str], myrank: int = 0):
@@ -544,7 +559,8 @@ def supernodes_from_lines(u_row_count, line_flags, max_supernode_size: int = 0) 
 def exported_symbols() -> List[str]:
     """Names of the C ABI entry points declared in include/gsofa.h."""
     return ["gsofa_symbfact_min_id", "gsofa_status_str", "gsofa_abi_version", "gsofa_default_params",
-            "gsofa_create", "gsofa_destroy", "gsofa_set_stream", "gsofa_read_text", "gsofa_free", "gsofa_upload",
+            "gsofa_create", "gsofa_destroy", "gsofa_set_stream", "gsofa_read_text", "gsofa_write_binary",
+            "gsofa_free", "gsofa_upload",
             "gsofa_matrix_free", "gsofa_matrix_n", "gsofa_symbfact", "gsofa_symbfact_batch",
             "gsofa_result_free", "gsofa_result_fetch", "gsofa_predict_scratch_bytes",
             "gsofa_symbfact_counts_noalloc", "gsofa_supernodes_from_lines", "gsofa_server_create",

@@ -781,6 +781,63 @@ void gsofa_free(void *p) { std::free(p); }
 
 int32_t gsofa_matrix_n(const gsofa_matrix *m) { return m ? m->n : -1; }
 
+// Binary form of the three input files: the 8-byte magic, little-endian
+// int64 counts (csr: nnz then n; colbeg and colend: n), then the int32 ids.
+static const char kBinMagic[8] = {'G', 'S', 'O', 'F', 'A', 'B', '0', '1'};
+
+namespace {
+
+// One input file, text or binary (told apart by the magic).  The id count is
+// counts[0]: read from the file's header -- text_counts numbers before the ids
+// in the text form, bin_counts in the binary one -- or, for a form without a
+// header, `want`.  `want` >= 0 is also checked against a header's count.  The
+// ids go to a malloc'd array.
+gsofa_status read_input_file(const char *path, int text_counts, int bin_counts, long long *counts,
+                             long long want, int32_t **ids_out)
+{
+    *ids_out = nullptr;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return GSOFA_ERR_IO;
+    char head[8] = {0};
+    const bool binary = std::fread(head, 1, 8, f) == 8 && std::memcmp(head, kBinMagic, 8) == 0;
+    if (!binary) std::rewind(f);
+    const int nc = binary ? bin_counts : text_counts;
+    for (int k = 0; k < nc; k++) {
+        long long v = -1;
+        if (binary) {
+            int64_t x = -1;
+            if (std::fread(&x, 8, 1, f) != 1) { std::fclose(f); return GSOFA_ERR_IO; }
+            v = (long long)x;
+        } else if (std::fscanf(f, "%lld", &v) != 1) {
+            std::fclose(f);
+            return GSOFA_ERR_IO;
+        }
+        if (v < 0 || v > INT32_MAX) { std::fclose(f); return GSOFA_ERR_IO; }
+        counts[k] = v;
+    }
+    if (nc == 0) counts[0] = want;
+    const long long cnt = counts[0];
+    if (cnt < 0 || (want >= 0 && cnt != want)) { std::fclose(f); return GSOFA_ERR_IO; }
+    int32_t *ids = (int32_t *)std::malloc((size_t)std::max<long long>(cnt, 1) * 4);
+    if (!ids) { std::fclose(f); return GSOFA_ERR_OOM; }
+    bool ok = true;
+    if (binary) {
+        ok = std::fread(ids, 4, (size_t)cnt, f) == (size_t)cnt;
+    } else {
+        for (long long i = 0; i < cnt && ok; i++) {
+            long long x;
+            ok = std::fscanf(f, "%lld", &x) == 1 && x >= INT32_MIN && x <= INT32_MAX;
+            if (ok) ids[i] = (int32_t)x;
+        }
+    }
+    std::fclose(f);
+    if (!ok) { std::free(ids); return GSOFA_ERR_IO; }
+    *ids_out = ids;
+    return GSOFA_OK;
+}
+
+}  // namespace
+
 gsofa_status gsofa_read_text(const char *beg_file, const char *end_file, const char *csr_file,
                              int32_t *n_out, int64_t *nnz_out, int32_t **beg_out,
                              int32_t **end_out, int32_t **adj_out)
@@ -788,51 +845,44 @@ gsofa_status gsofa_read_text(const char *beg_file, const char *end_file, const c
     if (!beg_file || !end_file || !csr_file || !n_out || !nnz_out || !beg_out || !end_out || !adj_out)
         return GSOFA_ERR_INVALID_INPUT;
     *beg_out = *end_out = *adj_out = nullptr;
-    FILE *f = std::fopen(csr_file, "r");
-    if (!f) return GSOFA_ERR_IO;
-    long long nnz = -1, n = -1;
-    if (std::fscanf(f, "%lld", &nnz) != 1 || std::fscanf(f, "%lld", &n) != 1 || nnz < 0 || n < 0 ||
-        n > INT32_MAX || nnz > INT32_MAX) {
-        std::fclose(f);
-        return GSOFA_ERR_IO;
-    }
-    int32_t *adj = (int32_t *)std::malloc((size_t)std::max<long long>(nnz, 1) * 4);
-    int32_t *beg = (int32_t *)std::malloc((size_t)std::max<long long>(n, 1) * 4);
-    int32_t *end = (int32_t *)std::malloc((size_t)std::max<long long>(n, 1) * 4);
-    if (!adj || !beg || !end) {
-        std::fclose(f);
+    // csr: "nnz n" then nnz ids; colbeg / colend: n ids each (their binary
+    // form repeats n in its header)
+    long long hc[2] = {-1, -1}, cb = -1, ce = -1;
+    int32_t *adj = nullptr, *beg = nullptr, *end = nullptr;
+    gsofa_status s = read_input_file(csr_file, 2, 2, hc, -1, &adj);
+    if (s != GSOFA_OK) return s;
+    const long long nnz = hc[0], n = hc[1];
+    s = read_input_file(beg_file, 0, 1, &cb, n, &beg);
+    if (s == GSOFA_OK) s = read_input_file(end_file, 0, 1, &ce, n, &end);
+    if (s != GSOFA_OK) {
         std::free(adj); std::free(beg); std::free(end);
-        return GSOFA_ERR_OOM;
-    }
-    auto read_ints = [](FILE *fp, int32_t *dst, long long cnt) -> bool {
-        for (long long i = 0; i < cnt; i++) {
-            long long x;
-            if (std::fscanf(fp, "%lld", &x) != 1 || x < INT32_MIN || x > INT32_MAX) return false;
-            dst[i] = (int32_t)x;
-        }
-        return true;
-    };
-    bool ok = read_ints(f, adj, nnz);
-    std::fclose(f);
-    if (ok) {
-        FILE *fb = std::fopen(beg_file, "r");
-        ok = fb && read_ints(fb, beg, n);
-        if (fb) std::fclose(fb);
-    }
-    if (ok) {
-        FILE *fe = std::fopen(end_file, "r");
-        ok = fe && read_ints(fe, end, n);
-        if (fe) std::fclose(fe);
-    }
-    if (!ok) {
-        std::free(adj); std::free(beg); std::free(end);
-        return GSOFA_ERR_IO;
+        return s;
     }
     *n_out = (int32_t)n;
     *nnz_out = nnz;
     *beg_out = beg;
     *end_out = end;
     *adj_out = adj;
+    return GSOFA_OK;
+}
+
+gsofa_status gsofa_write_binary(const char *beg_file, const char *end_file, const char *csr_file,
+                                int32_t n, int64_t nnz, const int32_t *beg, const int32_t *end,
+                                const int32_t *adj)
+{
+    if (!beg_file || !end_file || !csr_file || n < 0 || nnz < 0 || nnz > INT32_MAX ||
+        (n > 0 && (!beg || !end)) || (nnz > 0 && !adj))
+        return GSOFA_ERR_INVALID_INPUT;
+    auto put = [](const char *path, const int64_t *hdr, int nh, const int32_t *ids, int64_t cnt) -> bool {
+        FILE *f = std::fopen(path, "wb");
+        if (!f) return false;
+        bool ok = std::fwrite(kBinMagic, 1, 8, f) == 8 && std::fwrite(hdr, 8, (size_t)nh, f) == (size_t)nh &&
+                  (cnt == 0 || std::fwrite(ids, 4, (size_t)cnt, f) == (size_t)cnt);
+        return (std::fclose(f) == 0) && ok;
+    };
+    const int64_t hcsr[2] = {nnz, (int64_t)n}, hn[1] = {(int64_t)n};
+    if (!put(csr_file, hcsr, 2, adj, nnz) || !put(beg_file, hn, 1, beg, n) || !put(end_file, hn, 1, end, n))
+        return GSOFA_ERR_IO;
     return GSOFA_OK;
 }
 

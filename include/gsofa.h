@@ -165,10 +165,20 @@ gsofa_status gsofa_set_stream(gsofa_ctx *ctx, void *cuda_stream);
 
 /* Reads the reference's text files (csr: "nnz n" then nnz ids; colbeg and
  * colend: n ids each; without_space_optimization/symbfact.cuh:1022-1071) into
- * malloc'd arrays the caller frees with gsofa_free(). */
+ * malloc'd arrays the caller frees with gsofa_free().  Each file may instead
+ * be in the binary form gsofa_write_binary() produces (detected by its magic),
+ * which loads without text parsing. */
 gsofa_status gsofa_read_text(const char *beg_file, const char *end_file,
                              const char *csr_file, int32_t *n, int64_t *nnz,
                              int32_t **beg, int32_t **end, int32_t **adj);
+
+/* Writes the three input files in binary form: the magic "GSOFAB01", then
+ * little-endian int64 counts (csr: nnz, n; colbeg and colend: n) and the
+ * int32 ids.  No counterpart in the reference, which reads text only. */
+gsofa_status gsofa_write_binary(const char *beg_file, const char *end_file,
+                                const char *csr_file, int32_t n, int64_t nnz,
+                                const int32_t *beg, const int32_t *end,
+                                const int32_t *adj);
 void gsofa_free(void *p);
 
 /* Copies the caller's host arrays to the device, validates them (every range

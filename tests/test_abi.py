@@ -58,6 +58,31 @@ def test_read_text_matches_fixture(tmp_path):
     assert np.array_equal(r.adj, g.adj)
 
 
+def test_binary_files_round_trip_and_mix_with_text(tmp_path):
+    g = bundled()
+    p = {k: str(tmp_path / f"{k}.bin") for k in "bec"}
+    gsofa_b200.write_binary(g, p["b"], p["e"], p["c"])
+    assert open(p["c"], "rb").read(8) == b"GSOFAB01"
+    r = gsofa_b200.read_text(p["b"], p["e"], p["c"])
+    assert r.n == g.n and np.array_equal(r.beg, g.beg) and np.array_equal(r.end, g.end)
+    assert np.array_equal(r.adj, g.adj)
+    # a text colend beside binary colbeg and csr
+    (tmp_path / "e.dat").write_text(" ".join(map(str, g.end.tolist())) + "\n")
+    r = gsofa_b200.read_text(p["b"], str(tmp_path / "e.dat"), p["c"])
+    assert np.array_equal(r.end, g.end) and np.array_equal(r.adj, g.adj)
+    # a binary colbeg whose count disagrees with the csr header is an I/O error
+    small = gsofa_b200.matgen.grid2d(4)
+    gsofa_b200.write_binary(small, str(tmp_path / "sb.bin"), str(tmp_path / "se.bin"), str(tmp_path / "sc.bin"))
+    with pytest.raises(gsofa_b200.GsofaError) as e:
+        gsofa_b200.read_text(str(tmp_path / "sb.bin"), p["e"], p["c"])
+    assert e.value.status == 6
+    # truncated binary ids
+    data = open(p["c"], "rb").read()
+    open(str(tmp_path / "cut.bin"), "wb").write(data[: len(data) - 8])
+    with pytest.raises(gsofa_b200.GsofaError):
+        gsofa_b200.read_text(p["b"], p["e"], str(tmp_path / "cut.bin"))
+
+
 def test_read_text_errors(tmp_path):
     with pytest.raises(gsofa_b200.GsofaError) as e:
         gsofa_b200.read_text(str(tmp_path / "nope"), str(tmp_path / "nope"), str(tmp_path / "nope"))
@@ -78,4 +103,21 @@ def test_cli_usage():
     cli = os.path.join(ROOT, "gsofa_b200", "gsofa")
     assert os.path.exists(cli)
     r = subprocess.run([cli], capture_output=True, text=True)
-    assert r.returncode == 2 and "usage" in r.stderr
+    assert r.returncode == 2 and "usage" in r.stderr and "--to-binary" in r.stderr
+
+
+def test_cli_converts_text_to_binary(tmp_path):
+    g = bundled()
+    (tmp_path / "b.dat").write_text(" ".join(map(str, g.beg.tolist())))
+    (tmp_path / "e.dat").write_text(" ".join(map(str, g.end.tolist())))
+    (tmp_path / "c.dat").write_text(f"{g.nnz} {g.n}\n" + " ".join(map(str, g.adj.tolist())))
+    cli = os.path.join(ROOT, "gsofa_b200", "gsofa")
+    pre = str(tmp_path / "m")
+    r = subprocess.run([cli, "--to-binary", str(tmp_path / "b.dat"), str(tmp_path / "e.dat"),
+                        str(tmp_path / "c.dat"), pre], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    back = gsofa_b200.read_text(pre + ".colbeg.bin", pre + ".colend.bin", pre + ".csr.bin")
+    assert back.n == g.n and np.array_equal(back.adj, g.adj) and np.array_equal(back.beg, g.beg)
+    r = subprocess.run([cli, "--to-binary", str(tmp_path / "nope"), str(tmp_path / "e.dat"),
+                        str(tmp_path / "c.dat"), pre], capture_output=True, text=True)
+    assert r.returncode == 1

@@ -161,6 +161,11 @@ def test_reference_argv_entry(tmp_path):
                  ["gsofa", *files, "264", "5", "128", "1"]):
         fills, ms = gsofa_b200.symbfact_min_id(argv)
         assert fills == want and ms > 0
+    # the same matrix in the binary form
+    bins = [str(tmp_path / f) for f in ("b.bin", "e.bin", "c.bin")]
+    gsofa_b200.write_binary(g, *bins)
+    fills, ms = gsofa_b200.symbfact_min_id(["gsofa", *bins, "1"])
+    assert fills == want
 
 
 def test_batch_matches_one_by_one(ctx):
