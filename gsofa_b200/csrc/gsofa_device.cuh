@@ -9,8 +9,10 @@
 //                 gptr[2][L+1] int64-- CSR offsets after compaction
 //                 lrow[L] int32     -- |L row s| (histogram of the L columns)
 //                 snind[L] uint8    -- line starts a supernode
-//   pool / out  : int32 pattern entries (traversal writes pool, compaction
-//                 writes out in line order);
+//   pool / out  : int32 pattern entries (the traversals write pool, one range
+//                 per chain of sources; compaction writes out in line order);
+//   stamp       : pattern mode, per traversal: n uint16, the chain index at
+//                 which each vertex was first set;
 //   per CTA     : frontier queue of qcap int32 (every vertex enters at most
 //                 once per source, so qcap >= n never overflows).
 // The per-source visited set is an n-bit bitmap in shared memory.
@@ -380,10 +382,11 @@ __device__ __forceinline__ int32_t chain_start(const PassGraph &g, int32_t x, in
     } while (0)
 
 // One source s of one pass: seeds from adj(s), expands the frontier level by
-// level through vertices < s, then counts (and optionally writes) hi(s).
-// With `reuse`, the bitmap still holds the finished traversal of s-1, which is
-// valid because s-1 in adj(s) implies X(s-1) u {s-1} is inside X(s) and
-// hi(s-1) minus (s-1, s] is inside hi(s).
+// level through vertices < s, then records |hi(s)| and the s+1 link flag (the
+// list itself is written when the chain of sources ends, output_chain).
+// When the caller reuses state, the bitmap still holds the finished traversal
+// of s-1, which is valid whenever s-1 is in X(s): then X(s-1) u {s-1} is inside
+// X(s) and hi(s-1) minus {s} is inside hi(s).
 // END_SYNC: finish with a barrier of the traversal's threads (not needed when
 // the caller's next step is a barrier of the whole CTA).
 template <int GT, bool CG, bool END_SYNC>
