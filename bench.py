@@ -507,6 +507,36 @@ def main():
         e2e = {"value": world * k2 * nnz_lu / (te / 1000.0), "unit": "nnz/s", "steps": k2,
                "ms_per_step": te / k2, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "host_phases": phases, "kernel_ms": out.kernel_ms}
+        if want_pattern:
+            # the same steps for a consumer of the supernodal structure: the
+            # pattern stays on the device and only the per-supernode index
+            # lists come back
+            mm = ctx.upload(pb.numpy(), pe.numpy(), pa.numpy())
+            _, sup = ctx.symbfact_supernodal(mm, pe2e)
+            mm.free()
+            # page-locked result buffers, sized from the warm-up call, reused
+            snb = {k: torch.empty(max(getattr(sup, k).size, 1),
+                                  dtype=torch.int64 if k in ("xlsub", "xusub") else torch.int32).pin_memory().numpy()
+                   for k in ("xsup", "supno", "xlsub", "lsub", "xusub", "usub")}
+            torch.cuda.synchronize()
+            s0 = torch.cuda.Event(enable_timing=True)
+            s1 = torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            for i in range(k2):
+                if i:
+                    flush.fill_(i & 0xff)
+                mm = ctx.upload(pb.numpy(), pe.numpy(), pa.numpy())
+                rs, sup = ctx.symbfact_supernodal(mm, pe2e, out=snb)
+                mm.free()
+            s1.record(stream)
+            torch.cuda.synchronize()
+            ts = s0.elapsed_time(s1)
+            assert rs.nnz_lu == nnz_lu and sup.nsuper == res.n_supernodes
+            d2h_sn = sum(int(getattr(sup, k).nbytes) for k in ("xsup", "supno", "xlsub", "lsub", "xusub", "usub"))
+            e2e["supernodal"] = {"value": world * k2 * nnz_lu / (ts / 1000.0), "unit": "nnz/s",
+                                 "ms_per_step": ts / k2, "h2d_bytes_per_step": int(h2d),
+                                 "d2h_bytes_per_step": d2h_sn, "lsub": int(sup.lsub.size),
+                                 "usub": int(sup.usub.size)}
 
     # ---- roofline of the factorization kernel --------------------------------
     # Algorithmic bytes follow the per-source traversal model: every source

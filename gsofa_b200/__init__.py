@@ -188,6 +188,16 @@ def lib():
                                   _i32p, _i64p, ctypes.POINTER(_i32p), ctypes.POINTER(_i32p),
                                   ctypes.POINTER(_i32p)]
     L.gsofa_read_text.restype = ctypes.c_int
+    L.gsofa_result_supernodal.argtypes = [vp, ctypes.POINTER(_CResult), ctypes.POINTER(_CSupernodal)]
+    L.gsofa_result_supernodal.restype = ctypes.c_int
+    L.gsofa_supernodal_free.argtypes = [ctypes.POINTER(_CSupernodal)]
+    L.gsofa_supernodal_free.restype = None
+    L.gsofa_result_supernodal_sizes.argtypes = [vp, ctypes.POINTER(_CResult), ctypes.POINTER(ctypes.c_int32),
+                                                _i64p, _i64p]
+    L.gsofa_result_supernodal_sizes.restype = ctypes.c_int
+    L.gsofa_result_supernodal_fetch.argtypes = [vp, ctypes.POINTER(_CResult), _i32p, _i32p, _i64p, _i32p,
+                                                _i64p, _i32p]
+    L.gsofa_result_supernodal_fetch.restype = ctypes.c_int
     L.gsofa_write_binary.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32,
                                      ctypes.c_int64, _i32p, _i32p, _i32p]
     L.gsofa_write_binary.restype = ctypes.c_int
@@ -245,6 +255,28 @@ def lib():
 def _check(status: int, what: str = "") -> None:
     if status != OK:
         raise GsofaError(status, what)
+
+
+class _CSupernodal(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int32), ("nsuper", ctypes.c_int32), ("nlsub", ctypes.c_int64),
+                ("nusub", ctypes.c_int64), ("xsup", _i32p), ("supno", _i32p), ("xlsub", _i64p),
+                ("lsub", _i32p), ("xusub", _i64p), ("usub", _i32p)]
+
+
+@dataclasses.dataclass
+class Supernodal:
+    """SuperLU-style supernodal structure (gsofa_result_supernodal): supernode
+    k holds columns xsup[k] .. xsup[k+1]-1; its rows are lsub[xlsub[k] ..
+    xlsub[k+1]) (the diagonal block, then the rows below it of its last
+    column), its columns right of the block usub[xusub[k] .. xusub[k+1])."""
+    n: int
+    nsuper: int
+    xsup: np.ndarray
+    supno: np.ndarray
+    xlsub: np.ndarray
+    lsub: np.ndarray
+    xusub: np.ndarray
+    usub: np.ndarray
 
 
 def _arr(ptr, count: int, dtype) -> Optional[np.ndarray]:
@@ -352,6 +384,46 @@ class Context:
         _check(lib().gsofa_symbfact(self._h, m.handle, ctypes.byref(p), ctypes.byref(r)), "gsofa_symbfact")
         try:
             return _convert(r)
+        finally:
+            lib().gsofa_result_free(ctypes.byref(r))
+
+    def symbfact_supernodal(self, m: Matrix, params: Optional[Params] = None, out: Optional[dict] = None,
+                            **kw):
+        """Factorizes with the pattern kept on the device and returns
+        (Result without per-line arrays, Supernodal): only the compact
+        supernodal structure crosses PCIe, not the pattern.  `out` may hold
+        caller-owned buffers (e.g. views of page-locked memory) named like the
+        Supernodal fields; the returned arrays are then views of them."""
+        p = Params()
+        ctypes.pointer(p)[0] = params if params is not None else Params.default(**kw)
+        p.want_pattern = 1
+        p.flags |= FLAG_NO_DOWNLOAD
+        r = _CResult()
+        _check(lib().gsofa_symbfact(self._h, m.handle, ctypes.byref(p), ctypes.byref(r)), "gsofa_symbfact")
+        try:
+            res = _convert(r)
+            ns, nl, nu = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int64()
+            _check(lib().gsofa_result_supernodal_sizes(self._h, ctypes.byref(r), ctypes.byref(ns),
+                                                       ctypes.byref(nl), ctypes.byref(nu)),
+                   "gsofa_result_supernodal_sizes")
+            k, n = ns.value, res.n
+            need = {"xsup": (k + 1, np.int32), "supno": (n, np.int32), "xlsub": (k + 1, np.int64),
+                    "lsub": (nl.value, np.int32), "xusub": (k + 1, np.int64), "usub": (nu.value, np.int32)}
+            bufs = {}
+            for key, (cnt, dt) in need.items():
+                b = None if out is None else out.get(key)
+                if b is None:
+                    b = np.empty(max(cnt, 1), dt)
+                elif b.shape[0] < cnt or b.dtype != dt:
+                    raise GsofaError(1, f"buffer {key} holds {b.shape[0]} {b.dtype} < {cnt} {np.dtype(dt)}")
+                bufs[key] = b
+            ptr = lambda key: bufs[key].ctypes.data_as(_i64p if key.startswith("x") and key != "xsup"  # noqa: E731
+                                                        else _i32p)
+            _check(lib().gsofa_result_supernodal_fetch(self._h, ctypes.byref(r), ptr("xsup"), ptr("supno"),
+                                                       ptr("xlsub"), ptr("lsub"), ptr("xusub"), ptr("usub")),
+                   "gsofa_result_supernodal_fetch")
+            sup = Supernodal(n, k, *(bufs[key][:cnt] for key, (cnt, _) in need.items()))
+            return res, sup
         finally:
             lib().gsofa_result_free(ctypes.byref(r))
 
@@ -562,7 +634,9 @@ def exported_symbols() -> List[str]:
             "gsofa_create", "gsofa_destroy", "gsofa_set_stream", "gsofa_read_text", "gsofa_write_binary",
             "gsofa_free", "gsofa_upload",
             "gsofa_matrix_free", "gsofa_matrix_n", "gsofa_symbfact", "gsofa_symbfact_batch",
-            "gsofa_result_free", "gsofa_result_fetch", "gsofa_predict_scratch_bytes",
+            "gsofa_result_free", "gsofa_result_fetch", "gsofa_result_supernodal", "gsofa_supernodal_free",
+            "gsofa_result_supernodal_sizes", "gsofa_result_supernodal_fetch",
+            "gsofa_predict_scratch_bytes",
             "gsofa_symbfact_counts_noalloc", "gsofa_supernodes_from_lines", "gsofa_server_create",
             "gsofa_server_destroy", "gsofa_server_request_bytes", "gsofa_server_submit",
             "gsofa_server_poll", "gsofa_server_result", "gsofa_server_drain"]

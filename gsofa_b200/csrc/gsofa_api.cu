@@ -8,6 +8,7 @@
 #include "../../include/gsofa.h"
 #include "gsofa_device.cuh"
 #include "gsofa_server.cuh"
+#include "gsofa_supernodal.cuh"
 
 #include <cuda_runtime.h>
 
@@ -80,6 +81,10 @@ struct gsofa_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // job scratch
     DevBuf queue, cnt, nxt, poff, gptr, lrow, snind, snlist, tiles, misc, pool, out, mats, ranges, stamp;
+    DevBuf sn_head, sn_data;  // gsofa_result_supernodal: sizes and offsets; index lists
+    std::vector<int64_t> sn_xl, sn_xu;   // supernodal offsets of the result sizes were taken for
+    const void *sn_for = nullptr;        // ... that result (its internal record)
+    uint64_t sn_job = 0;                 // ... and its job
     // upload staging
     DevBuf st_beg, st_end, st_adj, st_tmp;
     std::vector<gsofa_matrix *> matrices;
@@ -177,6 +182,7 @@ struct ResultInternal {
     int64_t L, line_base, n;
     int64_t u0, l0;         // first index of the U rows / L columns in `out`
     int64_t sn0;            // first supernode of this matrix in the device list
+    int pattern;            // the job kept the pattern
 };
 
 int pick_block(int32_t max_n)
@@ -610,17 +616,19 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
                     r.u_idx = download(st, d_out, s0[i], (int64_t)r.nnz_u);
                     r.l_idx = download(st, d_out, tot[0] + s1[i], (int64_t)r.nnz_l);
                 }
-            } else {
-                ResultInternal *ri = new ResultInternal();
-                ri->job_id = ctx->job_id;
-                ri->L = L;
-                ri->line_base = lb;
-                ri->n = n;
-                ri->u0 = s0[i];
-                ri->l0 = tot[0] + s1[i];
-                ri->sn0 = ss[i];
-                r.internal = ri;
             }
+            // where the result sits on the device, for gsofa_result_fetch and
+            // gsofa_result_supernodal (valid until the next job on ctx)
+            ResultInternal *ri = new ResultInternal();
+            ri->job_id = ctx->job_id;
+            ri->L = L;
+            ri->line_base = lb;
+            ri->n = n;
+            ri->u0 = s0[i];
+            ri->l0 = tot[0] + s1[i];
+            ri->sn0 = ss[i];
+            ri->pattern = want_pattern ? 1 : 0;
+            r.internal = ri;
         }
         GS_CUDA(cudaStreamSynchronize(st));
         for (int i = 0; i < count && download_lines; i++) {
@@ -759,7 +767,8 @@ void gsofa_destroy(gsofa_ctx *c)
     while (!c->matrices.empty()) gsofa_matrix_free(c->matrices.back());
     DevBuf *bufs[] = {&c->queue, &c->cnt, &c->nxt, &c->poff, &c->gptr, &c->lrow, &c->snind,
                       &c->snlist, &c->tiles, &c->misc, &c->pool, &c->out, &c->mats, &c->ranges,
-                      &c->st_beg, &c->st_end, &c->st_adj, &c->st_tmp, &c->matinfo, &c->stamp};
+                      &c->st_beg, &c->st_end, &c->st_adj, &c->st_tmp, &c->matinfo, &c->stamp,
+                      &c->sn_head, &c->sn_data};
     for (DevBuf *b : bufs) c->release(*b);
     for (DevBuf &b : c->slabs) cudaFree(b.p);
     c->slabs.clear();
@@ -1128,6 +1137,175 @@ size_t gsofa_predict_scratch_bytes(const gsofa_ctx *c, int32_t n, int64_t nnz,
     if (p.want_pattern)                         // chain stamps, two traversals a CTA
         b += grid * 2 * ((size_t)(n + 4095) / 4096 * 4096) * 2;
     return b;
+}
+
+void gsofa_supernodal_free(gsofa_supernodal *s)
+{
+    if (!s) return;
+    std::free(s->xsup);
+    std::free(s->supno);
+    std::free(s->xlsub);
+    std::free(s->lsub);
+    std::free(s->xusub);
+    std::free(s->usub);
+    std::memset(s, 0, sizeof(*s));
+}
+
+namespace {
+
+// Arguments of the supernodal kernels for the result r; the head scratch
+// (sizes [2][ns] | offsets [2][ns + 1] | supno [n]) is grown to fit.
+SupernodalArgs supernodal_args(gsofa_ctx *c, const gsofa_result *r, const ResultInternal *ri)
+{
+    const int32_t n = (int32_t)ri->n, ns = r->n_supernodes;
+    const int64_t L = ri->L, lb = ri->line_base;
+    char *head = (char *)c->grow(c->sn_head, (size_t)(4 * (int64_t)ns + 2) * 8 + (size_t)n * 4);
+    SupernodalArgs a{};
+    a.sn = (const int32_t *)c->snlist.p + ri->sn0;
+    a.nsuper = ns;
+    a.n = n;
+    a.lb = lb;
+    a.ucnt = (const int32_t *)c->cnt.p + lb;
+    a.lcnt = (const int32_t *)c->cnt.p + L + lb;
+    a.uptr = (const int64_t *)c->gptr.p + lb;
+    a.lptr = (const int64_t *)c->gptr.p + (L + 1) + lb;
+    a.out = (const int32_t *)c->out.p;
+    a.u0 = ri->u0;
+    a.l0 = ri->l0;
+    a.lsize = (int64_t *)head;
+    a.usize = a.lsize + ns;
+    a.xlsub = a.usize + ns;
+    a.xusub = a.xlsub + ns + 1;
+    a.supno = (int32_t *)(a.xusub + ns + 1);
+    return a;
+}
+
+const ResultInternal *supernodal_source(gsofa_ctx *c, const gsofa_result *r)
+{
+    if (!c || !r) return nullptr;
+    const ResultInternal *ri = (const ResultInternal *)r->internal;
+    if (!ri || ri->job_id != c->job_id || !ri->pattern || !c->out.p) return nullptr;
+    const int64_t n = ri->n, ns = r->n_supernodes;
+    if (ns < 0 || ns > n || (n > 0 && ns == 0)) return nullptr;
+    return ri;
+}
+
+}  // namespace
+
+gsofa_status gsofa_result_supernodal_sizes(gsofa_ctx *c, const gsofa_result *r, int32_t *nsuper,
+                                           int64_t *nlsub, int64_t *nusub)
+{
+    const ResultInternal *ri = supernodal_source(c, r);
+    if (!ri || !nsuper || !nlsub || !nusub) return GSOFA_ERR_INVALID_INPUT;
+    const int32_t ns = r->n_supernodes;
+    *nsuper = ns;
+    *nlsub = *nusub = 0;
+    c->sn_xl.assign((size_t)ns + 1, 0);
+    c->sn_xu.assign((size_t)ns + 1, 0);
+    c->sn_for = nullptr;
+    if (ns == 0) {
+        c->sn_for = ri;
+        c->sn_job = ri->job_id;
+        return GSOFA_OK;
+    }
+    try {
+        GS_CUDA(cudaSetDevice(c->device));
+        cudaStream_t st = c->stream;
+        SupernodalArgs a = supernodal_args(c, r, ri);
+        const int tb = 256;
+        const int sgrid = (int)std::min<int64_t>(((int64_t)ns + tb - 1) / tb, (int64_t)c->sm_count * 8);
+        supernodal_size_kernel<<<sgrid, tb, 0, st>>>(a);
+        GS_CUDA(cudaGetLastError());
+        std::vector<int64_t> sz(2 * (size_t)ns);
+        GS_CUDA(cudaMemcpyAsync(sz.data(), a.lsize, sz.size() * 8, cudaMemcpyDeviceToHost, st));
+        GS_CUDA(cudaStreamSynchronize(st));
+        for (int32_t k = 0; k < ns; k++) {
+            if (sz[k] < 1 || sz[ns + k] < 0) return GSOFA_ERR_CUDA;   // not a supernode: internal fault
+            c->sn_xl[k + 1] = c->sn_xl[k] + sz[k];
+            c->sn_xu[k + 1] = c->sn_xu[k] + sz[ns + k];
+        }
+        GS_CUDA(cudaMemcpyAsync((void *)a.xlsub, c->sn_xl.data(), ((size_t)ns + 1) * 8, cudaMemcpyHostToDevice, st));
+        GS_CUDA(cudaMemcpyAsync((void *)a.xusub, c->sn_xu.data(), ((size_t)ns + 1) * 8, cudaMemcpyHostToDevice, st));
+        GS_CUDA(cudaStreamSynchronize(st));
+    } catch (CudaFail &f) {
+        return fail_cuda(f.e);
+    }
+    *nlsub = c->sn_xl[ns];
+    *nusub = c->sn_xu[ns];
+    c->sn_for = ri;
+    c->sn_job = ri->job_id;
+    return GSOFA_OK;
+}
+
+gsofa_status gsofa_result_supernodal_fetch(gsofa_ctx *c, const gsofa_result *r, int32_t *xsup,
+                                           int32_t *supno, int64_t *xlsub, int32_t *lsub,
+                                           int64_t *xusub, int32_t *usub)
+{
+    const ResultInternal *ri = supernodal_source(c, r);
+    if (!ri || c->sn_for != ri || c->sn_job != ri->job_id)   // sizes first, for this result
+        return GSOFA_ERR_INVALID_INPUT;
+    const int32_t n = (int32_t)ri->n, ns = r->n_supernodes;
+    const int64_t lb = ri->line_base;
+    if (xlsub) std::memcpy(xlsub, c->sn_xl.data(), ((size_t)ns + 1) * 8);
+    if (xusub) std::memcpy(xusub, c->sn_xu.data(), ((size_t)ns + 1) * 8);
+    if (ns == 0) {
+        if (xsup) xsup[0] = 0;
+        return GSOFA_OK;
+    }
+    try {
+        GS_CUDA(cudaSetDevice(c->device));
+        cudaStream_t st = c->stream;
+        SupernodalArgs a = supernodal_args(c, r, ri);   // same head: sizes and offsets stay
+        const int64_t nl = c->sn_xl[ns], nu = c->sn_xu[ns];
+        int32_t *data = (int32_t *)c->grow(c->sn_data, (size_t)(nl + nu) * 4);
+        a.lsub = data;
+        a.usub = data + nl;
+        const int tb = 256;
+        if (lsub || usub) {
+            const int fgrid = (int)std::min<int64_t>(((int64_t)ns * 32 + tb - 1) / tb, (int64_t)c->sm_count * 8);
+            supernodal_fill_kernel<<<fgrid, tb, 0, st>>>(a);
+            GS_CUDA(cudaGetLastError());
+        }
+        if (lsub) GS_CUDA(cudaMemcpyAsync(lsub, a.lsub, (size_t)nl * 4, cudaMemcpyDeviceToHost, st));
+        if (usub) GS_CUDA(cudaMemcpyAsync(usub, a.usub, (size_t)nu * 4, cudaMemcpyDeviceToHost, st));
+        if (supno) GS_CUDA(cudaMemcpyAsync(supno, a.supno, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
+        if (xsup) GS_CUDA(cudaMemcpyAsync(xsup, a.sn, (size_t)ns * 4, cudaMemcpyDeviceToHost, st));
+        GS_CUDA(cudaStreamSynchronize(st));
+        if (xsup) {
+            for (int32_t k = 0; k < ns; k++) xsup[k] -= (int32_t)lb;
+            xsup[ns] = n;
+        }
+    } catch (CudaFail &f) {
+        return fail_cuda(f.e);
+    }
+    return GSOFA_OK;
+}
+
+gsofa_status gsofa_result_supernodal(gsofa_ctx *c, const gsofa_result *r, gsofa_supernodal *o)
+{
+    if (!o) return GSOFA_ERR_INVALID_INPUT;
+    std::memset(o, 0, sizeof(*o));
+    int32_t ns = 0;
+    int64_t nl = 0, nu = 0;
+    gsofa_status s = gsofa_result_supernodal_sizes(c, r, &ns, &nl, &nu);
+    if (s != GSOFA_OK) return s;
+    o->n = (int32_t)((const ResultInternal *)r->internal)->n;
+    o->nsuper = ns;
+    o->nlsub = nl;
+    o->nusub = nu;
+    o->xsup = (int32_t *)std::malloc(((size_t)ns + 1) * 4);
+    o->supno = (int32_t *)std::malloc((size_t)std::max(o->n, 1) * 4);
+    o->xlsub = (int64_t *)std::malloc(((size_t)ns + 1) * 8);
+    o->xusub = (int64_t *)std::malloc(((size_t)ns + 1) * 8);
+    o->lsub = (int32_t *)std::malloc((size_t)std::max<int64_t>(nl, 1) * 4);
+    o->usub = (int32_t *)std::malloc((size_t)std::max<int64_t>(nu, 1) * 4);
+    if (!o->xsup || !o->supno || !o->xlsub || !o->xusub || !o->lsub || !o->usub) {
+        gsofa_supernodal_free(o);
+        return GSOFA_ERR_OOM;
+    }
+    s = gsofa_result_supernodal_fetch(c, r, o->xsup, o->supno, o->xlsub, o->lsub, o->xusub, o->usub);
+    if (s != GSOFA_OK) gsofa_supernodal_free(o);
+    return s;
 }
 
 // ---------------------------------------------------------------------------

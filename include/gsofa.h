@@ -213,6 +213,48 @@ gsofa_status gsofa_result_fetch(gsofa_ctx *ctx, const gsofa_result *r,
                                 int64_t *u_ptr, int32_t *u_idx,
                                 int64_t *l_ptr, int32_t *l_idx);
 
+/* SuperLU-style supernodal structure of a factorization with the pattern,
+ * built on the device from the result and downloaded without the full
+ * pattern.  Supernode k holds columns / rows xsup[k] .. xsup[k+1]-1:
+ *   lsub[xlsub[k] .. xlsub[k+1]) -- its rows: the diagonal block xsup[k] ..
+ *       xsup[k+1]-1, then the rows below the block of its last column, which
+ *       hold those of every column of the supernode (L columns of a supernode
+ *       nest, so this is the union: a relaxed supernode where they differ);
+ *   usub[xusub[k] .. xusub[k+1]) -- the columns right of the block, the same
+ *       for every row of the supernode;
+ *   supno[j] -- the supernode of column j.
+ * The consumer-side format of SuperLU_DIST's symbolic stage; no counterpart in
+ * the reference, which returns no pattern.  Host arrays are library-owned until
+ * gsofa_supernodal_free().  Needs the result of the last factorization on ctx,
+ * made with the pattern (GSOFA_FLAG_NO_DOWNLOAD spares its download). */
+typedef struct gsofa_supernodal {
+    int32_t n, nsuper;
+    int64_t nlsub, nusub;
+    int32_t *xsup;    /* [nsuper + 1] */
+    int32_t *supno;   /* [n] */
+    int64_t *xlsub;   /* [nsuper + 1] */
+    int32_t *lsub;    /* [nlsub] */
+    int64_t *xusub;   /* [nsuper + 1] */
+    int32_t *usub;    /* [nusub] */
+} gsofa_supernodal;
+
+gsofa_status gsofa_result_supernodal(gsofa_ctx *ctx, const gsofa_result *r,
+                                     gsofa_supernodal *out);
+void gsofa_supernodal_free(gsofa_supernodal *s);
+
+/* The same structure into caller-owned (e.g. page-locked) buffers, in two
+ * calls: the sizes first (nsuper + 1 entries for xsup, xlsub and xusub, n for
+ * supno, nlsub for lsub, nusub for usub), then the fetch.  Any fetch pointer
+ * may be NULL.  The fetch needs the sizes call for the same result just before
+ * it on ctx. */
+gsofa_status gsofa_result_supernodal_sizes(gsofa_ctx *ctx, const gsofa_result *r,
+                                           int32_t *nsuper, int64_t *nlsub,
+                                           int64_t *nusub);
+gsofa_status gsofa_result_supernodal_fetch(gsofa_ctx *ctx, const gsofa_result *r,
+                                           int32_t *xsup, int32_t *supno,
+                                           int64_t *xlsub, int32_t *lsub,
+                                           int64_t *xusub, int32_t *usub);
+
 /* Supernode partition from per-line U row counts and link flags (as in
  * gsofa_result), computed on the host: used to finish a factorization whose
  * lines were computed in partitions (on several GPUs) and summed.  Writes the

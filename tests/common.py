@@ -86,3 +86,26 @@ def assert_same(gpu, ref: dict, pattern: bool = True, where: str = ""):
                                      f"{g[bad].tolist()} != {r[bad].tolist()}")
         else:
             assert int(g) == int(r), f"{where}: {f} {g} != {r}"
+
+
+def supernodal_reference(ref: dict) -> dict:
+    """The supernodal structure built from an oracle result with the pattern:
+    per supernode, the diagonal block's rows then the rows below it of its
+    last column, and the columns right of the block of its first row."""
+    n = ref["n"]
+    up, ui, lp, li = ref["u_ptr"], ref["u_idx"], ref["l_ptr"], ref["l_idx"]
+    xsup = np.append(np.asarray(ref["sn_start"], np.int64), n)
+    lsub, usub, xl, xu = [], [], [0], [0]
+    supno = np.zeros(n, np.int32)
+    for k in range(len(xsup) - 1):
+        f, l = int(xsup[k]), int(xsup[k + 1])
+        supno[f:l] = k
+        rows = np.concatenate([np.arange(f, l), li[lp[l - 1]:lp[l]]])
+        cols = ui[up[f]:up[f + 1]][l - f - 1:]
+        lsub.append(rows)
+        usub.append(cols)
+        xl.append(xl[-1] + len(rows))
+        xu.append(xu[-1] + len(cols))
+    cat = lambda parts: np.concatenate(parts).astype(np.int32) if parts else np.zeros(0, np.int32)  # noqa: E731
+    return {"xsup": xsup.astype(np.int32), "supno": supno, "xlsub": np.array(xl, np.int64),
+            "lsub": cat(lsub), "xusub": np.array(xu, np.int64), "usub": cat(usub)}

@@ -46,6 +46,8 @@ def test_params_layout_matches_header():
     # the ctypes mirror must have the C struct's size: 4*i32, 2*i64, 6*i32
     assert ctypes.sizeof(gsofa_b200.Params) == 4 * 4 + 2 * 8 + 6 * 4
     assert ctypes.sizeof(gsofa_b200._CResult) == 2 * 4 + 18 * 8 + 8 + 10 * 8
+    # gsofa_supernodal: 2*i32, 2*i64, 6 pointers
+    assert ctypes.sizeof(gsofa_b200._CSupernodal) == 2 * 4 + 2 * 8 + 6 * 8
 
 
 def test_read_text_matches_fixture(tmp_path):

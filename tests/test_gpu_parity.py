@@ -6,7 +6,7 @@ import pytest
 import gsofa_b200
 import oracle
 from gsofa_b200 import matgen
-from tests.common import assert_same, bundled, expected, random_graph
+from tests.common import assert_same, bundled, expected, random_graph, supernodal_reference
 
 pytestmark = pytest.mark.gpu
 
@@ -112,6 +112,27 @@ def test_reused_device_slab_gives_exact_results(ctx):
     m3 = ctx.upload(big)
     assert_same(ctx.symbfact(m3), _oracle(big), where="slab reused again")
     m3.free()
+
+
+@pytest.mark.parametrize("max_sn", [0, 8])
+def test_supernodal_structure(ctx, max_sn):
+    for g in (bundled(), matgen.grid3d(16, ordering="nd", drop_frac=0.1, seed=3),
+              matgen.powerlaw(1500, seed=9), random_graph(400, 0.02, 7)):
+        ref = _oracle(g, max_sn)
+        want = supernodal_reference(ref)
+        m = ctx.upload(g)
+        r, s = ctx.symbfact_supernodal(m, max_supernode_size=max_sn)
+        assert r.nnz_lu == ref["nnz_lu"] and s.n == g.n and s.nsuper == len(ref["sn_start"])
+        for k, v in want.items():
+            assert np.array_equal(getattr(s, k), v), f"{g.name} max_sn={max_sn}: {k}"
+        # into caller buffers larger than needed: the results are views of them
+        out = {k: np.full(v.size + 5, -7, v.dtype) for k, v in want.items()}
+        _, s2 = ctx.symbfact_supernodal(m, max_supernode_size=max_sn, out=out)
+        for k, v in want.items():
+            assert np.array_equal(getattr(s2, k), v) and np.shares_memory(getattr(s2, k), out[k])
+    small = {"lsub": np.zeros(1, np.int32)}
+    with pytest.raises(gsofa_b200.GsofaError):
+        ctx.symbfact_supernodal(ctx.upload(bundled()), out=small)
 
 
 def test_counts_only_and_pool_retry(ctx):

@@ -137,3 +137,26 @@ def test_serial_and_threaded_agree():
     for k in ("u_idx", "l_idx", "u_row_count", "l_col_count", "sn_start"):
         assert np.array_equal(a[k], b[k])
     assert a["fill_count"] == b["fill_count"] and a["e_insp"] == b["e_insp"]
+
+
+@pytest.mark.parametrize("max_sn", [0, 4])
+def test_supernode_structure_claims(max_sn):
+    """What the supernodal output relies on, checked on oracle patterns: in a
+    supernode [f, l) every U row j is {j+1 .. l-1} plus the same columns >= l,
+    and every L column's rows >= l lie inside the last column's."""
+    for g in (bundled(), matgen.grid3d(12, ordering="nd", drop_frac=0.1, seed=5),
+              matgen.powerlaw(800, seed=9), random_graph(200, 0.03, 4)):
+        r = oracle.symbfact(g.beg, g.end, g.adj, want_pattern=True, max_supernode_size=max_sn)
+        up, ui, lp, li = r["u_ptr"], r["u_idx"], r["l_ptr"], r["l_idx"]
+        xs = np.append(r["sn_start"], g.n)
+        for k in range(len(xs) - 1):
+            f, l = xs[k], xs[k + 1]
+            right = ui[up[f]:up[f + 1]]
+            right = right[right >= l]
+            last = set(li[lp[l - 1]:lp[l]].tolist())
+            for j in range(f, l):
+                row = ui[up[j]:up[j + 1]]
+                assert np.array_equal(row[:l - j - 1], np.arange(j + 1, l))
+                assert np.array_equal(row[row >= l], right)
+                col = li[lp[j]:lp[j + 1]]
+                assert set(col[col >= l].tolist()) <= last
