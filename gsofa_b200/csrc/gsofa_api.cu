@@ -654,9 +654,10 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         }
         if (host_timing)
             std::fprintf(stderr,
-                         "gsofa host: setup %.3f ms, launch..sync %.3f ms (kernel %.3f, traversals %.3f), "
-                         "results %.3f ms\n",
-                         t_launch - t_enter, t_done - t_launch, ms, h_misc[16] * 1e-6, now_ms() - t_done);
+                         "gsofa host: setup %.3f ms, launch..sync %.3f ms (kernel %.3f, traversals %.3f, "
+                         "mean CTA %.3f), results %.3f ms\n",
+                         t_launch - t_enter, t_done - t_launch, ms, h_misc[16] * 1e-6,
+                         h_misc[17] * 1e-6 / std::max(grid, 1), now_ms() - t_done);
         if (part_count > 1 && !download_lines) {
             for (int i = 0; i < count; i++) {
                 gsofa_result &r = out[i];

@@ -101,7 +101,8 @@ struct JobArgs {
                                   // [5] levels, [6] sources that reused state,
                                   // [7..13] cycles: seeding, levels, fold, count,
                                   // list output, clearing, pair wait;
-                                  // [14] ns until the traversals ended
+                                  // [14] ns until the traversals ended,
+                                  // [15] CTAs' traversal ns, summed
     uint32_t *status;
     uint16_t *stamp;           // pattern mode: per traversal, stamp_stride entries:
     int64_t stamp_stride;      // the chain index at which each vertex was first set
@@ -847,7 +848,7 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
 
     // ---- phase 1: traversals ------------------------------------------------
     unsigned long long t_start = 0;
-    if (blockIdx.x == 0 && tid == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_start));
+    if (tid == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_start));
     for (int w = tid; w < NS * a.state_words; w += BLOCK) smem_dyn[w] = 0u;
     if (gtid == 0) {
         sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0; sh.pool_cur = sh.pool_end = 0;
@@ -908,6 +909,11 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
         }
     }
     {
+        if (tid == 0) {   // this CTA's busy time, summed over CTAs (load balance)
+            unsigned long long t_done;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_done));
+            atomicAdd(&a.counters[15], t_done - t_start);
+        }
         int64_t *wsum = shs[0].warp;
         const int64_t e = block_sum<BLOCK>((int64_t)acc.edges, wsum);
         const int64_t x = block_sum<BLOCK>((int64_t)acc.xcnt, wsum);
