@@ -1,4 +1,4 @@
-"""The sharded (multi-GPU) path on CPU: two gloo ranks each compute their
+"""The sharded (multi-GPU) path on CPU: two or three gloo ranks each compute their
 interleaved source partition (with the oracle standing in for the rank's
 GPU, exactly as the kernel fills only its own lines), then combine through
 the library's all-reduce assembly and host supernode scan."""
@@ -49,12 +49,12 @@ def _worker(rank, world, port, kind, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("kind", ["bundled", "grid3d"])
-def test_two_gloo_ranks_assemble_the_full_factorization(kind):
+@pytest.mark.parametrize("kind,world", [("bundled", 2), ("grid3d", 2), ("grid3d", 3)])
+def test_gloo_ranks_assemble_the_full_factorization(kind, world):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, kind, q)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, kind, q)) for r in range(world)]
     for p in procs:
         p.start()
     outs = [q.get(timeout=300) for _ in procs]
