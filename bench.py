@@ -17,9 +17,10 @@ Printed (rank 0, one JSON line):
             result array including the pattern, all inside the timed region;
   roofline, cpu_baseline, clocks, gpu_launches as documented in the keys.
 
-Multi-GPU (torchrun): every rank factorizes its own copy of the workload (the
-units are independent factorizations; no data-path collective), so per-GPU
-work is fixed: weak scaling.
+Multi-GPU (torchrun): ONE matrix is split into contiguous source-line ranges
+of equal predicted work, one per rank; each rank factorizes its range with
+traversal reuse and the per-line arrays are summed over NCCL.  Total work is
+fixed as N grows: strong scaling.
 
 --impl reference times the CPU restatement of the reference algorithm (the
 reference has no CPU path of its own) on a bounded, evenly strided sample of
@@ -66,6 +67,13 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--form", choices=["ranges", "csr"], default="ranges",
+                    help="pattern form: begin/end ranges into a pool (no compaction) or CSR")
+    ap.add_argument("--state", choices=["auto", "global", "shared"], default="auto",
+                    help="where the traversals keep their visited bitmaps")
+    ap.add_argument("--partitions", type=int, default=4,
+                    help="one GPU: also time the matrix as this many work-predicted line ranges, "
+                         "one after another (the multi-GPU split, measured on one device; 0: skip)")
     ap.add_argument("--pattern", type=int, default=-1,
                     help="materialize the L+U pattern (-1: yes except for the circuit workload, "
                          "whose pattern does not fit in memory)")
@@ -176,24 +184,42 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def traffic_per_launch(cfg_name):
-    """DRAM bytes per factorization launch from the committed ncu summary."""
+def traffic_per_launch(cfg_name, form):
+    """DRAM bytes per factorization launch from the committed ncu summary
+    (profiles/traffic.json, keyed by workload and pattern form)."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(p) as f:
             d = json.load(f)
-        e = d.get(cfg_name)
+        e = d.get(f"{cfg_name}/{form}")
         return None if e is None else float(e["dram_bytes_per_launch"])
     except Exception:
         return None
 
 
-def cpu_sample(g, budget_s, step_hint=None):
-    """Times the oracle (all host threads) on every k-th source of both passes.
-    Returns (nnz_per_s, cores, description, k)."""
+def _line_orig(g, src):
+    """Distinct off-diagonal original entries of each listed line."""
+    out = np.zeros(src.shape[0], np.int64)
+    for i, s in enumerate(src.tolist()):
+        row = np.unique(g.adj[g.beg[s]:g.end[s]])
+        out[i] = row.shape[0] - int(np.any(row == s))
+    return out
+
+
+def cpu_sample(g, budget_s, step_hint=None, extras=True):
+    """Times the CPU oracle on every k-th line of the workload (the highest
+    line included), both reachability passes, all OpenMP threads, one line per
+    scheduling step with the heaviest lines first.  k is calibrated so the
+    timed run takes at least a quarter of budget_s (or given as step_hint).
+
+    Returns a dict: rate (nnz(L+U) of the sampled lines per second), the
+    sample, the oracle's per-line counts (c0: U rows, c1: L columns) for the
+    parity check, and -- with extras -- the same sample timed on one thread
+    (serial) and with the max-id restatement of the reference's own algorithm
+    (OpenMP) on a sub-sample."""
     import oracle
     n = g.n
-    cores = os.cpu_count() or 1
+    threads = oracle.threads()
 
     def run(k):
         src = np.arange(n - 1, -1, -k, dtype=np.int32)   # includes the heaviest line
@@ -201,18 +227,53 @@ def cpu_sample(g, budget_s, step_hint=None):
         c0, _, _, _ = oracle.counts(g.beg, g.end, g.adj, 0, nthreads=0, sources=src)
         c1, _, _, _ = oracle.counts(g.beg, g.end, g.adj, 1, nthreads=0, sources=src)
         dt = time.perf_counter() - t0
-        nnz = int(c0[src].sum() + c1[src].sum() + src.shape[0])
-        return nnz, dt, src.shape[0]
+        nnz = int(c0[src].sum(dtype=np.int64) + c1[src].sum(dtype=np.int64) + src.shape[0])
+        return nnz, dt, src, c0, c1
 
     k = step_hint or max(1, n // 64)
-    nnz, dt, ns = run(k)
-    while dt < budget_s / 4 and k > 1:
-        k = max(1, int(k * max(dt, 1e-3) / (budget_s / 2)) if dt > 0 else k // 8)
-        k = max(1, min(k, n))
-        nnz, dt, ns = run(k)
-        if dt >= budget_s / 4:
-            break
-    return nnz / dt, cores, f"every {k}-th line of both passes ({ns} of {n} sources), {dt:.2f} s", k
+    nnz, dt, src, c0, c1 = run(k)
+    while step_hint is None and dt < budget_s / 4 and k > 1:
+        k = max(1, min(n, int(k * max(dt, 1e-3) / (budget_s / 2))))
+        nnz, dt, src, c0, c1 = run(k)
+    out = {"rate": nnz / dt, "seconds": dt, "k": k, "sources": src, "c0": c0, "c1": c1,
+           "threads": threads, "cores": os.cpu_count() or 1,
+           "omp_num_threads": os.environ.get("OMP_NUM_THREADS"),
+           "desc": f"every {k}-th line of both passes ({src.shape[0]} of {n} sources), {dt:.2f} s"}
+    if not extras:
+        return out
+    # one thread on every m-th sampled line (about a quarter of the budget)
+    m = max(1, int(round(threads * dt / max(budget_s / 4, 1e-3))))
+    sub = src[::m]
+    t0 = time.perf_counter()
+    s0, _, _, _ = oracle.counts(g.beg, g.end, g.adj, 0, nthreads=1, sources=sub)
+    s1, _, _, _ = oracle.counts(g.beg, g.end, g.adj, 1, nthreads=1, sources=sub)
+    ts = time.perf_counter() - t0
+    out["serial"] = {"value": int(s0[sub].sum(dtype=np.int64) + s1[sub].sum(dtype=np.int64) + sub.shape[0]) / ts,
+                     "unit": "nnz/s", "cores": 1, "sample": f"every {k * m}-th line ({sub.shape[0]} sources), "
+                     f"{ts:.2f} s"}
+    # the reference's algorithm (max-id label propagation) on every 4th
+    # sampled line: nnz of a line = its fills + its distinct originals + 1
+    sub = src[::4]
+    t0 = time.perf_counter()
+    fills, _, _ = oracle.maxid_counts(g.beg, g.end, g.adj, sub)
+    tm = time.perf_counter() - t0
+    nnz_m = fills + int(_line_orig(g, sub).sum()) + sub.shape[0]
+    out["maxid"] = {"value": nnz_m / tm, "unit": "nnz/s", "cores": threads,
+                    "sample": f"every {4 * k}-th line ({sub.shape[0]} sources), {tm:.2f} s"}
+    return out
+
+
+def cpu_baseline_obj(cs):
+    """The JSON object of a CPU sample: the OpenMP reachability restatement is
+    the divisor; the serial run and the max-id restatement ride along."""
+    o = {"value": cs["rate"], "unit": "nnz/s", "cores": cs["threads"], "host_cores": cs["cores"],
+         "omp_num_threads": cs["omp_num_threads"], "kind": "port",
+         "algorithm": "two-pass reachability restatement, OpenMP, one line per scheduling step",
+         "sample": cs["desc"], "sample_sources": int(cs["sources"].shape[0])}
+    for key in ("serial", "maxid"):
+        if key in cs:
+            o[key] = cs[key]
+    return o
 
 
 def reference_arm(args):
@@ -220,26 +281,26 @@ def reference_arm(args):
     if rank != 0:
         return 0
     g, cfg = workload(args)
-    per_step = max(args.cpu_seconds / max(args.steps, 1), 1.0)
-    # one calibration + warm-up runs
-    rate, cores, desc, k = cpu_sample(g, per_step)
+    # one calibration (which also times the serial and max-id runs), then
+    # warm-up and timed steps on the same sample as the GPU arm's baseline
+    cs = cpu_sample(g, args.cpu_seconds)
     for _ in range(max(args.warmup - 1, 0)):
-        cpu_sample(g, per_step, step_hint=k)
+        cpu_sample(g, args.cpu_seconds, step_hint=cs["k"], extras=False)
     rates = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        r, cores, desc, _ = cpu_sample(g, per_step, step_hint=k)
-        rates.append(r)
+        rates.append(cpu_sample(g, args.cpu_seconds, step_hint=cs["k"], extras=False)["rate"])
     wall = time.perf_counter() - t0
     value = statistics.mean(rates)
+    base = cpu_baseline_obj(cs)
+    base["value"] = value
     line = {
         "metric": "nnz(L+U)/s", "value": value, "unit": "nnz/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * wall / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded generator)", "impl": "reference",
-        "config": dict(cfg, sample=desc),
-        "cpu_baseline": {"value": value, "unit": "nnz/s", "cores": cores, "kind": "port",
-                         "sample": desc},
+        "config": dict(cfg, sample=cs["desc"]),
+        "cpu_baseline": base,
         "e2e": {"value": value, "unit": "nnz/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -373,6 +434,198 @@ def serve_main(args):
     return 0
 
 
+def _sha(a, dtype) -> str:
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=dtype).tobytes()).hexdigest()
+
+
+def check_parity(g, workload_name, res, cs, want_pattern):
+    """Compares a GPU result (per-line arrays downloaded through the public
+    API) with the CPU oracle: the U row and L column counts of every sampled
+    line, the sorted lists of every 8th sampled line (pattern mode), and --
+    where tests/golden/large.json holds the workload -- the SHA-256 digests of
+    the full per-line arrays and supernode starts from a full oracle run."""
+    import oracle
+    src = cs["sources"]
+    bad = int(np.count_nonzero(res.u_row_count[src] != cs["c0"][src]))
+    bad += int(np.count_nonzero(res.l_col_count[src] != cs["c1"][src]))
+    out = {"lines_checked": int(src.shape[0]), "fields": ["u_row_count", "l_col_count"],
+           "sample": cs["desc"]}
+    if want_pattern and (res.u_ptr is not None or res.u_beg is not None):
+        sub = src[::8]
+        for pass_, cnt, row in ((0, cs["c0"], res.u_row), (1, cs["c1"], res.l_col)):
+            rp, ri = oracle.lists(g.beg, g.end, g.adj, pass_, sub, cnt)
+            for i, s_ in enumerate(sub.tolist()):
+                if not np.array_equal(row(s_), ri[rp[i]:rp[i + 1]]):
+                    bad += 1
+        out["lists_checked"] = int(2 * sub.shape[0])
+        out["fields"].append("sorted U row / L column lists")
+    gold = None
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "large.json")) as f:
+            gold = json.load(f).get(workload_name)
+    except (OSError, ValueError):
+        gold = None
+    if gold is not None:
+        flags = res.line_flags if res.line_flags is not None else None
+        got = {"u_row_count": _sha(res.u_row_count, "<i4"), "l_col_count": _sha(res.l_col_count, "<i4"),
+               "sn_start": _sha(res.sn_start, "<i4")}
+        if flags is not None:
+            got["line_flags"] = _sha(flags, "u1")
+        gm = [k for k, v in got.items() if v != gold["sha256"][k]]
+        gm += [k for k in ("fill_count", "nnz_lu", "n_supernodes") if int(getattr(res, k)) != int(gold[k])]
+        bad += len(gm)
+        out["golden"] = {"file": "tests/golden/large.json", "compared": sorted(got) + ["fill_count", "nnz_lu",
+                         "n_supernodes"], "mismatched": gm}
+    out["mismatches"] = bad
+    return out
+
+
+def _params(gsofa_b200, args, **kw):
+    """Library parameters from the command line (plus overrides)."""
+    flags = {"auto": 0, "global": gsofa_b200.FLAG_GLOBAL_STATE, "shared": gsofa_b200.FLAG_SHARED_STATE}[args.state]
+    base = dict(reuse=args.reuse, block_size=args.block, src_chunk=args.chunk, threads_per_source=args.lanes,
+                ctas_per_sm=args.ctas_per_sm, flags=flags)
+    extra_flags = kw.pop("flags", 0)
+    base.update(kw)
+    base["flags"] = flags | extra_flags
+    return gsofa_b200.Params.default(**base)
+
+
+def _device_timed(torch, stream, flush, steps, fn):
+    """Runs fn() `steps` times between CUDA events on the launching stream,
+    flushing L2 between steps; returns (ms, results)."""
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = []
+    for i in range(steps):
+        if i:
+            flush.fill_(i & 0xff)
+        out.append(fn())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), out
+
+
+def sharded_main(args, world, rank, local):
+    """N GPUs (torchrun): ONE matrix split over the ranks as contiguous line
+    ranges of equal predicted work (gsofa_partition_lines), each rank
+    factorizing its range with traversal reuse; the per-line arrays are then
+    summed over NCCL (distributed.symbfact_sharded).  Total work is fixed as N
+    grows: strong scaling.  value = factorizations of the whole matrix per
+    second, timed on the device as the max over ranks."""
+    import torch
+    import torch.distributed as dist
+    import gsofa_b200
+    from gsofa_b200 import distributed
+
+    g, cfg = workload(args)
+    want_pattern = args.pattern if args.pattern >= 0 else int(args.workload != "circuit")
+    ctx = gsofa_b200.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    m = ctx.upload(g)
+    nd = gsofa_b200.FLAG_NO_DOWNLOAD
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    cuts, pred = gsofa_b200.partition_lines(g, world)
+    lo, hi = int(cuts[rank]), int(cuts[rank + 1])
+    rp = distributed.rank_params(rank, world, cuts, _params(gsofa_b200, args, flags=nd))
+    share = ctx.symbfact(m, rp)
+    need = int(share.nnz_u + share.nnz_l)
+    if want_pattern:
+        dpool = torch.empty(max(need, 1), dtype=torch.int32, device="cuda")
+        pr = distributed.rank_params(rank, world, cuts, _params(gsofa_b200, args, flags=nd))
+        pr.want_pattern = 2
+        step = lambda: ctx.symbfact_ranges(m, dpool, pr)  # noqa: E731
+    else:
+        step = lambda: ctx.symbfact(m, rp)  # noqa: E731
+    for i in range(max(args.warmup, 1)):
+        if i:
+            flush.fill_(i & 0xff)
+        step()
+
+    def max_over_ranks(t):
+        tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    dist.barrier()
+    with ClockSampler(local) as clk:
+        t_ms, rs = _device_timed(torch, stream, flush, args.steps, step)
+    dist.barrier()
+    t_max = max_over_ranks(t_ms)
+    # assemble the whole factorization once (one sum-all-reduce over NCCL)
+    full = distributed.symbfact_sharded(ctx, m, rank, world, distributed.torch_allreduce(), 0,
+                                        params=_params(gsofa_b200, args), cuts=cuts)
+    nnz_lu = full["nnz_lu"]
+    value = args.steps * nnz_lu / (t_max / 1000.0)
+
+    # end to end: upload from pinned host buffers, this rank's range (counts
+    # and link flags to pinned buffers, lists to a pinned host pool), the NCCL
+    # sum of the per-line arrays and the host supernode scan, every step
+    pb = torch.from_numpy(g.beg).pin_memory()
+    pe = torch.from_numpy(g.end).pin_memory()
+    pa = torch.from_numpy(g.adj).pin_memory()
+    allred = distributed.torch_allreduce()
+    hpool = torch.empty(max(need, 1), dtype=torch.int32).pin_memory().numpy() if want_pattern else None
+
+    def e2e_step():
+        mm = ctx.upload(pb.numpy(), pe.numpy(), pa.numpy())
+        if want_pattern:
+            pp = distributed.rank_params(rank, world, cuts, _params(gsofa_b200, args))
+            pp.want_pattern = 2
+            r = ctx.symbfact_ranges(mm, hpool, pp)
+        else:
+            r = ctx.symbfact(mm, distributed.rank_params(rank, world, cuts, _params(gsofa_b200, args)))
+        mm.free()
+        return distributed.combine(g.n, r.u_row_count, r.l_col_count, r.line_flags, r.fill_count, allred)
+
+    e2e_step()
+    dist.barrier()
+    te, outs = _device_timed(torch, stream, flush, args.steps, e2e_step)
+    dist.barrier()
+    te = max_over_ranks(te)
+    assert outs[-1]["nnz_lu"] == nnz_lu
+    parity = None
+    if rank == 0:
+        gold = None
+        try:
+            with open(os.path.join(ROOT, "tests", "golden", "large.json")) as f:
+                gold = json.load(f).get(cfg["workload"])
+        except (OSError, ValueError):
+            gold = None
+        if gold is not None:
+            got = {"u_row_count": _sha(full["u_row_count"], "<i4"), "l_col_count": _sha(full["l_col_count"], "<i4"),
+                   "line_flags": _sha(full["line_flags"], "u1"), "sn_start": _sha(full["sn_start"], "<i4")}
+            bad = [k for k, v in got.items() if v != gold["sha256"][k]]
+            bad += [k for k in ("fill_count", "nnz_lu") if int(full[k]) != int(gold[k])]
+            parity = {"golden": "tests/golden/large.json", "mismatched": bad, "mismatches": len(bad)}
+        line = {
+            "metric": "nnz(L+U)/s", "value": value, "unit": "nnz/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator)",
+            "config": dict(cfg, nnz_lu=int(nnz_lu), fill_count=int(full["fill_count"]),
+                           supernodes=int(len(full["sn_start"])),
+                           pattern="begin/end ranges into a device pool per rank" if want_pattern else "counts only",
+                           l2="flushed between steps (256 MiB write)",
+                           parallelism=f"one matrix in {world} contiguous work-predicted line ranges, "
+                                       "one per rank; per-line arrays summed over NCCL"),
+            "cuts": [int(c) for c in cuts], "predicted_work": [float(w) for w in pred],
+            "factorizations_per_s": args.steps / (t_max / 1000.0),
+            "e2e": {"value": args.steps * nnz_lu / (te / 1000.0), "unit": "nnz/s", "ms_per_step": te / args.steps,
+                    "h2d_bytes_per_step": int((2 * g.n + g.nnz) * 4),
+                    "d2h_bytes_per_step": int(4 * need + 12 * g.n + 16 * g.n * int(bool(want_pattern))),
+                    "note": "per rank: its range's lists and per-line arrays; the NCCL sum is inside"},
+            "parity": parity, "clocks": clk.summary(), "gpu_launches": args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    dist.destroy_process_group()
+    return 1 if parity is not None and parity["mismatches"] else 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -393,145 +646,183 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
+        return sharded_main(args, world, rank, local)
 
     g, cfg = workload(args)
     want_pattern = args.pattern if args.pattern >= 0 else int(args.workload != "circuit")
+    form = args.form if want_pattern else "counts"
     ctx = gsofa_b200.Context(local)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
     m = ctx.upload(g)
-    params = gsofa_b200.Params.default(want_pattern=want_pattern, flags=gsofa_b200.FLAG_NO_DOWNLOAD,
-                                       reuse=args.reuse, block_size=args.block, src_chunk=args.chunk,
-                                       threads_per_source=args.lanes, ctas_per_sm=args.ctas_per_sm)
+    nd = gsofa_b200.FLAG_NO_DOWNLOAD
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    # one counts-only run sizes the pattern pool exactly
+    first = ctx.symbfact(m, _params(gsofa_b200, args, want_pattern=0, flags=nd))
+    need = int(first.nnz_u + first.nnz_l)
+    dpool = torch.empty(max(need, 1), dtype=torch.int32, device="cuda") if form == "ranges" else None
+    if form == "ranges":
+        params = _params(gsofa_b200, args, flags=nd)
+        step = lambda: ctx.symbfact_ranges(m, dpool, params)  # noqa: E731
+    else:
+        params = _params(gsofa_b200, args, want_pattern=int(form == "csr"), flags=nd)
+        step = lambda: ctx.symbfact(m, params)  # noqa: E731
 
     res = None
     # warm-up steps are timed steps untimed: the L2 flush runs too, so its
     # kernel is loaded before the timed region starts
-    for i in range(max(args.warmup, 0)):
+    for i in range(max(args.warmup, 1)):
         if i:
             flush.fill_(i & 0xff)
-        res = ctx.symbfact(m, params)
-    if res is None:
-        res = ctx.symbfact(m, params)
+        res = step()
 
     def barrier():
         if world > 1:
             dist.barrier()
 
-    # ---- device-resident timed region ------------------------------------
-    kernel_ms = []
-    barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for i in range(args.steps):
-            if i:
-                flush.fill_(i & 0xff)      # evict L2 between steps
-            r = ctx.symbfact(m, params)
-            kernel_ms.append(r.kernel_ms)
-        e1.record(stream)
-        torch.cuda.synchronize()
-    barrier()
-    t_ms = e0.elapsed_time(e1)
-    t_max = t_ms
-    if world > 1:
-        tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
+    def max_over_ranks(t):
+        if world == 1:
+            return t
+        tt = torch.tensor([t], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
+        return float(tt.item())
+
+    # ---- device-resident timed region ------------------------------------
+    barrier()
+    with ClockSampler(local) as clk:
+        t_ms, rs = _device_timed(torch, stream, flush, args.steps, step)
+    barrier()
+    kernel_ms = [r.kernel_ms for r in rs]
+    t_max = max_over_ranks(t_ms)
     nnz_lu = res.nnz_lu
     value = world * args.steps * nnz_lu / (t_max / 1000.0)
     facts = world * args.steps / (t_max / 1000.0)
 
+    # the other output forms of the same matrix, a few steps each (side numbers)
+    forms = {}
+    if want_pattern:
+        k3 = max(1, min(args.steps, 5))
+        for name, p in (("csr", _params(gsofa_b200, args, want_pattern=1, flags=nd)),
+                        ("counts", _params(gsofa_b200, args, want_pattern=0, flags=nd))):
+            if name == form:
+                continue
+            ctx.symbfact(m, p)
+            tf, rf = _device_timed(torch, stream, flush, k3, lambda: ctx.symbfact(m, p))
+            forms[name] = {"ms_per_step": tf / k3, "kernel_ms": statistics.mean(r.kernel_ms for r in rf),
+                           "value": k3 * nnz_lu / (tf / 1000.0)}
+
+    # the multi-GPU split measured on this device: the matrix as K contiguous
+    # line ranges of equal predicted work, one launch each, back to back
+    split = None
+    if world == 1 and args.partitions > 1:
+        cuts, pred = gsofa_b200.partition_lines(g, args.partitions)
+        part_ms, part_nnz = [], 0
+        for k in range(args.partitions):
+            lo, hi = int(cuts[k]), int(cuts[k + 1])
+            if form == "ranges":
+                pk = _params(gsofa_b200, args, flags=nd, line_lo=lo, line_hi=hi)
+                fn = lambda pk=pk: ctx.symbfact_ranges(m, dpool, pk)  # noqa: E731
+            else:
+                pk = _params(gsofa_b200, args, want_pattern=int(form == "csr"), flags=nd, line_lo=lo, line_hi=hi)
+                fn = lambda pk=pk: ctx.symbfact(m, pk)  # noqa: E731
+            fn()
+            k3 = max(1, min(args.steps, 5))
+            _, rk = _device_timed(torch, stream, flush, k3, fn)
+            part_ms.append(statistics.mean(r.kernel_ms for r in rk))
+            part_nnz += rk[-1].nnz_u + rk[-1].nnz_l
+        full_ms = statistics.mean(kernel_ms)
+        split = {"parts": args.partitions, "cuts": [int(c) for c in cuts], "predicted_work": [float(w) for w in pred],
+                 "kernel_ms": part_ms, "summed_kernel_ms": sum(part_ms), "unsplit_kernel_ms": full_ms,
+                 "summed_over_unsplit": sum(part_ms) / full_ms,
+                 "slowest_over_mean": max(part_ms) / statistics.mean(part_ms),
+                 "entries_match": bool(part_nnz == res.nnz_u + res.nnz_l)}
+
     # ---- end-to-end through the public API ----------------------------------
     e2e = None
+    out = None
     if not args.no_e2e:
         pb = torch.from_numpy(g.beg).pin_memory()
         pe = torch.from_numpy(g.end).pin_memory()
         pa = torch.from_numpy(g.adj).pin_memory()
-        pe2e = gsofa_b200.Params.default(want_pattern=want_pattern, reuse=args.reuse, block_size=args.block,
-                                         src_chunk=args.chunk, threads_per_source=args.lanes,
-                                         ctas_per_sm=args.ctas_per_sm)
-        # page-locked result buffers, sized from the warm-up result, reused
         n1 = g.n + 1
 
         def pinned(count, dt):
             return torch.empty(max(int(count), 1), dtype=dt).pin_memory().numpy()
 
+        # page-locked result buffers, sized from the counts run, reused
         bufs = {"u_row_count": pinned(g.n, torch.int32), "l_col_count": pinned(g.n, torch.int32),
                 "l_row_count": pinned(g.n, torch.int32), "sn_start": pinned(g.n, torch.int32)}
-        if want_pattern:
-            bufs.update(u_ptr=pinned(n1, torch.int64), l_ptr=pinned(n1, torch.int64),
-                        u_idx=pinned(res.nnz_u, torch.int32), l_idx=pinned(res.nnz_l, torch.int32))
-        out = None
+        if form == "ranges":
+            # the lists stream into page-locked host memory while the
+            # traversals run; per-line begins come back with the counts
+            hpool = pinned(need, torch.int32)
+            bufs.update(u_beg=pinned(g.n, torch.int64), l_beg=pinned(g.n, torch.int64))
+            pe2e = _params(gsofa_b200, args)
+            run = lambda mm: ctx.symbfact_ranges(mm, hpool, pe2e, out=bufs)  # noqa: E731
+        else:
+            if form == "csr":
+                bufs.update(u_ptr=pinned(n1, torch.int64), l_ptr=pinned(n1, torch.int64),
+                            u_idx=pinned(first.nnz_u, torch.int32), l_idx=pinned(first.nnz_l, torch.int32))
+            pe2e = _params(gsofa_b200, args, want_pattern=int(form == "csr"))
+            run = lambda mm: ctx.symbfact_into(mm, pe2e, bufs)  # noqa: E731
         for _ in range(2):   # warm the host-side allocations
             flush.fill_(1)
             mm = ctx.upload(pb.numpy(), pe.numpy(), pa.numpy())
-            out = ctx.symbfact_into(mm, pe2e, bufs)
+            out = run(mm)
             mm.free()
-        k2 = max(1, min(args.steps, 3))
-        barrier()
-        torch.cuda.synchronize()
-        f0 = torch.cuda.Event(enable_timing=True)
-        f1 = torch.cuda.Event(enable_timing=True)
-        f0.record(stream)
+        k2 = args.steps
         phases = {"upload_ms": 0.0, "factor_and_fetch_ms": 0.0, "free_ms": 0.0}
-        for i in range(k2):
-            if i:
-                flush.fill_(i & 0xff)
+
+        def e2e_step():
             h0 = time.perf_counter()
             mm = ctx.upload(pb.numpy(), pe.numpy(), pa.numpy())
             h1 = time.perf_counter()
-            out = ctx.symbfact_into(mm, pe2e, bufs)
+            o = run(mm)
             h2 = time.perf_counter()
             mm.free()
             h3 = time.perf_counter()
             phases["upload_ms"] += 1000 * (h1 - h0) / k2
             phases["factor_and_fetch_ms"] += 1000 * (h2 - h1) / k2
             phases["free_ms"] += 1000 * (h3 - h2) / k2
-        f1.record(stream)
-        torch.cuda.synchronize()
+            return o
+
         barrier()
-        te = f0.elapsed_time(f1)
-        if world > 1:
-            tt = torch.tensor([te], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            te = float(tt.item())
+        te, outs = _device_timed(torch, stream, flush, k2, e2e_step)
+        barrier()
+        te = max_over_ranks(te)
+        out = outs[-1]
         assert out.nnz_lu == nnz_lu and out.fill_count == res.fill_count
         h2d = (2 * g.n + g.nnz) * 4
         d2h = 3 * 4 * g.n + 4 * out.n_supernodes
-        if want_pattern:
-            d2h += 4 * (out.nnz_u + out.nnz_l) + 2 * 8 * (g.n + 1)
+        if form == "csr":
+            d2h += 4 * (out.nnz_u + out.nnz_l) + 2 * 8 * n1
+        elif form == "ranges":
+            d2h += 4 * out.pool_used + 2 * 8 * g.n
         e2e = {"value": world * k2 * nnz_lu / (te / 1000.0), "unit": "nnz/s", "steps": k2,
                "ms_per_step": te / k2, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "host_phases": phases, "kernel_ms": out.kernel_ms}
+               "form": form, "host_phases": phases, "kernel_ms": out.kernel_ms}
         if want_pattern:
             # the same steps for a consumer of the supernodal structure: the
             # pattern stays on the device and only the per-supernode index
             # lists come back
+            pcsr = _params(gsofa_b200, args)
             mm = ctx.upload(pb.numpy(), pe.numpy(), pa.numpy())
-            _, sup = ctx.symbfact_supernodal(mm, pe2e)
+            _, sup = ctx.symbfact_supernodal(mm, pcsr)
             mm.free()
-            # page-locked result buffers, sized from the warm-up call, reused
             snb = {k: torch.empty(max(getattr(sup, k).size, 1),
                                   dtype=torch.int64 if k in ("xlsub", "xusub") else torch.int32).pin_memory().numpy()
                    for k in ("xsup", "supno", "xlsub", "lsub", "xusub", "usub")}
-            torch.cuda.synchronize()
-            s0 = torch.cuda.Event(enable_timing=True)
-            s1 = torch.cuda.Event(enable_timing=True)
-            s0.record(stream)
-            for i in range(k2):
-                if i:
-                    flush.fill_(i & 0xff)
+
+            def sn_step():
                 mm = ctx.upload(pb.numpy(), pe.numpy(), pa.numpy())
-                rs, sup = ctx.symbfact_supernodal(mm, pe2e, out=snb)
+                o = ctx.symbfact_supernodal(mm, pcsr, out=snb)
                 mm.free()
-            s1.record(stream)
-            torch.cuda.synchronize()
-            ts = s0.elapsed_time(s1)
-            assert rs.nnz_lu == nnz_lu and sup.nsuper == res.n_supernodes
+                return o
+
+            ts, sns = _device_timed(torch, stream, flush, k2, sn_step)
+            rs_, sup = sns[-1]
+            assert rs_.nnz_lu == nnz_lu and sup.nsuper == res.n_supernodes
             d2h_sn = sum(int(getattr(sup, k).nbytes) for k in ("xsup", "supno", "xlsub", "lsub", "xusub", "usub"))
             e2e["supernodal"] = {"value": world * k2 * nnz_lu / (ts / 1000.0), "unit": "nnz/s",
                                  "ms_per_step": ts / k2, "h2d_bytes_per_step": int(h2d),
@@ -544,16 +835,14 @@ def main():
     # the model's |X| and E_insp come from one untimed run without reuse.
     ideal = res
     if args.reuse != 0:
-        ideal = ctx.symbfact(m, gsofa_b200.Params.default(
-            want_pattern=0, flags=gsofa_b200.FLAG_NO_DOWNLOAD, reuse=0, block_size=args.block,
-            threads_per_source=args.lanes, ctas_per_sm=args.ctas_per_sm))
+        ideal = ctx.symbfact(m, _params(gsofa_b200, args, want_pattern=0, flags=nd, reuse=0, src_chunk=0))
         assert ideal.nnz_lu == nnz_lu
     peak, peak_kind = hbm_peak()
     kms = statistics.mean(kernel_ms)
     n = g.n
     b_alg = 8 * ideal.x_total + 8 * ideal.e_insp + (4 * nnz_lu if want_pattern else 0) + 8 * n
     achieved = b_alg / (kms / 1000.0) / 1e9
-    traffic = traffic_per_launch(cfg["workload"])
+    traffic = traffic_per_launch(cfg["workload"], form)
     # the same byte model over the work this kernel actually did (expansions of
     # both passes, edges it inspected): how close the traversal it runs comes
     # to the bandwidth bound, as opposed to the per-source model above
@@ -570,9 +859,17 @@ def main():
                                res.cycles)), "ctas": res.ctas}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, cores, desc, _ = cpu_sample(g, args.cpu_seconds)
-        cpu = {"value": rate, "unit": "nnz/s", "cores": cores, "kind": "port", "sample": desc}
+    parity = None
+    if rank == 0:
+        # the oracle on a strided sample of the lines: timed as the CPU
+        # baseline, and its per-line results checked against the GPU's
+        cs = cpu_sample(g, args.cpu_seconds, extras=(world == 1))
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline_obj(cs)
+        chk = out
+        if chk is None:
+            chk = ctx.symbfact(m, _params(gsofa_b200, args, want_pattern=int(want_pattern != 0)))
+        parity = check_parity(g, cfg["workload"], chk, cs, want_pattern)
 
     if rank == 0:
         line = {
@@ -582,13 +879,17 @@ def main():
             "data": "synthetic (seeded generator)",
             "config": dict(cfg, nnz_lu=int(nnz_lu), fill_count=int(res.fill_count),
                            supernodes=int(res.n_supernodes),
-                           pattern="on device" if want_pattern else "counts only",
-                           reuse=args.reuse, l2="flushed between steps (256 MiB write)",
+                           pattern={"ranges": "begin/end ranges into a device pool", "csr": "CSR on the device",
+                                    "counts": "counts only"}[form],
+                           state=args.state, reuse=args.reuse, l2="flushed between steps (256 MiB write)",
                            parallelism=f"independent factorization per rank x{world}"),
             "factorizations_per_s": facts,
+            "other_forms": forms,
+            "split_on_one_gpu": split,
             "e2e": e2e,
             "roofline": roof,
             "cpu_baseline": cpu,
+            "parity": parity,
             "clocks": clk.summary(),
             "gpu_launches": args.steps,
         }
@@ -596,6 +897,9 @@ def main():
     ctx.close()
     if world > 1:
         dist.destroy_process_group()
+    if parity is not None and parity["mismatches"]:
+        print(f"parity check failed: {parity}", file=sys.stderr)
+        return 1
     return 0
 
 

@@ -40,6 +40,8 @@ BUSY = 8
 FLAG_NO_DOWNLOAD = 0x1
 FLAG_DEVICE_TIMING = 0x2
 FLAG_GRAPH = 0x4
+FLAG_GLOBAL_STATE = 0x8    # visited bitmaps in global memory (many traversals per SM, any n)
+FLAG_SHARED_STATE = 0x10   # visited bitmaps in shared memory (at most two per SM)
 
 
 class GsofaError(RuntimeError):
@@ -65,6 +67,8 @@ class Params(ctypes.Structure):
         ("flags", ctypes.c_int32),
         ("part_count", ctypes.c_int32),
         ("part_index", ctypes.c_int32),
+        ("line_lo", ctypes.c_int32),
+        ("line_hi", ctypes.c_int32),
     ]
 
     @classmethod
@@ -124,6 +128,9 @@ class _CResult(ctypes.Structure):
         ("l_ptr", _i64p),
         ("l_idx", _i32p),
         ("internal", ctypes.c_void_p),
+        ("u_beg", _i64p),
+        ("l_beg", _i64p),
+        ("pool_used", ctypes.c_int64),
     ]
 
 
@@ -159,6 +166,26 @@ class Result:
     u_idx: Optional[np.ndarray] = None
     l_ptr: Optional[np.ndarray] = None
     l_idx: Optional[np.ndarray] = None
+    # ranges form (Context.symbfact_ranges): U row s = pool[u_beg[s] :
+    # u_beg[s] + u_row_count[s]], L column j = pool[l_beg[j] : ...]
+    u_beg: Optional[np.ndarray] = None
+    l_beg: Optional[np.ndarray] = None
+    pool_used: int = 0
+    pool: Optional[np.ndarray] = None
+
+    def u_row(self, s: int) -> np.ndarray:
+        """Sorted columns > s of U row s (either pattern form)."""
+        if self.u_ptr is not None:
+            return self.u_idx[self.u_ptr[s]:self.u_ptr[s + 1]]
+        b = int(self.u_beg[s])
+        return self.pool[b:b + int(self.u_row_count[s])]
+
+    def l_col(self, j: int) -> np.ndarray:
+        """Sorted rows > j of L column j (either pattern form)."""
+        if self.l_ptr is not None:
+            return self.l_idx[self.l_ptr[j]:self.l_ptr[j + 1]]
+        b = int(self.l_beg[j])
+        return self.pool[b:b + int(self.l_col_count[j])]
 
 
 _lib = None
@@ -220,10 +247,20 @@ def lib():
     L.gsofa_result_fetch.argtypes = [vp, ctypes.POINTER(_CResult), _i32p, _i32p, _i32p, _i32p,
                                      _i64p, _i32p, _i64p, _i32p]
     L.gsofa_result_fetch.restype = ctypes.c_int
+    L.gsofa_symbfact_ranges.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.POINTER(Params),
+                                        vp, ctypes.c_int64, ctypes.POINTER(_CResult)]
+    L.gsofa_symbfact_ranges.restype = ctypes.c_int
+    L.gsofa_result_fetch_ranges.argtypes = [vp, ctypes.POINTER(_CResult), _i64p, _i64p]
+    L.gsofa_result_fetch_ranges.restype = ctypes.c_int
     L.gsofa_symbfact_counts_noalloc.argtypes = [ctypes.c_int, vp, ctypes.c_int32, ctypes.c_int64,
                                                 vp, vp, vp, ctypes.c_int32, vp, vp, vp,
                                                 ctypes.POINTER(ctypes.c_uint64)]
     L.gsofa_symbfact_counts_noalloc.restype = ctypes.c_int
+    L.gsofa_predict_line_counts.argtypes = [ctypes.c_int32, ctypes.c_int64, _i32p, _i32p, _i32p, _i64p]
+    L.gsofa_predict_line_counts.restype = ctypes.c_int
+    L.gsofa_partition_lines.argtypes = [ctypes.c_int32, ctypes.c_int64, _i32p, _i32p, _i32p, ctypes.c_int32,
+                                        _i32p, ctypes.POINTER(ctypes.c_double)]
+    L.gsofa_partition_lines.restype = ctypes.c_int
     L.gsofa_supernodes_from_lines.argtypes = [ctypes.c_int32, _i32p, ctypes.POINTER(ctypes.c_uint8),
                                               ctypes.c_int32, _i32p]
     L.gsofa_supernodes_from_lines.restype = ctypes.c_int32
@@ -304,6 +341,9 @@ def _convert(r: _CResult) -> Result:
     out.l_ptr = _arr(r.l_ptr, n + 1, np.int64)
     out.u_idx = _arr(r.u_idx, int(r.nnz_u), np.int32)
     out.l_idx = _arr(r.l_idx, int(r.nnz_l), np.int32)
+    out.u_beg = _arr(r.u_beg, n, np.int64)
+    out.l_beg = _arr(r.l_beg, n, np.int64)
+    out.pool_used = int(r.pool_used)
     return out
 
 
@@ -402,30 +442,34 @@ class Context:
         _check(lib().gsofa_symbfact(self._h, m.handle, ctypes.byref(p), ctypes.byref(r)), "gsofa_symbfact")
         try:
             res = _convert(r)
-            ns, nl, nu = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int64()
-            _check(lib().gsofa_result_supernodal_sizes(self._h, ctypes.byref(r), ctypes.byref(ns),
-                                                       ctypes.byref(nl), ctypes.byref(nu)),
-                   "gsofa_result_supernodal_sizes")
-            k, n = ns.value, res.n
-            need = {"xsup": (k + 1, np.int32), "supno": (n, np.int32), "xlsub": (k + 1, np.int64),
-                    "lsub": (nl.value, np.int32), "xusub": (k + 1, np.int64), "usub": (nu.value, np.int32)}
-            bufs = {}
-            for key, (cnt, dt) in need.items():
-                b = None if out is None else out.get(key)
-                if b is None:
-                    b = np.empty(max(cnt, 1), dt)
-                elif b.shape[0] < cnt or b.dtype != dt:
-                    raise GsofaError(1, f"buffer {key} holds {b.shape[0]} {b.dtype} < {cnt} {np.dtype(dt)}")
-                bufs[key] = b
-            ptr = lambda key: bufs[key].ctypes.data_as(_i64p if key.startswith("x") and key != "xsup"  # noqa: E731
-                                                        else _i32p)
-            _check(lib().gsofa_result_supernodal_fetch(self._h, ctypes.byref(r), ptr("xsup"), ptr("supno"),
-                                                       ptr("xlsub"), ptr("lsub"), ptr("xusub"), ptr("usub")),
-                   "gsofa_result_supernodal_fetch")
-            sup = Supernodal(n, k, *(bufs[key][:cnt] for key, (cnt, _) in need.items()))
-            return res, sup
+            return res, self._supernodal_of(r, res.n, out)
         finally:
             lib().gsofa_result_free(ctypes.byref(r))
+
+    def _supernodal_of(self, r: "_CResult", n: int, out: Optional[dict]) -> "Supernodal":
+        """The supernodal structure of the C result r (last job on this
+        context, made with the pattern) into new or caller buffers."""
+        ns, nl, nu = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().gsofa_result_supernodal_sizes(self._h, ctypes.byref(r), ctypes.byref(ns),
+                                                   ctypes.byref(nl), ctypes.byref(nu)),
+               "gsofa_result_supernodal_sizes")
+        k = ns.value
+        need = {"xsup": (k + 1, np.int32), "supno": (n, np.int32), "xlsub": (k + 1, np.int64),
+                "lsub": (nl.value, np.int32), "xusub": (k + 1, np.int64), "usub": (nu.value, np.int32)}
+        bufs = {}
+        for key, (cnt, dt) in need.items():
+            b = None if out is None else out.get(key)
+            if b is None:
+                b = np.empty(max(cnt, 1), dt)
+            elif b.shape[0] < cnt or b.dtype != dt:
+                raise GsofaError(1, f"buffer {key} holds {b.shape[0]} {b.dtype} < {cnt} {np.dtype(dt)}")
+            bufs[key] = b
+        ptr = lambda key: bufs[key].ctypes.data_as(_i64p if key.startswith("x") and key != "xsup"  # noqa: E731
+                                                    else _i32p)
+        _check(lib().gsofa_result_supernodal_fetch(self._h, ctypes.byref(r), ptr("xsup"), ptr("supno"),
+                                                   ptr("xlsub"), ptr("lsub"), ptr("xusub"), ptr("usub")),
+               "gsofa_result_supernodal_fetch")
+        return Supernodal(n, k, *(bufs[key][:cnt] for key, (cnt, _) in need.items()))
 
     def symbfact_into(self, m: Matrix, params: Params, out: dict) -> Result:
         """Factorizes and copies every result array into caller-owned host
@@ -457,6 +501,81 @@ class Context:
             return res
         finally:
             lib().gsofa_result_free(ctypes.byref(r))
+
+    def symbfact_ranges(self, mats, pool, params: Optional[Params] = None, out: Optional[dict] = None,
+                        supernodal: bool = False, **kw):
+        """The pattern in the reference's begin/end layout, written straight
+        into `pool`: a numpy int32 array in page-locked host memory (e.g. a
+        view of a pinned torch tensor; the lists then travel to the host
+        while the traversals run) or a CUDA int32 torch tensor on this
+        context's device.  `mats` is one Matrix or a sequence (one launch).
+
+        Returns a Result (or a list of them) whose u_beg / l_beg index into
+        the pool (Result.u_row / l_col read lists back from a host pool).
+        Raises GsofaError(3) when the pool is too small; its `needed`
+        attribute then holds the entries the job needs.  `out` may hold
+        caller buffers for the per-line arrays (u_row_count, l_col_count,
+        l_row_count, sn_start, u_beg, l_beg), filled without allocation.
+        supernodal=True (one matrix) returns (Result, Supernodal), the
+        structure built on the device from the pool."""
+        single = isinstance(mats, Matrix)
+        ms = [mats] if single else list(mats)
+        p = Params()
+        ctypes.pointer(p)[0] = params if params is not None else Params.default(**kw)
+        p.want_pattern = 2
+        if out is not None:
+            p.flags |= FLAG_NO_DOWNLOAD
+        host = isinstance(pool, np.ndarray)
+        if host:
+            if pool.dtype != np.int32 or not pool.flags["C_CONTIGUOUS"]:
+                raise GsofaError(1, "pool must be a contiguous int32 array")
+            addr, cap = pool.ctypes.data, pool.shape[0]
+        else:
+            if str(getattr(pool, "dtype", "")) != "torch.int32" or not pool.is_contiguous():
+                raise GsofaError(1, "pool must be a contiguous int32 tensor")
+            addr, cap = pool.data_ptr(), pool.numel()
+        k = len(ms)
+        hs = (ctypes.c_void_p * k)(*[m.handle for m in ms])
+        rs = (_CResult * k)()
+        st = lib().gsofa_symbfact_ranges(self._h, k, hs, ctypes.byref(p), ctypes.c_void_p(addr), int(cap), rs)
+        if st != OK:
+            err = GsofaError(st, "gsofa_symbfact_ranges")
+            err.needed = int(rs[0].pool_used)
+            raise err
+        try:
+            res = [_convert(rs[i]) for i in range(k)]
+            if out is not None:
+                if k != 1:
+                    raise GsofaError(1, "caller buffers take one matrix")
+                r0 = res[0]
+                n = r0.n
+                for key, dt in (("u_row_count", np.int32), ("l_col_count", np.int32), ("l_row_count", np.int32),
+                                ("sn_start", np.int32), ("u_beg", np.int64), ("l_beg", np.int64)):
+                    cnt = r0.n_supernodes if key == "sn_start" else n
+                    b = out.get(key)
+                    if b is None or b.shape[0] < cnt or b.dtype != dt:
+                        raise GsofaError(1, f"buffer {key} missing or smaller than {cnt} {np.dtype(dt)}")
+                    setattr(r0, key, b[:cnt])
+                _check(lib().gsofa_result_fetch(self._h, ctypes.byref(rs[0]),
+                                                out["u_row_count"].ctypes.data_as(_i32p),
+                                                out["l_col_count"].ctypes.data_as(_i32p),
+                                                out["l_row_count"].ctypes.data_as(_i32p),
+                                                out["sn_start"].ctypes.data_as(_i32p), None, None, None, None),
+                       "gsofa_result_fetch")
+                _check(lib().gsofa_result_fetch_ranges(self._h, ctypes.byref(rs[0]),
+                                                       out["u_beg"].ctypes.data_as(_i64p),
+                                                       out["l_beg"].ctypes.data_as(_i64p)),
+                       "gsofa_result_fetch_ranges")
+            for r in res:
+                r.pool = pool if host else None
+            if supernodal:
+                if k != 1:
+                    raise GsofaError(1, "the supernodal structure takes one matrix")
+                return res[0], self._supernodal_of(rs[0], res[0].n, None)
+            return res[0] if single else res
+        finally:
+            for i in range(k):
+                lib().gsofa_result_free(ctypes.byref(rs[i]))
 
     def symbfact_batch(self, mats: Sequence[Matrix], params: Optional[Params] = None, **kw) -> List[Result]:
         p = params if params is not None else Params.default(**kw)
@@ -614,6 +733,35 @@ def symbfact_counts_noalloc(device: int, stream: int, n: int, nnz: int, d_beg: i
     return int(summary[0]), int(summary[1]), int(summary[2])
 
 
+def partition_lines(g: Graph, parts: int):
+    """Contiguous source-line ranges of equal predicted work (host):
+    returns (cuts int32[parts+1], predicted work float64[parts]); part p is
+    lines [cuts[p], cuts[p+1])."""
+    beg = np.ascontiguousarray(g.beg, dtype=np.int32)
+    end = np.ascontiguousarray(g.end, dtype=np.int32)
+    adj = np.ascontiguousarray(g.adj if g.nnz else np.zeros(1, np.int32), dtype=np.int32)
+    cuts = np.zeros(parts + 1, np.int32)
+    work = np.zeros(parts, np.float64)
+    _check(lib().gsofa_partition_lines(int(g.n), int(g.nnz), beg.ctypes.data_as(_i32p), end.ctypes.data_as(_i32p),
+                                       adj.ctypes.data_as(_i32p), int(parts), cuts.ctypes.data_as(_i32p),
+                                       work.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+           "gsofa_partition_lines")
+    return cuts, work
+
+
+def predict_line_counts(g: Graph) -> np.ndarray:
+    """Upper bound on every line's |U row| and |L column| from the symmetric
+    structure A + A^T (exact for symmetric patterns); host-only."""
+    beg = np.ascontiguousarray(g.beg, dtype=np.int32)
+    end = np.ascontiguousarray(g.end, dtype=np.int32)
+    adj = np.ascontiguousarray(g.adj if g.nnz else np.zeros(1, np.int32), dtype=np.int32)
+    out = np.zeros(max(g.n, 1), np.int64)
+    _check(lib().gsofa_predict_line_counts(int(g.n), int(g.nnz), beg.ctypes.data_as(_i32p),
+                                           end.ctypes.data_as(_i32p), adj.ctypes.data_as(_i32p),
+                                           out.ctypes.data_as(_i64p)), "gsofa_predict_line_counts")
+    return out[:g.n]
+
+
 def supernodes_from_lines(u_row_count, line_flags, max_supernode_size: int = 0) -> np.ndarray:
     """Supernode starts from per-line U row counts and link flags (host)."""
     u = np.ascontiguousarray(u_row_count, dtype=np.int32)
@@ -634,9 +782,12 @@ def exported_symbols() -> List[str]:
             "gsofa_create", "gsofa_destroy", "gsofa_set_stream", "gsofa_read_text", "gsofa_write_binary",
             "gsofa_free", "gsofa_upload",
             "gsofa_matrix_free", "gsofa_matrix_n", "gsofa_symbfact", "gsofa_symbfact_batch",
-            "gsofa_result_free", "gsofa_result_fetch", "gsofa_result_supernodal", "gsofa_supernodal_free",
+            "gsofa_result_free", "gsofa_result_fetch", "gsofa_symbfact_ranges", "gsofa_result_fetch_ranges",
+            "gsofa_result_supernodal", "gsofa_supernodal_free",
             "gsofa_result_supernodal_sizes", "gsofa_result_supernodal_fetch",
             "gsofa_predict_scratch_bytes",
-            "gsofa_symbfact_counts_noalloc", "gsofa_supernodes_from_lines", "gsofa_server_create",
+            "gsofa_symbfact_counts_noalloc", "gsofa_supernodes_from_lines", "gsofa_partition_lines",
+            "gsofa_predict_line_counts",
+            "gsofa_server_create",
             "gsofa_server_destroy", "gsofa_server_request_bytes", "gsofa_server_submit",
             "gsofa_server_poll", "gsofa_server_result", "gsofa_server_drain"]

@@ -9,6 +9,7 @@
 #include "gsofa_device.cuh"
 #include "gsofa_server.cuh"
 #include "gsofa_supernodal.cuh"
+#include "gsofa_partition.hpp"
 
 #include <cuda_runtime.h>
 
@@ -52,6 +53,15 @@ gsofa_status fail_cuda(cudaError_t e)
     return (e == cudaErrorMemoryAllocation) ? GSOFA_ERR_OOM : GSOFA_ERR_CUDA;
 }
 
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) belongs to the kernel and
+// is shared by every caller in the process: each launch sets it and launches
+// under this lock, so another host thread cannot resize it in between.
+std::mutex &kernel_attr_mutex()
+{
+    static std::mutex m;
+    return m;
+}
+
 // Grow-only device buffer owned by a context.
 struct DevBuf {
     void *p = nullptr;
@@ -81,6 +91,7 @@ struct gsofa_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // job scratch
     DevBuf queue, cnt, nxt, poff, gptr, lrow, snind, snlist, tiles, misc, pool, out, mats, ranges, stamp;
+    DevBuf gstate;            // visited bitmaps of the global-state kernels
     DevBuf sn_head, sn_data;  // gsofa_result_supernodal: sizes and offsets; index lists
     std::vector<int64_t> sn_xl, sn_xu;   // supernodal offsets of the result sizes were taken for
     const void *sn_for = nullptr;        // ... that result (its internal record)
@@ -92,7 +103,7 @@ struct gsofa_ctx {
     DevBuf matinfo;
     GraphCache graph;         // last captured job (GSOFA_FLAG_GRAPH)
     // launch shapes already sized: (block, bitmap words) -> (ring, CTAs/SM)
-    struct Shape { int block; int32_t words; bool paired; int ring; int occ; };
+    struct Shape { int block; int32_t words; bool paired; bool gbm; int ring; int occ; };
     std::vector<Shape> shapes;
 
     void *grow(DevBuf &b, size_t bytes)
@@ -182,7 +193,17 @@ struct ResultInternal {
     int64_t L, line_base, n;
     int64_t u0, l0;         // first index of the U rows / L columns in `out`
     int64_t sn0;            // first supernode of this matrix in the device list
-    int pattern;            // the job kept the pattern
+    int pattern;            // the job's pattern form: 0 none, 1 CSR in `out`,
+                            // 2 ranges in the caller's pool (begins in poff)
+    const int32_t *pool;    // ranges form: the pool's device address
+};
+
+// The caller's pattern pool of the ranges form (gsofa_symbfact_ranges):
+// a device address (device memory, or the device alias of page-locked host
+// memory) and its capacity in entries.
+struct ExtPool {
+    int32_t *dev = nullptr;
+    int64_t cap = 0;
 };
 
 int pick_block(int32_t max_n)
@@ -191,19 +212,29 @@ int pick_block(int32_t max_n)
     return 512;
 }
 
-template <int BLOCK, bool PAIRED>
+template <int BLOCK, bool PAIRED, bool GBM>
 void *factor_fn()
 {
-    return (void *)factor_kernel<BLOCK, PAIRED>;
+    return (void *)factor_kernel<BLOCK, PAIRED, GBM>;
 }
 
-void *factor_kernel_for(int block, bool paired)
+// The factorization kernel for a launch shape: threads per CTA, the two
+// passes side by side (paired), the visited bitmaps in global memory (gbm).
+void *factor_kernel_for(int block, bool paired, bool gbm = false)
 {
+    if (gbm) {
+        switch (block) {
+        case 128: return paired ? factor_fn<128, true, true>() : factor_fn<128, false, true>();
+        case 256: return paired ? factor_fn<256, true, true>() : factor_fn<256, false, true>();
+        case 512: return paired ? factor_fn<512, true, true>() : factor_fn<512, false, true>();
+        default: return nullptr;
+        }
+    }
     switch (block) {
-    case 128: return paired ? nullptr : factor_fn<128, false>();
-    case 256: return paired ? factor_fn<256, true>() : factor_fn<256, false>();
-    case 512: return paired ? factor_fn<512, true>() : factor_fn<512, false>();
-    case 1024: return paired ? factor_fn<1024, true>() : factor_fn<1024, false>();
+    case 128: return paired ? nullptr : factor_fn<128, false, false>();
+    case 256: return paired ? factor_fn<256, true, false>() : factor_fn<256, false, false>();
+    case 512: return paired ? factor_fn<512, true, false>() : factor_fn<512, false, false>();
+    case 1024: return paired ? factor_fn<1024, true, false>() : factor_fn<1024, false, false>();
     default: return nullptr;
     }
 }
@@ -237,6 +268,9 @@ void free_result_arrays(gsofa_result *r)
     std::free(r->u_idx);
     std::free(r->l_ptr);
     std::free(r->l_idx);
+    std::free(r->u_beg);
+    std::free(r->l_beg);
+    r->u_beg = r->l_beg = nullptr;
     r->u_row_count = r->l_col_count = r->l_row_count = r->sn_start = nullptr;
     r->u_ptr = r->l_ptr = nullptr;
     r->u_idx = r->l_idx = nullptr;
@@ -250,7 +284,7 @@ double now_ms()
 }
 
 gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
-                     const gsofa_params *pin, gsofa_result *out)
+                     const gsofa_params *pin, gsofa_result *out, const ExtPool *ext = nullptr)
 {
     static const bool host_timing = std::getenv("GSOFA_HOST_TIMING") != nullptr;
     const double t_enter = now_ms();
@@ -265,11 +299,39 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     const int part_count = p.part_count > 1 ? p.part_count : 1;
     const int part_index = p.part_count > 1 ? p.part_index : 0;
     if (part_index < 0 || part_index >= part_count) return GSOFA_ERR_INVALID_INPUT;
-    const bool want_pattern = p.want_pattern != 0 && part_count == 1;
+    // a contiguous range of source lines [line_lo, line_hi) of one matrix
+    const bool line_range = p.line_lo != 0 || p.line_hi != 0;
+    if (line_range && (count != 1 || part_count > 1 || p.line_lo < 0 || p.line_hi < p.line_lo))
+        return GSOFA_ERR_INVALID_INPUT;
+    const int32_t range_lo = line_range ? std::min(p.line_lo, mats[0]->n) : 0;
+    const int32_t range_hi = line_range ? std::min(p.line_hi, mats[0]->n) : 0;
+    const bool subset = part_count > 1 || line_range;   // some lines are not processed
+    // pattern form: 1 CSR (lists compacted into line order), 2 ranges (lists
+    // left where their chains wrote them, in the caller's pool)
+    if (p.want_pattern == 2 && !ext) return GSOFA_ERR_INVALID_INPUT;
+    if (ext && (p.want_pattern != 2 || part_count != 1)) return GSOFA_ERR_INVALID_INPUT;
+    const int pattern_form = (p.want_pattern != 0 && part_count == 1) ? (ext ? 2 : 1) : 0;
+    const bool want_pattern = pattern_form != 0;
     // reuse: -1 (auto) or 1 = paired passes with exact reuse when two bitmaps
     // fit in shared memory, else adjacency chains; 2 = adjacency chains;
-    // 0 = every source from scratch
+    // 0 = every source from scratch.  Interleaved partitions have no
+    // consecutive sources, so they run without reuse; line ranges keep it.
     const int reuse = (p.reuse != 0 && part_count == 1) ? 1 : 0;
+    // distinct original entries of the processed lines (their fill count
+    // subtracts them)
+    auto processed_orig = [&](int i) -> uint64_t {
+        const int64_t n = mats[i]->n;
+        std::vector<int32_t> ou((size_t)n), ol((size_t)n);
+        GS_CUDA(cudaMemcpy(ou.data(), mats[i]->d_orig_up, n * 4, cudaMemcpyDeviceToHost));
+        GS_CUDA(cudaMemcpy(ol.data(), mats[i]->d_orig_lo, n * 4, cudaMemcpyDeviceToHost));
+        uint64_t o = 0;
+        if (line_range) {
+            for (int64_t q = range_lo; q < range_hi; q++) o += (uint64_t)ou[q] + (uint64_t)ol[q];
+        } else {
+            for (int64_t q = part_index; q < n; q += part_count) o += (uint64_t)ou[q] + (uint64_t)ol[q];
+        }
+        return o;
+    };
 
     // line space and per-matrix descriptors
     std::vector<MatDesc> md(count);
@@ -292,11 +354,20 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     // whole number of 16-byte groups
     const int32_t words_needed = ((max_n + 31) / 32 + 127) / 128 * 128;
     const int32_t state_needed = words_needed + words_needed / 32 + ((words_needed / 32 + 31) / 32 + 3) / 4 * 4;
-    const bool paired = reuse && p.reuse != 2 &&
-                        (size_t)2 * state_needed * 4 + 2 * 1024 * 4 + sizeof(SharedState) * 2 + 1024 <=
-                            ctx->smem_optin;
-    int block = p.block_size ? p.block_size : pick_block(max_n) * (paired ? 2 : 1);
-    void *kfn = factor_kernel_for(block, paired);
+    // Where the visited bitmaps live: shared memory holds two of them (the
+    // paired kernel) up to ~850K lines and one up to ~1.7M; global memory
+    // holds any number of any size.  GSOFA_FLAG_GLOBAL_STATE /
+    // GSOFA_FLAG_SHARED_STATE choose; else shared memory while the pair fits.
+    const size_t pair_smem = (size_t)2 * state_needed * 4 + 2 * 1024 * 4 + sizeof(SharedState) * 2 + 1024;
+    if ((p.flags & GSOFA_FLAG_GLOBAL_STATE) && (p.flags & GSOFA_FLAG_SHARED_STATE)) return GSOFA_ERR_INVALID_INPUT;
+    const size_t single_smem = (size_t)state_needed * 4 + 1024 * 4 + sizeof(SharedState) + 1024;
+    const bool want_pair = reuse && p.reuse != 2;
+    const bool gbm = (p.flags & GSOFA_FLAG_GLOBAL_STATE) ||
+                     (!(p.flags & GSOFA_FLAG_SHARED_STATE) &&
+                      ((want_pair && pair_smem > ctx->smem_optin) || single_smem > ctx->smem_optin));
+    const bool paired = want_pair && (gbm || pair_smem <= ctx->smem_optin);
+    int block = p.block_size ? p.block_size : (gbm ? (paired ? 256 : 128) : pick_block(max_n) * (paired ? 2 : 1));
+    void *kfn = factor_kernel_for(block, paired, gbm);
     if (!kfn) return GSOFA_ERR_INVALID_INPUT;
     const int NS = paired ? 2 : 1;
     int lanes = p.threads_per_source ? p.threads_per_source : 1;
@@ -306,21 +377,25 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     const int32_t bitmap_words = words_needed;
     const int32_t state_words = state_needed;
     const size_t static_smem = sizeof(SharedState) * NS + 1024;
-    if ((size_t)NS * (state_words * 4 + 1024 * 4) + static_smem > ctx->smem_optin) return GSOFA_ERR_UNSUPPORTED;
+    // shared memory per traversal: its bitmap and summaries (unless in global
+    // memory) and its frontier ring
+    const size_t smem_state = gbm ? 0 : (size_t)state_words * 4;
+    if ((size_t)NS * (smem_state + 1024 * 4) + static_smem > ctx->smem_optin) return GSOFA_ERR_UNSUPPORTED;
     // frontier ring: the largest of 8K/4K/2K/1K entries that keeps the most
     // CTAs (each with its own bitmap) resident on an SM; sized once per shape
     int ring = 0, occ = 0;
     size_t smem = 0;
     bool cached = false;
     for (const auto &sh : ctx->shapes)
-        if (sh.block == block && sh.words == bitmap_words && sh.paired == paired) {
+        if (sh.block == block && sh.words == bitmap_words && sh.paired == paired && sh.gbm == gbm) {
             ring = sh.ring; occ = sh.occ; cached = true;
         }
     if (cached) {
-        smem = (size_t)NS * ((size_t)state_words * 4 + (size_t)ring * 4);
+        smem = (size_t)NS * (smem_state + (size_t)ring * 4);
     } else {
+        std::lock_guard<std::mutex> lk(kernel_attr_mutex());
         for (int cand = 8192; cand >= 1024; cand >>= 1) {
-            const size_t sm = (size_t)NS * ((size_t)state_words * 4 + (size_t)cand * 4);
+            const size_t sm = (size_t)NS * (smem_state + (size_t)cand * 4);
             if (sm + static_smem > ctx->smem_optin) continue;
             GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
             int o = 0;
@@ -328,19 +403,37 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
             if (o > occ) { occ = o; ring = cand; smem = sm; }
         }
         if (occ <= 0) return GSOFA_ERR_UNSUPPORTED;
-        ctx->shapes.push_back({block, bitmap_words, paired, ring, occ});
+        ctx->shapes.push_back({block, bitmap_words, paired, gbm, ring, occ});
     }
-    // the attribute belongs to the kernel, which other callers may resize
-    GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = p.ctas_per_sm > 0 ? std::min(p.ctas_per_sm, occ) : occ;
-    const int grid = per_sm * ctx->sm_count;
+    int grid = per_sm * ctx->sm_count;
+    {
+        // Concurrent traversals within the memory budget (the reference
+        // shrinks its sources per pass until the state fits its pool,
+        // with_space_optimization/symbfact.cuh:1465-1507): every traversal
+        // holds a frontier queue of n entries and, with the pattern, a row of
+        // n chain stamps; the per-line arrays and a minimal pool come first.
+        const int64_t q = std::max<int64_t>(p.queue_capacity, max_n);
+        const int64_t per_cta = (int64_t)NS * (q * 4 + (want_pattern ? (int64_t)words_needed * 32 * 2 : 0) +
+                                               (gbm ? (int64_t)state_words * 4 : 0));
+        // cnt, nxt, poff, gptr, lrow, snind, sn_list
+        const int64_t per_line = 2 * 4 + 2 + 2 * 8 + 2 * 8 + 4 + 1 + 4;
+        const int64_t fixed = L * per_line + ((L + TILE - 1) / TILE) * 32 + 64 * 1024 +
+                              (want_pattern ? (int64_t)2 * 4 * (1 << 20) : 0);
+        const int64_t others = (int64_t)ctx->held - (int64_t)ctx->queue.bytes - (int64_t)ctx->stamp.bytes -
+                               (int64_t)ctx->gstate.bytes;
+        const int64_t room = (int64_t)ctx->budget - others - fixed;
+        if (room < per_cta) return GSOFA_ERR_OOM;
+        grid = (int)std::min<int64_t>(grid, room / per_cta);
+    }
     // sources per work piece: a piece's first source cannot reuse state, so
     // pieces are long (up to 512 sources) while there are still about eight
     // per concurrent traversal -- the last pieces handed out are the light,
     // low-numbered sources, so the launch's tail stays short
     int chunk = p.src_chunk;
     if (chunk <= 0) {
-        const int64_t per = (int64_t)(paired ? 1 : 2) * L / ((int64_t)8 * grid);
+        const int64_t lines = line_range ? (int64_t)(range_hi - range_lo) : L;   // sources per pass
+        const int64_t per = (int64_t)(paired ? 1 : 2) * lines / ((int64_t)8 * grid);
         chunk = reuse ? (int)std::min<int64_t>(512, std::max<int64_t>(32, per)) : 1;
     }
 
@@ -360,6 +453,11 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         r.stride = part_count;
         r.offset = part_index;
         r.nj = (n - part_index + part_count - 1) / part_count;
+        if (line_range) {
+            r.offset = range_lo;
+            r.nj = range_hi - range_lo;
+            if (r.nj <= 0) continue;
+        }
         r.piece_base = npieces;
         r.npieces = (paired ? 1 : 2) * (((int64_t)r.nj + chunk - 1) / chunk);
         npieces += r.npieces;
@@ -369,14 +467,14 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     const int64_t qcap = std::max<int64_t>(p.queue_capacity, max_n);
     const int64_t ntiles = (L + TILE - 1) / TILE;
 
-    // pool sizing: the last run's exact need (plus the traversals' unused
-    // chunk ends), else a share of the budget
-    const int64_t pool_slack = (int64_t)grid * NS * POOL_CHUNK;
-    // entries plus what chunked allocation may leave unused: under 1/7 of the
-    // entries at refills and one chunk per traversal at the end
-    auto pool_need = [&](int64_t entries) { return std::max<int64_t>(entries, 1) * 8 / 7 + 1 + pool_slack; };
+    // pool sizing: the last run's exact need (every chain takes an exact
+    // range, so the pool holds the lists with no gaps), else a share of the
+    // budget; the ranges form writes into the caller's pool
+    auto pool_need = [&](int64_t entries) { return std::max<int64_t>(entries, 1); };
     int64_t pool_cap = 0;
-    if (want_pattern) {
+    if (pattern_form == 2) {
+        pool_cap = ext->cap;
+    } else if (want_pattern) {
         if (p.pool_capacity > 0) {
             pool_cap = p.pool_capacity;
         } else {
@@ -419,11 +517,15 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         // a 16-bit chain index per vertex for every traversal: its lists are
         // read off the bitmap when the chain ends
         const int64_t stamp_stride = (int64_t)bitmap_words * 32;
-        if (want_pattern) {
+        if (pattern_form == 1) {
             d_pool = (int32_t *)ctx->grow(ctx->pool, (size_t)pool_cap * sizeof(int32_t));
             d_out = (int32_t *)ctx->grow(ctx->out, (size_t)pool_cap * sizeof(int32_t));
-            d_stamp = (uint16_t *)ctx->grow(ctx->stamp, (size_t)grid * NS * stamp_stride * sizeof(uint16_t));
+        } else if (pattern_form == 2) {
+            d_pool = ext->dev;
         }
+        if (want_pattern)
+            d_stamp = (uint16_t *)ctx->grow(ctx->stamp, (size_t)grid * NS * stamp_stride * sizeof(uint16_t));
+        uint32_t *d_gstate = gbm ? (uint32_t *)ctx->grow(ctx->gstate, (size_t)grid * NS * state_words * 4) : nullptr;
         MatDesc *d_mats = (MatDesc *)ctx->grow(ctx->mats, md.size() * sizeof(MatDesc));
         int64_t *d_minfo = (int64_t *)ctx->grow(ctx->matinfo, (size_t)3 * count * sizeof(int64_t));
         Range *d_ranges = (Range *)ctx->grow(ctx->ranges, std::max<size_t>(ranges.size(), 1) * sizeof(Range));
@@ -443,7 +545,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         a.ring_size = ring;
         a.lanes = lanes;
         a.reuse = reuse;
-        a.want_pattern = want_pattern ? 1 : 0;
+        a.want_pattern = pattern_form;
         a.max_sn = p.max_supernode_size;
         a.L = L;
         a.cnt = d_cnt;
@@ -466,22 +568,30 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         a.status = d_status;
         a.stamp = d_stamp;
         a.stamp_stride = stamp_stride;
+        a.gbm = d_gstate;
 
         // The job: descriptor copies, clears and the cooperative launch.  With
         // GSOFA_FLAG_GRAPH it is captured once into a CUDA graph and replayed
         // while the same job (matrices, parameters, buffers) comes back.
         const MatDesc *md_src = md.data();
         const Range *rg_src = ranges.data();
-        auto issue = [&](void *const *kargs) {
+        // The shared-memory attribute is set under the lock right before each
+        // launch (and graph launch); inside a capture it was set beforehand.
+        auto issue = [&](void *const *kargs, bool capturing) {
             GS_CUDA(cudaMemcpyAsync(d_mats, md_src, md.size() * sizeof(MatDesc), cudaMemcpyHostToDevice, st));
             if (!ranges.empty())
                 GS_CUDA(cudaMemcpyAsync(d_ranges, rg_src, ranges.size() * sizeof(Range),
                                         cudaMemcpyHostToDevice, st));
             GS_CUDA(cudaMemsetAsync(d_misc, 0, 256, st));
             GS_CUDA(cudaMemsetAsync(d_lrow, 0, (size_t)L * sizeof(int32_t), st));
-            if (part_count > 1) {
+            if (subset) {
                 GS_CUDA(cudaMemsetAsync(d_cnt, 0, (size_t)2 * L * sizeof(int32_t), st));
                 GS_CUDA(cudaMemsetAsync(d_nxt, 0, (size_t)2 * L, st));
+            }
+            std::unique_lock<std::mutex> lk(kernel_attr_mutex(), std::defer_lock);
+            if (!capturing) {
+                lk.lock();
+                GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             }
             GS_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(block), (void **)kargs, smem, st));
         };
@@ -509,10 +619,14 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
                 gc.args = a;
                 void *gargs[] = {&gc.args};
                 cudaGraph_t graph = nullptr;
+                {
+                    std::lock_guard<std::mutex> lk(kernel_attr_mutex());
+                    GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                }
                 bool ok = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
                 if (ok) {
                     try {
-                        issue(gargs);
+                        issue(gargs, true);
                     } catch (CudaFail &) {
                         ok = false;
                     }
@@ -530,8 +644,13 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         }
         const double t_launch = now_ms();
         GS_CUDA(cudaEventRecord(ctx->ev0, st));
-        if (graphed) GS_CUDA(cudaGraphLaunch(ctx->graph.exec, st));
-        else issue(args);
+        if (graphed) {
+            std::lock_guard<std::mutex> lk(kernel_attr_mutex());
+            GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            GS_CUDA(cudaGraphLaunch(ctx->graph.exec, st));
+        } else {
+            issue(args, false);
+        }
         GS_CUDA(cudaEventRecord(ctx->ev1, st));
 
         unsigned long long h_misc[25];
@@ -553,10 +672,12 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         // a property of the input
         if (status & ERR_COUNT_MISMATCH) return GSOFA_ERR_CUDA;
         if (want_pattern && (status & ERR_POOL_OVERFLOW)) {
-            if (attempt == 0) {
+            if (attempt == 0 && pattern_form == 1) {
                 pool_cap = pool_need(tot[0] + tot[1]);
                 continue;   // rerun with the pool the counts ask for
             }
+            // the caller's pool is too small: report what the job needs
+            for (int i = 0; i < count; i++) out[i].pool_used = (int64_t)h_misc[1];
             return GSOFA_ERR_QUEUE_OVERFLOW;
         }
 
@@ -598,7 +719,8 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
             r.reused_sources = reused;
             for (int q = 0; q < 7; q++) r.cycles[q] = h_misc[9 + q];
             r.ctas = (uint64_t)grid;
-            if (part_count == 1) {
+            r.pool_used = want_pattern ? (int64_t)h_misc[1] : 0;
+            if (!subset) {
                 r.fill_count = r.nnz_u - mats[i]->orig_up + r.nnz_l - mats[i]->orig_lo;
                 const_cast<gsofa_matrix *>(mats[i])->last_pattern_total = (int64_t)(r.nnz_u + r.nnz_l);
             }
@@ -610,11 +732,14 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
                 // link flags: bit 0 from pass G, bit 1 from pass G^T (merged below)
                 r.line_flags = download(st, d_nxt, lb, n);
                 lflags.push_back(download(st, d_nxt, L + lb, n));
-                if (want_pattern) {
+                if (pattern_form == 1) {
                     r.u_ptr = download(st, d_gptr, lb, n + 1);
                     r.l_ptr = download(st, d_gptr, (L + 1) + lb, n + 1);
                     r.u_idx = download(st, d_out, s0[i], (int64_t)r.nnz_u);
                     r.l_idx = download(st, d_out, tot[0] + s1[i], (int64_t)r.nnz_l);
+                } else if (pattern_form == 2) {
+                    r.u_beg = download(st, d_poff, lb, n);
+                    r.l_beg = download(st, d_poff, L + lb, n);
                 }
             }
             // where the result sits on the device, for gsofa_result_fetch and
@@ -627,7 +752,8 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
             ri->u0 = s0[i];
             ri->l0 = tot[0] + s1[i];
             ri->sn0 = ss[i];
-            ri->pattern = want_pattern ? 1 : 0;
+            ri->pattern = pattern_form;
+            ri->pool = pattern_form == 2 ? d_pool : nullptr;
             r.internal = ri;
         }
         GS_CUDA(cudaStreamSynchronize(st));
@@ -638,19 +764,12 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
             std::free(lflags[i]);
             lflags[i] = nullptr;
             for (int32_t k = 0; k < r.n_supernodes; k++) r.sn_start[k] -= (int32_t)lb;
-            if (want_pattern) {
+            if (pattern_form == 1) {
                 const int64_t u0 = r.u_ptr[0], l0 = r.l_ptr[0];
                 for (int64_t q = 0; q <= n; q++) { r.u_ptr[q] -= u0; r.l_ptr[q] -= l0; }
             }
-            if (part_count > 1) {
-                // fills of the processed lines: subtract their original entries
-                std::vector<int32_t> ou((size_t)n), ol((size_t)n);
-                GS_CUDA(cudaMemcpy(ou.data(), mats[i]->d_orig_up, n * 4, cudaMemcpyDeviceToHost));
-                GS_CUDA(cudaMemcpy(ol.data(), mats[i]->d_orig_lo, n * 4, cudaMemcpyDeviceToHost));
-                uint64_t o = 0;
-                for (int64_t q = part_index; q < n; q += part_count) o += (uint64_t)ou[q] + (uint64_t)ol[q];
-                r.fill_count = r.nnz_u + r.nnz_l - o;
-            }
+            // fills of the processed lines: subtract their original entries
+            if (subset) r.fill_count = r.nnz_u + r.nnz_l - processed_orig(i);
         }
         if (host_timing)
             std::fprintf(stderr,
@@ -658,18 +777,8 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
                          "mean CTA %.3f), results %.3f ms\n",
                          t_launch - t_enter, t_done - t_launch, ms, h_misc[16] * 1e-6,
                          h_misc[17] * 1e-6 / std::max(grid, 1), now_ms() - t_done);
-        if (part_count > 1 && !download_lines) {
-            for (int i = 0; i < count; i++) {
-                gsofa_result &r = out[i];
-                const int64_t n = md[i].n;
-                std::vector<int32_t> ou((size_t)n), ol((size_t)n);
-                GS_CUDA(cudaMemcpy(ou.data(), mats[i]->d_orig_up, n * 4, cudaMemcpyDeviceToHost));
-                GS_CUDA(cudaMemcpy(ol.data(), mats[i]->d_orig_lo, n * 4, cudaMemcpyDeviceToHost));
-                uint64_t o = 0;
-                for (int64_t q = part_index; q < n; q += part_count) o += (uint64_t)ou[q] + (uint64_t)ol[q];
-                r.fill_count = r.nnz_u + r.nnz_l - o;
-            }
-        }
+        if (subset && !download_lines)
+            for (int i = 0; i < count; i++) out[i].fill_count = out[i].nnz_u + out[i].nnz_l - processed_orig(i);
         return GSOFA_OK;
     }
     return GSOFA_ERR_QUEUE_OVERFLOW;
@@ -769,7 +878,7 @@ void gsofa_destroy(gsofa_ctx *c)
     DevBuf *bufs[] = {&c->queue, &c->cnt, &c->nxt, &c->poff, &c->gptr, &c->lrow, &c->snind,
                       &c->snlist, &c->tiles, &c->misc, &c->pool, &c->out, &c->mats, &c->ranges,
                       &c->st_beg, &c->st_end, &c->st_adj, &c->st_tmp, &c->matinfo, &c->stamp,
-                      &c->sn_head, &c->sn_data};
+                      &c->sn_head, &c->sn_data, &c->gstate};
     for (DevBuf *b : bufs) c->release(*b);
     for (DevBuf &b : c->slabs) cudaFree(b.p);
     c->slabs.clear();
@@ -1071,11 +1180,12 @@ gsofa_status gsofa_result_fetch(gsofa_ctx *c, const gsofa_result *r, int32_t *u_
         auto cp = [&](void *dst, const void *src, size_t bytes) {
             if (dst && bytes) GS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
         };
+        if (l_row_count && !ri->pattern) return GSOFA_ERR_INVALID_INPUT;   // counted with the pattern only
+        if ((u_ptr || u_idx || l_ptr || l_idx) && (ri->pattern != 1 || !outb))
+            return GSOFA_ERR_INVALID_INPUT;   // the CSR form only
         cp(u_row_count, cnt + lb, (size_t)n * 4);
         cp(l_col_count, cnt + L + lb, (size_t)n * 4);
-        if (l_row_count && !outb) return GSOFA_ERR_INVALID_INPUT;   // counted with the pattern only
         cp(l_row_count, (const int32_t *)c->lrow.p + lb, (size_t)n * 4);
-        if ((u_ptr || u_idx || l_ptr || l_idx) && !outb) return GSOFA_ERR_INVALID_INPUT;
         cp(u_ptr, gptr + lb, (size_t)(n + 1) * 8);
         cp(l_ptr, gptr + (L + 1) + lb, (size_t)(n + 1) * 8);
         cp(u_idx, outb + ri->u0, (size_t)r->nnz_u * 4);
@@ -1094,6 +1204,113 @@ gsofa_status gsofa_result_fetch(gsofa_ctx *c, const gsofa_result *r, int32_t *u_
         }
     } catch (CudaFail &f) {
         return fail_cuda(f.e);
+    }
+    return GSOFA_OK;
+}
+
+gsofa_status gsofa_result_fetch_ranges(gsofa_ctx *c, const gsofa_result *r, int64_t *u_beg,
+                                       int64_t *l_beg)
+{
+    if (!c || !r || !r->internal) return GSOFA_ERR_INVALID_INPUT;
+    const ResultInternal *ri = (const ResultInternal *)r->internal;
+    if (ri->job_id != c->job_id || ri->pattern != 2) return GSOFA_ERR_INVALID_INPUT;
+    try {
+        GS_CUDA(cudaSetDevice(c->device));
+        cudaStream_t st = c->stream;
+        const int64_t *poff = (const int64_t *)c->poff.p;
+        if (u_beg && ri->n)
+            GS_CUDA(cudaMemcpyAsync(u_beg, poff + ri->line_base, (size_t)ri->n * 8, cudaMemcpyDeviceToHost, st));
+        if (l_beg && ri->n)
+            GS_CUDA(cudaMemcpyAsync(l_beg, poff + ri->L + ri->line_base, (size_t)ri->n * 8,
+                                    cudaMemcpyDeviceToHost, st));
+        GS_CUDA(cudaStreamSynchronize(st));
+    } catch (CudaFail &f) {
+        return fail_cuda(f.e);
+    }
+    return GSOFA_OK;
+}
+
+gsofa_status gsofa_symbfact_ranges(gsofa_ctx *c, int count, const gsofa_matrix *const *mats,
+                                   const gsofa_params *params, int32_t *pool, int64_t pool_capacity,
+                                   gsofa_result *out)
+{
+    if (!c || !pool || pool_capacity <= 0 || count <= 0 || !out) return GSOFA_ERR_INVALID_INPUT;
+    gsofa_params p;
+    resolve_params(params, &p);
+    if (p.part_count > 1) return GSOFA_ERR_INVALID_INPUT;
+    p.want_pattern = 2;
+    try {
+        GS_CUDA(cudaSetDevice(c->device));
+        // the pool: device memory of this device, or page-locked host memory
+        // (written through its device alias while the traversals run)
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, pool) != cudaSuccess) {
+            cudaGetLastError();
+            return GSOFA_ERR_INVALID_INPUT;
+        }
+        ExtPool ext;
+        ext.cap = pool_capacity;
+        if (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) {
+            if (at.type == cudaMemoryTypeDevice && at.device != c->device) return GSOFA_ERR_INVALID_INPUT;
+            ext.dev = pool;
+        } else if (at.type == cudaMemoryTypeHost) {
+            void *d = nullptr;
+            if (cudaHostGetDevicePointer(&d, pool, 0) != cudaSuccess) {
+                cudaGetLastError();
+                return GSOFA_ERR_INVALID_INPUT;
+            }
+            ext.dev = (int32_t *)d;
+        } else {
+            return GSOFA_ERR_INVALID_INPUT;   // pageable host memory
+        }
+        gsofa_status s = run_job(c, count, mats, &p, out, &ext);
+        if (s != GSOFA_OK)
+            for (int i = 0; i < count; i++) free_result_arrays(&out[i]);
+        return s;
+    } catch (CudaFail &f) {
+        for (int i = 0; i < count; i++) free_result_arrays(&out[i]);
+        return fail_cuda(f.e);
+    } catch (std::bad_alloc &) {
+        for (int i = 0; i < count; i++) free_result_arrays(&out[i]);
+        return GSOFA_ERR_OOM;
+    }
+}
+
+static bool valid_lines(int32_t n, int64_t nnz, const int32_t *beg, const int32_t *end, const int32_t *adj)
+{
+    if (n < 0 || nnz < 0 || (n > 0 && (!beg || !end)) || (nnz > 0 && !adj)) return false;
+    for (int32_t v = 0; v < n; v++)
+        if (beg[v] < 0 || end[v] < beg[v] || (int64_t)end[v] > nnz) return false;
+    for (int32_t v = 0; v < n; v++)
+        for (int32_t k = beg[v]; k < end[v]; k++)
+            if (adj[k] < 0 || adj[k] >= n) return false;
+    return true;
+}
+
+gsofa_status gsofa_predict_line_counts(int32_t n, int64_t nnz, const int32_t *beg, const int32_t *end,
+                                       const int32_t *adj, int64_t *counts)
+{
+    if (!counts || !valid_lines(n, nnz, beg, end, adj)) return GSOFA_ERR_INVALID_INPUT;
+    try {
+        const gsofa::part::Sym sy = gsofa::part::symmetric_structure(n, beg, end, adj);
+        const std::vector<int32_t> parent = gsofa::part::etree(n, sy);
+        const std::vector<int32_t> post = gsofa::part::postorder(n, parent);
+        const std::vector<int64_t> cc = gsofa::part::column_counts(n, sy, parent, post);
+        for (int32_t v = 0; v < n; v++) counts[v] = cc[(size_t)v] - 1;
+    } catch (std::bad_alloc &) {
+        return GSOFA_ERR_OOM;
+    }
+    return GSOFA_OK;
+}
+
+gsofa_status gsofa_partition_lines(int32_t n, int64_t nnz, const int32_t *beg, const int32_t *end,
+                                   const int32_t *adj, int32_t parts, int32_t *cuts, double *work)
+{
+    if (parts <= 0 || !cuts || !valid_lines(n, nnz, beg, end, adj)) return GSOFA_ERR_INVALID_INPUT;
+    try {
+        gsofa::part::partition(n, beg, end, adj, parts, cuts, work);
+    } catch (std::bad_alloc &) {
+        return GSOFA_ERR_OOM;
     }
     return GSOFA_OK;
 }
@@ -1170,9 +1387,11 @@ SupernodalArgs supernodal_args(gsofa_ctx *c, const gsofa_result *r, const Result
     a.lcnt = (const int32_t *)c->cnt.p + L + lb;
     a.uptr = (const int64_t *)c->gptr.p + lb;
     a.lptr = (const int64_t *)c->gptr.p + (L + 1) + lb;
-    a.out = (const int32_t *)c->out.p;
+    a.out = ri->pattern == 2 ? ri->pool : (const int32_t *)c->out.p;
     a.u0 = ri->u0;
     a.l0 = ri->l0;
+    a.ubeg = ri->pattern == 2 ? (const int64_t *)c->poff.p + lb : nullptr;
+    a.lbeg = ri->pattern == 2 ? (const int64_t *)c->poff.p + L + lb : nullptr;
     a.lsize = (int64_t *)head;
     a.usize = a.lsize + ns;
     a.xlsub = a.usize + ns;
@@ -1185,7 +1404,8 @@ const ResultInternal *supernodal_source(gsofa_ctx *c, const gsofa_result *r)
 {
     if (!c || !r) return nullptr;
     const ResultInternal *ri = (const ResultInternal *)r->internal;
-    if (!ri || ri->job_id != c->job_id || !ri->pattern || !c->out.p) return nullptr;
+    if (!ri || ri->job_id != c->job_id || !ri->pattern) return nullptr;
+    if (ri->pattern == 1 ? !c->out.p : !ri->pool) return nullptr;
     const int64_t n = ri->n, ns = r->n_supernodes;
     if (ns < 0 || ns > n || (n > 0 && ns == 0)) return nullptr;
     return ri;
@@ -1328,9 +1548,12 @@ gsofa_status gsofa_symbfact_min_id(int argc, char **argv, int myrank, uint64_t *
     gsofa_status s = gsofa_read_text(argv[1], argv[2], argv[3], &n, &nnz, &beg, &end, &adj);
     if (s != GSOFA_OK) return s;
     gsofa_ctx *c = nullptr;
-    // the reference's budget counts the traversal state only; ours adds the
-    // queues, so it is a floor rather than a cap
-    s = gsofa_create(&c, myrank % gpus_per_node, 0);
+    // argv[5] is the device memory pool in GB, as in the reference
+    // (with_space_optimization/symbfact.cuh:1683-1686): here the context's
+    // budget, which bounds the concurrent traversals (frontier queues) the
+    // launch keeps; 0 or absent: 90% of the free memory
+    const size_t budget = mem_gb > 0 ? (size_t)(mem_gb * 1073741824.0) : 0;
+    s = gsofa_create(&c, myrank % gpus_per_node, budget);
     gsofa_matrix *m = nullptr;
     if (s == GSOFA_OK) s = gsofa_upload(c, n, nnz, beg, end, adj, &m);
     std::free(beg);
@@ -1382,9 +1605,24 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[GSOFA_NOALLOC_S
 
 constexpr int kNoallocMaxDevices = 64;
 std::mutex g_noalloc_mu;
-void *g_noalloc_base[kNoallocMaxDevices];
-int g_noalloc_sms[kNoallocMaxDevices];
-size_t g_noalloc_smem[kNoallocMaxDevices];
+int g_noalloc_sms[kNoallocMaxDevices];     // 0: device not checked yet
+
+// Makes `device` current for the lifetime of the guard and puts the
+// caller's current device back on every return path.
+struct DeviceGuard {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceGuard(int device)
+    {
+        err = cudaGetDevice(&prev);
+        if (err == cudaSuccess && prev != device) err = cudaSetDevice(device);
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
 
 // Carves the static array for an n-line, nnz-entry input: sequential,
 // 256-byte aligned slices.
@@ -1422,23 +1660,26 @@ extern "C" gsofa_status gsofa_symbfact_counts_noalloc(int device, void *cuda_str
     if (device < 0 || device >= kNoallocMaxDevices) return GSOFA_ERR_INVALID_INPUT;
     summary[0] = summary[1] = summary[2] = 0;
     if (n == 0) return GSOFA_OK;
+    DeviceGuard dg(device);   // the caller's current device comes back on return
+    if (dg.err != cudaSuccess) return fail_cuda(dg.err);
     try {
-        GS_CUDA(cudaSetDevice(device));
+        int sms = 0;
         {
             std::lock_guard<std::mutex> lk(g_noalloc_mu);
-            if (!g_noalloc_base[device]) {
-                void *p = nullptr;
-                GS_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+            if (!g_noalloc_sms[device]) {
                 cudaDeviceProp prop;
                 GS_CUDA(cudaGetDeviceProperties(&prop, device));
                 if (prop.major < 10 || !prop.cooperativeLaunch) return GSOFA_ERR_UNSUPPORTED;
                 g_noalloc_sms[device] = prop.multiProcessorCount;
-                g_noalloc_smem[device] = prop.sharedMemPerBlockOptin;
-                g_noalloc_base[device] = p;
             }
+            sms = g_noalloc_sms[device];
         }
+        // The array's name is a host-side stand-in; its device address is
+        // looked up with this device current, on every call (a cheap lookup
+        // once the module is loaded, and never stale after a device reset).
+        void *scratch = nullptr;
+        GS_CUDA(cudaGetSymbolAddress(&scratch, g_noalloc_scratch));
         cudaStream_t st = (cudaStream_t)cuda_stream;
-        const int sms = g_noalloc_sms[device];
 
         // launch shape: 256 threads, one CTA per SM (its queue slice is n ints)
         constexpr int BLOCK = 256;
@@ -1447,9 +1688,12 @@ extern "C" gsofa_status gsofa_symbfact_counts_noalloc(int device, void *cuda_str
         const int32_t state_words = bitmap_words + bitmap_words / 32 + ((bitmap_words / 32 + 31) / 32 + 3) / 4 * 4;
         const int ring = 4096;
         const size_t smem = (size_t)state_words * 4 + (size_t)ring * 4;
-        GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int occ = 0;
-        GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, BLOCK, smem));
+        {
+            std::lock_guard<std::mutex> lk(kernel_attr_mutex());
+            GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, BLOCK, smem));
+        }
         if (occ <= 0) return GSOFA_ERR_UNSUPPORTED;
         const int grid = sms;
         const int64_t L = n;
@@ -1457,7 +1701,7 @@ extern "C" gsofa_status gsofa_symbfact_counts_noalloc(int device, void *cuda_str
         const int64_t scan_tiles = ((int64_t)n + 1 + 255) / 256 + 1;
 
         NoallocLayout lay;
-        lay.base = (char *)g_noalloc_base[device];
+        lay.base = (char *)scratch;
         lay.limit = GSOFA_NOALLOC_SCRATCH_BYTES;
         int32_t *gptr_g = lay.take<int32_t>(n + 1);
         int32_t *gadj = lay.take<int32_t>((size_t)nnz);
@@ -1577,7 +1821,13 @@ extern "C" gsofa_status gsofa_symbfact_counts_noalloc(int device, void *cuda_str
         a.counters = (unsigned long long *)(misc + 16);
         a.status = (uint32_t *)(misc + 192);
         void *args[] = {&a};
-        GS_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(BLOCK), args, smem, st));
+        {
+            // the shared-memory attribute is per kernel and process-wide: set
+            // it and launch under one lock so no other caller resizes it between
+            std::lock_guard<std::mutex> lk(kernel_attr_mutex());
+            GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            GS_CUDA(cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(BLOCK), args, smem, st));
+        }
         GS_CUDA(cudaMemcpyAsync(d_u_row_count, cnt, (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
         GS_CUDA(cudaMemcpyAsync(d_l_col_count, cnt + L, (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
         unsigned long long hm[25];
@@ -1586,7 +1836,10 @@ extern "C" gsofa_status gsofa_symbfact_counts_noalloc(int device, void *cuda_str
         GS_CUDA(cudaMemcpyAsync(&tot[0], gp + L, 8, cudaMemcpyDeviceToHost, st));
         GS_CUDA(cudaMemcpyAsync(&tot[1], gp + (L + 1) + L, 8, cudaMemcpyDeviceToHost, st));
         GS_CUDA(cudaStreamSynchronize(st));
-        if ((uint32_t)(hm[24] & 0xffffffffu) & ERR_QUEUE_OVERFLOW) return GSOFA_ERR_QUEUE_OVERFLOW;
+        const uint32_t kst = (uint32_t)(hm[24] & 0xffffffffu);
+        if (kst & ERR_QUEUE_OVERFLOW) return GSOFA_ERR_QUEUE_OVERFLOW;
+        // any other status bit is an internal fault: no result is returned
+        if (kst != 0u) return GSOFA_ERR_CUDA;
         summary[0] = (uint64_t)(tot[0] + tot[1]) - hc[0] - hc[1];
         summary[1] = (uint64_t)(tot[0] + tot[1] + n);
         summary[2] = hm[4];

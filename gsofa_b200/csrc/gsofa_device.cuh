@@ -106,6 +106,8 @@ struct JobArgs {
     uint32_t *status;
     uint16_t *stamp;           // pattern mode: per traversal, stamp_stride entries:
     int64_t stamp_stride;      // the chain index at which each vertex was first set
+    uint32_t *gbm;             // global-state kernels: per traversal, state_words
+                               // words (bitmap and its summaries) in global memory
 };
 
 constexpr int TILE = 2048;     // lines per tile in the post-traversal phases
@@ -208,12 +210,15 @@ __device__ __forceinline__ int bm_summary_words(const uint32_t *bm, const uint32
 // nonzero, so output scans can skip empty stretches 32 words at a time.
 // summ is followed by a second level (one bit per summary word, i.e. per
 // 32K vertices) at summ + summary_words; SUMM2_OFF gives that offset.
+// GBM: the bitmap lives in global memory (L2), where a read before the
+// atomic would cost as much as the atomic itself, so the atomic goes first.
+template <bool GBM>
 __device__ __forceinline__ bool test_and_set(uint32_t *bm, uint32_t *summ, int32_t m)
 {
     const uint32_t bit = 1u << (m & 31);
     const int wi = m >> 5;
     uint32_t *w = bm + wi;
-    if (*reinterpret_cast<volatile uint32_t *>(w) & bit) return false;
+    if (!GBM && (*reinterpret_cast<volatile uint32_t *>(w) & bit)) return false;
     const uint32_t old = atomicOr(w, bit);
     if (old == 0u) {
         const int si = wi >> 5;
@@ -221,6 +226,16 @@ __device__ __forceinline__ bool test_and_set(uint32_t *bm, uint32_t *summ, int32
         if (olds == 0u) atomicOr(summ + (bm_summary_words(bm, summ)) + (si >> 5), 1u << (si & 31));
     }
     return !(old & bit);
+}
+
+// Reads a word of a traversal's state: from shared memory, or (GBM) from
+// global memory through L2 only -- its words change by atomics in L2 and are
+// cleared by plain stores, so an L1 copy could be stale.
+template <bool GBM>
+__device__ __forceinline__ uint32_t bm_word(const uint32_t *p)
+{
+    if (GBM) return __ldcg(p);
+    return *p;
 }
 
 // Frontier queue of one source: absolute positions 0, 1, 2, ... in BFS order.
@@ -270,9 +285,6 @@ struct SharedState {
     int chain_lo;     // lowest vertex set in the bitmap since the last clear
     int chain_hi;     // highest vertex set since the last clear
     int seg[2];       // piece boundaries after chain alignment
-    int64_t pool_base;
-    int64_t pool_cur;  // this traversal's private slice of the pattern pool:
-    int64_t pool_end;  // [pool_cur, pool_end), refilled POOL_CHUNK entries at a time
     int64_t warp[32];
     // tallies kept by the half's first thread only: levels, then cycles of
     // seeding, level loop, range fold, count and link flag, list output (per
@@ -298,10 +310,6 @@ __device__ __forceinline__ void stamp_set(const SharedState &sh, int32_t v)
     if (st != nullptr && v > sh.chain_s0) st[v] = (uint16_t)sh.chain_idx;
 }
 
-// Pattern pool entries a traversal takes from the shared pool at a time (one
-// global atomic per chunk instead of one per source).
-constexpr int64_t POOL_CHUNK = 1 << 16;
-
 // Clears the bitmap words covering vertices [lo, hi]; gtid/GT: the calling
 // thread's index and the size of the thread group that shares the bitmap.
 template <int GT>
@@ -317,13 +325,13 @@ __device__ __forceinline__ void clear_range(uint32_t *bm, uint32_t *summ, int lo
 // Visits the nonzero chunks c in [c0, c1) (chunk = 32 bitmap words = one
 // summary word) in increasing order, using the second summary level to skip
 // empty stretches; fn(c) runs warp-uniformly.
-template <class F>
+template <bool GBM, class F>
 __device__ __forceinline__ void for_nonzero_chunks(const uint32_t *summ2, int c0, int c1, F fn)
 {
     int c = c0;
     while (c < c1) {
         const int wb = c & ~31;
-        uint32_t m = summ2[wb >> 5] & (~0u << (c & 31));
+        uint32_t m = bm_word<GBM>(summ2 + (wb >> 5)) & (~0u << (c & 31));
         if (c1 - wb < 32) m &= (1u << (c1 - wb)) - 1u;
         while (m) {
             const int b = __ffs(m) - 1;
@@ -373,7 +381,7 @@ __device__ __forceinline__ int32_t chain_start(const PassGraph &g, int32_t x, in
 #define GSOFA_VISIT(m)                                                          \
     do {                                                                        \
         const int32_t _m = (m);                                                 \
-        if (test_and_set(bm, summ, _m)) {                                             \
+        if (test_and_set<GBM>(bm, summ, _m)) {                                        \
             t_lo = min(t_lo, _m);                                               \
             t_hi = max(t_hi, _m);                                               \
             stamp_set(sh, _m);                                                  \
@@ -390,7 +398,7 @@ __device__ __forceinline__ int32_t chain_start(const PassGraph &g, int32_t x, in
 // X(s) and hi(s-1) minus {s} is inside hi(s).
 // END_SYNC: finish with a barrier of the traversal's threads (not needed when
 // the caller's next step is a barrier of the whole CTA).
-template <int GT, bool CG, bool END_SYNC>
+template <int GT, bool CG, bool END_SYNC, bool GBM>
 __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                                int64_t line, int pass, int32_t s, uint32_t *bm, uint32_t *summ,
                                const Frontier &f, SharedState &sh,
@@ -411,7 +419,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         sh.fetch[0] = sh.fetch[1] = sh.fetch[2] = 0;
         sh.chain_idx = sh.chain_len;
         sh.chain_len = sh.chain_idx + 1;
-        if (test_and_set(bm, summ, s)) { t_lo = s; t_hi = s; stamp_set(sh, s); }
+        if (test_and_set<GBM>(bm, summ, s)) { t_lo = s; t_hi = s; stamp_set(sh, s); }
         else sh.hcount--;   // s was in hi(s-1): counted, but not above s
     }
     gsync<GT>(bar);
@@ -476,7 +484,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                     for (int32_t k0 = 0; k0 < hd; k0 += 32) {
                         const bool on = k0 + lane < hd;
                         const int32_t m = on ? ld<CG>(g.adj + hb + k0 + lane) : 0;
-                        const bool fresh = on && test_and_set(bm, summ, m);
+                        const bool fresh = on && test_and_set<GBM>(bm, summ, m);
                         if (fresh) { t_lo = min(t_lo, m); t_hi = max(t_hi, m); stamp_set(sh, m); }
                         const bool low = fresh && m < s;
                         const unsigned bal = __ballot_sync(0xffffffffu, low);
@@ -501,7 +509,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                     unsigned fresh = 0u;
 #pragma unroll
                     for (int u = 0; u < 8; u++)
-                        if (buf[u] >= 0 && test_and_set(bm, summ, buf[u])) fresh |= 1u << u;
+                        if (buf[u] >= 0 && test_and_set<GBM>(bm, summ, buf[u])) fresh |= 1u << u;
                     // new vertices below s in the low 16 bits, above s in
                     // the high ones (a warp step finds at most 256)
                     int nlh = 0;
@@ -586,7 +594,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         const int total = sh.hcount;
         const int64_t slot = (int64_t)pass * a.L + line;
         a.cnt[slot] = (int32_t)total;
-        const int nx = (s + 1 < n) && ((bm[(s + 1) >> 5] >> ((s + 1) & 31)) & 1u);
+        const int nx = (s + 1 < n) && ((bm_word<GBM>(bm + ((s + 1) >> 5)) >> ((s + 1) & 31)) & 1u);
         a.nxt[slot] = (uint8_t)nx;
         sh.flag = nx;
         sh.chain_total += total;
@@ -605,7 +613,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
 // lists on its own, in increasing order, with no barrier per source.  Lists
 // of pass G^T (columns of L) also count their entries into the L row
 // histogram (fire-and-forget reductions that overlap other traversals).
-template <int GT>
+template <int GT, bool GBM>
 __device__ void output_chain(const JobArgs &a, int64_t line_base, int pass, const uint32_t *bm,
                              const uint32_t *summ, SharedState &sh, int gtid, int bar)
 {
@@ -619,27 +627,15 @@ __device__ void output_chain(const JobArgs &a, int64_t line_base, int pass, cons
     if (wid == 0) {
         long long base = -1;
         if (lane == 0) {
-            // Ranges up to POOL_CHUNK / 8 come from this traversal's chunk (a
-            // refill abandons less than one such range, so under 1/7 of the
-            // entries are lost); longer ones take an exact range.
+            // one exact range per chain (one global atomic per chain of
+            // sources, so the pool holds the lists with no gaps); past the
+            // capacity the chain's lists are not written, the tail still
+            // advances, and its final value is the capacity the job needs
             const int64_t total = sh.chain_total;
-            if (total > POOL_CHUNK / 8) {
+            base = 0;
+            if (total > 0) {
                 const unsigned long long o = atomicAdd(a.pool_tail, (unsigned long long)total);
-                if ((int64_t)o + total <= a.pool_cap) base = (long long)o;
-            } else {
-                if (sh.pool_cur + total > sh.pool_end) {
-                    const unsigned long long o = atomicAdd(a.pool_tail, (unsigned long long)POOL_CHUNK);
-                    if ((int64_t)o + POOL_CHUNK > a.pool_cap) {
-                        sh.pool_cur = sh.pool_end = 0;
-                    } else {
-                        sh.pool_cur = (int64_t)o;
-                        sh.pool_end = (int64_t)o + POOL_CHUNK;
-                    }
-                }
-                if (sh.pool_cur + total <= sh.pool_end) {
-                    base = sh.pool_cur;
-                    sh.pool_cur += total;
-                }
+                base = ((int64_t)o + total <= a.pool_cap) ? (long long)o : -1;
             }
             if (base < 0) atomicOr(a.status, ERR_POOL_OVERFLOW);
         }
@@ -673,9 +669,9 @@ __device__ void output_chain(const JobArgs &a, int64_t line_base, int pass, cons
         const uint32_t first_mask = ~0u << ((s + 1) & 31);
         const bool last = (i == len - 1);   // every set bit was set by then
         int pos = 0;
-        for_nonzero_chunks(summ2, w0 >> 5, cend, [&](int cc) {
+        for_nonzero_chunks<GBM>(summ2, w0 >> 5, cend, [&](int cc) {
             const int w = (cc << 5) + lane;
-            uint32_t x = ((summ[cc] >> lane) & 1u) ? bm[w] : 0u;
+            uint32_t x = ((bm_word<GBM>(summ + cc) >> lane) & 1u) ? bm_word<GBM>(bm + w) : 0u;
             if (w < w0) x = 0u;
             if (w == w0) x &= first_mask;
             if (x != 0u && !last) {
@@ -751,7 +747,7 @@ struct Tally {
 
 // The sources s_lo, s_lo + stride, ... < s_hi of one work piece, in order,
 // each starting from the previous source's state whenever that is valid.
-template <int BLOCK, bool PAIRED, bool CG>
+template <int BLOCK, bool PAIRED, bool CG, bool GBM>
 __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &g, int pass,
                           int32_t s_lo, int32_t s_hi, int32_t stride, uint32_t *bm, uint32_t *summ,
                           const Frontier &fr, SharedState &sh, int (*pair_flag)[2], int half,
@@ -779,7 +775,7 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
         if (!reuse) {
             if (a.want_pattern && sh.chain_len > 0) {
                 const long long co = clock64();
-                output_chain<GT>(a, md.line_base, pass, bm, summ, sh, gtid, bar);
+                output_chain<GT, GBM>(a, md.line_base, pass, bm, summ, sh, gtid, bar);
                 if (gtid == 0) sh.prof[5] += (unsigned long long)(clock64() - co);
             }
             const long long cc = clock64();
@@ -795,7 +791,7 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
             sh.nreuse++;
         }
         // paired: the pass-flag exchange below is a barrier of the whole CTA
-        process_source<GT, CG, !PAIRED>(a, g, md.n, md.line_base + s, pass, s, bm, summ, fr, sh, acc.edges,
+        process_source<GT, CG, !PAIRED, GBM>(a, g, md.n, md.line_base + s, pass, s, bm, summ, fr, sh, acc.edges,
                            md.rawdeg, acc.xcnt, acc.einsp, sh.prof, gtid, bar);
         if (PAIRED) {
             if (gtid == 0) pair_flag[idx & 1][half] = sh.flag;
@@ -809,7 +805,7 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
     // the piece's last chain
     if (a.want_pattern && sh.chain_len > 0) {
         const long long co = clock64();
-        output_chain<GT>(a, md.line_base, pass, bm, summ, sh, gtid, bar);
+        output_chain<GT, GBM>(a, md.line_base, pass, bm, summ, sh, gtid, bar);
         if (gtid == 0) {
             sh.prof[5] += (unsigned long long)(clock64() - co);
             sh.chain_len = 0;
@@ -827,8 +823,15 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
 // exchange their s+1 flags after every source.  By the fill-path theorem,
 // s-1 is in X_G(s) exactly when s is in hi_{G^T}(s-1) (and likewise with G
 // and G^T swapped), so each half reuses s-1's state whenever it is valid.
-template <int BLOCK, bool PAIRED>
-__global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
+//
+// GBM = true: every traversal's visited bitmap and summaries live in global
+// memory (a.gbm, resident in L2 for the sizes that matter) instead of shared
+// memory, which then holds only the frontier rings.  A traversal's state no
+// longer bounds how many traversals an SM runs (shared memory holds two
+// bitmaps of at most ~850K lines each), so small CTAs run many traversals per
+// SM side by side, and n is bounded only by device memory.
+template <int BLOCK, bool PAIRED, bool GBM>
+__global__ void __launch_bounds__(BLOCK, (BLOCK >= 1024 ? 1 : 1024 / BLOCK)) factor_kernel(JobArgs a)
 {
     constexpr int GT = PAIRED ? BLOCK / 2 : BLOCK;
     constexpr int NS = PAIRED ? 2 : 1;
@@ -842,16 +845,17 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
     const int gtid = PAIRED ? tid % GT : tid;
     const int bar = PAIRED ? 1 + half : 0;
     SharedState &sh = shs[half];
-    uint32_t *bm = smem_dyn + (size_t)half * a.state_words;
+    uint32_t *const state = GBM ? a.gbm + ((int64_t)blockIdx.x * NS) * a.state_words : smem_dyn;
+    uint32_t *bm = state + (size_t)half * a.state_words;
     uint32_t *summ = bm + a.bitmap_words;
-    int32_t *ring = (int32_t *)(smem_dyn + (size_t)NS * a.state_words) + (size_t)half * a.ring_size;
+    int32_t *ring = (int32_t *)(GBM ? smem_dyn : smem_dyn + (size_t)NS * a.state_words) + (size_t)half * a.ring_size;
 
     // ---- phase 1: traversals ------------------------------------------------
     unsigned long long t_start = 0;
     if (tid == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_start));
-    for (int w = tid; w < NS * a.state_words; w += BLOCK) smem_dyn[w] = 0u;
+    for (int w = tid; w < NS * a.state_words; w += BLOCK) state[w] = 0u;
     if (gtid == 0) {
-        sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0; sh.pool_cur = sh.pool_end = 0;
+        sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0;
         sh.stamp = a.want_pattern ? a.stamp + ((int64_t)blockIdx.x * NS + half) * a.stamp_stride : nullptr;
         sh.chain_s0 = 0; sh.chain_len = 0; sh.chain_idx = 0; sh.chain_total = 0;
         for (int q = 0; q < 8; q++) sh.prof[q] = 0;
@@ -897,7 +901,7 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
             s_lo = sh.seg[0];
             s_hi = sh.seg[1];
         }
-        run_piece<BLOCK, PAIRED, false>(a, md, g, pass, s_lo, s_hi, rg.stride, bm, summ, fr, sh, pair_flag,
+        run_piece<BLOCK, PAIRED, false, GBM>(a, md, g, pass, s_lo, s_hi, rg.stride, bm, summ, fr, sh, pair_flag,
                                         half, gtid, bar, acc);
         // the next piece starts from an empty bitmap
         {
@@ -1076,7 +1080,9 @@ __global__ void __launch_bounds__(BLOCK) factor_kernel(JobArgs a)
             c += tot;
         }
     }
-    if (a.want_pattern && (*a.status & ERR_POOL_OVERFLOW) == 0) {
+    // CSR form only (want_pattern == 1); the ranges form (2) leaves the
+    // lists where the chains wrote them, at poff
+    if (a.want_pattern == 1 && (*a.status & ERR_POOL_OVERFLOW) == 0) {
         const int warps = (gridDim.x * BLOCK) >> 5;
         const int gw = (blockIdx.x * BLOCK + tid) >> 5;
         const int lane = tid & 31;

@@ -12,7 +12,7 @@
 //     columns.
 // Two passes: sizes per supernode (and supno), then, after the host turns the
 // sizes into offsets, one warp per supernode copies its index lists out of
-// the compacted pattern.
+// the pattern (CSR form, or the ranges form's pool and begins).
 #pragma once
 
 #include <stdint.h>
@@ -29,8 +29,11 @@ struct SupernodalArgs {
     const int32_t *lcnt;      // [n] |L col s|
     const int64_t *uptr;      // [n+1] U row offsets (job-wide, pass 0)
     const int64_t *lptr;      // [n+1] L column offsets (job-wide, pass 1)
-    const int32_t *out;       // compacted pattern of the job
+    const int32_t *out;       // compacted pattern of the job (CSR form), or the
+                              // pool of the ranges form
     int64_t u0, l0;           // where this matrix's U rows / L columns start in out
+    const int64_t *ubeg;      // ranges form: [n] where U row s / L column s start
+    const int64_t *lbeg;      //   in out (null: the CSR form)
     int64_t *lsize, *usize;   // [nsuper] per-supernode list sizes (first pass)
     const int64_t *xlsub;     // [nsuper+1] offsets (second pass)
     const int64_t *xusub;
@@ -67,12 +70,12 @@ __global__ void supernodal_fill_kernel(SupernodalArgs a)
         // rows: the diagonal block, then the last column's rows below it
         int32_t *ld = a.lsub + a.xlsub[k];
         for (int32_t i = lane; i < w; i += 32) ld[i] = fst + i;
-        const int32_t *lc = a.out + a.l0 + (a.lptr[lst - 1] - a.lptr[0]);
+        const int32_t *lc = a.lbeg ? a.out + a.lbeg[lst - 1] : a.out + a.l0 + (a.lptr[lst - 1] - a.lptr[0]);
         const int32_t nl = a.lcnt[lst - 1];
         for (int32_t i = lane; i < nl; i += 32) ld[w + i] = lc[i];
         // columns right of the block: U row fst past its first w-1 entries
         int32_t *ud = a.usub + a.xusub[k];
-        const int32_t *uc = a.out + a.u0 + (a.uptr[fst] - a.uptr[0]) + (w - 1);
+        const int32_t *uc = (a.ubeg ? a.out + a.ubeg[fst] : a.out + a.u0 + (a.uptr[fst] - a.uptr[0])) + (w - 1);
         const int64_t nu = a.xusub[k + 1] - a.xusub[k];
         for (int64_t i = lane; i < nu; i += 32) ud[i] = uc[i];
     }

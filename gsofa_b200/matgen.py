@@ -237,6 +237,35 @@ def powerlaw(n: int, alpha: float = 2.1, cap: int = 4000, local_frac: float = 0.
     return _csr_from_pairs(n, rows, cols, f"powerlaw_{n}_{ordering}")
 
 
+def bordered_blocks(n_blocks: int, block: int = 32, border: int = 8, per_line: int = 5,
+                    seed: int = 0) -> Graph:
+    """Bordered block-diagonal pattern, the shape nested dissection gives at
+    its top level: `n_blocks` diagonal blocks of `block` lines (each line with
+    `per_line` seeded entries inside its block), then `border` separator lines
+    numbered last.  Every block couples to one or two random border lines
+    (entries both ways) and the border lines to each other.  A traversal from
+    a block line stays inside its block (border lines are numbered above it),
+    so X(s) holds at most `block` lines and any n stays cheap for the oracle;
+    only the border lines traverse the whole matrix."""
+    rng = np.random.default_rng(seed)
+    nb = n_blocks * block
+    n = nb + border
+    rows = np.repeat(np.arange(nb, dtype=np.int64), per_line)
+    base = (rows // block) * block
+    cols = base + rng.integers(0, block, size=rows.shape[0])
+    # block -> border couplings (one or two per block, both directions)
+    k = rng.integers(1, 3, size=n_blocks)
+    blk = np.repeat(np.arange(n_blocks, dtype=np.int64), k)
+    line = blk * block + rng.integers(0, block, size=blk.shape[0])
+    sep = nb + rng.integers(0, border, size=blk.shape[0])
+    # border lines: a ring among themselves
+    b = np.arange(border, dtype=np.int64)
+    diag = np.arange(n, dtype=np.int64)
+    r = np.concatenate([rows, line, sep, nb + b, diag])
+    c = np.concatenate([cols, sep, line, nb + (b + 1) % border, diag])
+    return _csr_from_pairs(n, r, c, f"bordered_{n_blocks}x{block}+{border}")
+
+
 # ----------------------------------------------------------------------------
 # The named workloads
 

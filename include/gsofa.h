@@ -73,7 +73,9 @@ typedef struct gsofa_params {
     int64_t queue_capacity;     /* frontier entries per CTA (>= n, else n)    */
     int64_t pool_capacity;      /* pattern entries kept on the device         */
     int32_t max_supernode_size; /* 0 or negative: unbounded                   */
-    int32_t want_pattern;       /* 1: return u/l index arrays                 */
+    int32_t want_pattern;       /* 1: the pattern in CSR form (u/l index
+                                   arrays in line order); 2: the ranges form,
+                                   through gsofa_symbfact_ranges only          */
     int32_t reuse;              /* -1 (default) or 1: a source reuses the
                                    finished traversal of s-1 whenever s-1 is
                                    reachable from s; the two passes of a
@@ -88,6 +90,12 @@ typedef struct gsofa_params {
                                    reference's interleaved virtual-GPU
                                    partition, symbfact.cuh:1093); per-line
                                    outputs of other lines are zero            */
+    int32_t line_lo;            /* either nonzero: process only the source   */
+    int32_t line_hi;            /*   lines [line_lo, line_hi) of one matrix
+                                   (a contiguous partition, see
+                                   gsofa_partition_lines; [n, n) is empty);
+                                   reuse and the pattern stay available;
+                                   per-line outputs of other lines are zero   */
 } gsofa_params;
 
 #define GSOFA_FLAG_NO_DOWNLOAD 0x1 /* keep per-line arrays on the device only */
@@ -95,6 +103,14 @@ typedef struct gsofa_params {
 #define GSOFA_FLAG_GRAPH 0x4       /* capture the launch in a CUDA graph and
                                       replay it while the same job (matrices,
                                       parameters, buffers) repeats            */
+#define GSOFA_FLAG_GLOBAL_STATE 0x8 /* keep every traversal's visited bitmap
+                                      in global memory (L2): many small
+                                      traversals per SM, any n              */
+#define GSOFA_FLAG_SHARED_STATE 0x10 /* keep them in shared memory (at most
+                                      two per SM; GSOFA_ERR_UNSUPPORTED when
+                                      they do not fit).  Neither flag: shared
+                                      memory while two bitmaps fit, else
+                                      global memory                         */
 
 typedef struct gsofa_result {
     int32_t n;
@@ -134,6 +150,13 @@ typedef struct gsofa_result {
     int64_t *l_ptr;          /* [n+1] */
     int32_t *l_idx;          /* [nnz_l] */
     void *internal;
+    /* ranges form (gsofa_symbfact_ranges): begins into the caller's pool
+     * (host, library-owned; NULL with NO_DOWNLOAD, see
+     * gsofa_result_fetch_ranges) */
+    int64_t *u_beg;          /* [n] U row s = pool[u_beg[s] .. + u_row_count[s])  */
+    int64_t *l_beg;          /* [n] L col j = pool[l_beg[j] .. + l_col_count[j])  */
+    int64_t pool_used;       /* pool entries the job wrote; after
+                                GSOFA_ERR_QUEUE_OVERFLOW: the entries it needs */
 } gsofa_result;
 
 /* ---- reference-compatible entry ------------------------------------------
@@ -141,7 +164,10 @@ typedef struct gsofa_result {
  * with_space_optimization/symbfact.cuh:1553).  argv as the reference's CLI:
  *   argv[1] colbeg file, argv[2] colend file, argv[3] csr file,
  *   argv[4] N_GPU (source partitions, run back to back),
- *   optional argv[5] memory budget in GB, argv[6] max_supernode_size,
+ *   optional argv[5] device memory pool in GB (the context's budget: it bounds
+ *   the concurrent traversals, each holding an n-entry frontier queue, as the
+ *   reference's pool bounds its sources per pass; GSOFA_ERR_OOM when not even
+ *   one fits; 0: 90% of the free memory), argv[6] max_supernode_size,
  *   argv[7] GPUs per node.
  * The device is myrank % GPUs-per-node.  *fill_count receives the TOTAL over
  * all partitions; *time_ms the factorization time.  Returns a status. */
@@ -201,6 +227,33 @@ gsofa_status gsofa_symbfact_batch(gsofa_ctx *ctx, int count,
                                   gsofa_result *out);
 
 void gsofa_result_free(gsofa_result *r);
+
+/* The pattern in the reference's own begin/end layout (colbeg/colend into
+ * one id array, without_space_optimization/symbfact.cuh:1022-1071), written
+ * straight into caller memory: U row s is pool[u_beg[s] .. u_beg[s] +
+ * u_row_count[s]) and L column j is pool[l_beg[j] .. l_beg[j] +
+ * l_col_count[j]), each list sorted; lists sit in the order the traversals
+ * finished them, with no gaps (pool_used = nnz_u + nnz_l of all `count`
+ * matrices).  No compaction pass runs.
+ *
+ * `pool` is either device memory on ctx's device or page-locked host memory
+ * (cudaHostAlloc, cudaHostRegister): then the lists travel to the host while
+ * the traversals run, so the pattern needs no device memory of its own and
+ * may be larger than the device.  pool_capacity counts int32 entries.  When
+ * it is too small the call returns GSOFA_ERR_QUEUE_OVERFLOW with
+ * out[i].pool_used set to the entries the job needs.  The other result
+ * fields are as for gsofa_symbfact.  Results of a device pool can feed
+ * gsofa_result_supernodal while the pool stays allocated. */
+gsofa_status gsofa_symbfact_ranges(gsofa_ctx *ctx, int count,
+                                   const gsofa_matrix *const *mats,
+                                   const gsofa_params *params, int32_t *pool,
+                                   int64_t pool_capacity, gsofa_result *out);
+
+/* Copies the begins of a ranges-form result made with GSOFA_FLAG_NO_DOWNLOAD
+ * into caller buffers of n entries each (either may be NULL); valid until the
+ * next factorization on ctx. */
+gsofa_status gsofa_result_fetch_ranges(gsofa_ctx *ctx, const gsofa_result *r,
+                                       int64_t *u_beg, int64_t *l_beg);
 
 /* Copies the arrays of a result made with GSOFA_FLAG_NO_DOWNLOAD into
  * caller-owned host buffers (page-locked buffers give full PCIe speed).  Any
@@ -262,6 +315,29 @@ gsofa_status gsofa_result_supernodal_fetch(gsofa_ctx *ctx, const gsofa_result *r
 int32_t gsofa_supernodes_from_lines(int32_t n, const int32_t *u_row_count,
                                     const uint8_t *line_flags,
                                     int32_t max_supernode_size, int32_t *sn_start);
+
+/* Contiguous partition of the source lines into `parts` ranges of equal
+ * predicted work, for factorizing one matrix on several GPUs with
+ * gsofa_params.line_lo / line_hi (replaces the reference's interleaved
+ * partition, with_space_optimization/symbfact.cuh:1084-1099, which leaves no
+ * consecutive sources on one GPU and so no traversal reuse).  Work of line s:
+ * a fixed cost per traversal plus a cost per list entry, the list lengths
+ * predicted from the column counts of the Cholesky factor of A + A^T
+ * (elimination tree and skeleton counts, near-linear time); each cut moves to
+ * a nearby line that does not hold its predecessor.  Host-only.  cuts
+ * receives parts + 1 entries (cuts[0] = 0, cuts[parts] = n); work, when
+ * non-NULL, the predicted work of each part (SM cycles). */
+gsofa_status gsofa_partition_lines(int32_t n, int64_t nnz, const int32_t *beg,
+                                   const int32_t *end, const int32_t *adj,
+                                   int32_t parts, int32_t *cuts, double *work);
+
+/* Predicted list length of every line, the work model of
+ * gsofa_partition_lines: counts[s] = |column s of the Cholesky factor of
+ * A + A^T| minus the diagonal, an upper bound on both |U row s| and
+ * |L column s| (equal to them when the pattern is symmetric).  Host-only. */
+gsofa_status gsofa_predict_line_counts(int32_t n, int64_t nnz, const int32_t *beg,
+                                       const int32_t *end, const int32_t *adj,
+                                       int64_t *counts);
 
 /* Device scratch bytes a factorization of an n-line, nnz-entry matrix needs
  * with these parameters, excluding the pattern pool (admission control). */
@@ -329,13 +405,16 @@ gsofa_status gsofa_server_result(gsofa_server *srv, int64_t id, gsofa_result *ou
  *
  * Limits: n <= GSOFA_NOALLOC_MAX_N and the line ranges' total length
  * <= GSOFA_NOALLOC_MAX_NNZ; larger inputs return GSOFA_ERR_UNSUPPORTED before
- * any work is issued.  Counts only (no pattern): per-line U row counts,
+ * any work is issued.  The array also holds one n-entry frontier queue per SM,
+ * so the limits hold on GPUs with up to 200 SMs (the B200 has 148); on a
+ * larger GPU an input near both limits returns GSOFA_ERR_UNSUPPORTED too.  Counts only (no pattern): per-line U row counts,
  * L column counts, the supernode starts and a host summary
  * summary[0] = fill count, [1] = nnz(L+U), [2] = number of supernodes.
  *
- * The first call on a device looks up the static array's device address
- * (with that device current); make that first call before any stream
- * capture.  All calls on a device share the one array and it keeps the last
+ * Every call looks up the static array's device address with `device`
+ * current (the first call on a device also reads its properties); make the
+ * first call on a device before any stream capture.  The caller's current
+ * device is restored before the call returns.  All calls on a device share the one array and it keeps the last
  * call's contents (everything that must start at zero is cleared by the
  * call), so calls that overlap on the GPU race: issue them one at a time.
  * The call returns after its work on `cuda_stream` (NULL: the legacy default

@@ -51,11 +51,24 @@ def lib():
         L.gsofa_oracle_maxid_fills.argtypes = [ctypes.c_int32, _i32p, _i32p, _i32p, ctypes.c_int64,
                                                ctypes.c_int, _i64p, _i64p]
         L.gsofa_oracle_maxid_fills.restype = ctypes.c_int64
+        L.gsofa_oracle_threads.argtypes = []
+        L.gsofa_oracle_threads.restype = ctypes.c_int
+        L.gsofa_oracle_maxid_counts.argtypes = [ctypes.c_int32, _i32p, _i32p, _i32p, ctypes.c_int64,
+                                                ctypes.c_int, _i32p, ctypes.c_int32, _i64p, _i64p]
+        L.gsofa_oracle_maxid_counts.restype = ctypes.c_int64
+        L.gsofa_oracle_lists.argtypes = [ctypes.c_int32, _i32p, _i32p, _i32p, ctypes.c_int64,
+                                         ctypes.c_int, ctypes.c_int, _i32p, ctypes.c_int32, _i64p, _i32p]
+        L.gsofa_oracle_lists.restype = ctypes.c_int
         L.gsofa_oracle_maxid_line.argtypes = [ctypes.c_int32, _i32p, _i32p, _i32p, ctypes.c_int64,
                                               ctypes.c_int32, _i32p]
         L.gsofa_oracle_maxid_line.restype = ctypes.c_int32
         _lib = L
     return _lib
+
+
+def threads() -> int:
+    """Threads the OpenMP restatements use by default."""
+    return int(lib().gsofa_oracle_threads())
 
 
 def _p(a, t):
@@ -123,6 +136,38 @@ def maxid_fills(beg, end, adj, nthreads: int = 0):
     if tot < 0:
         raise ValueError("oracle max-id traversal failed")
     return int(tot), lo, hi
+
+
+def maxid_counts(beg, end, adj, sources, nthreads: int = 0):
+    """Faithful max-id traversal of the listed lines only: (total fills,
+    fills_lo[n], fills_hi[n]) with entries set at those lines."""
+    beg, end, adj = _inputs(beg, end, adj)
+    n = beg.shape[0]
+    src = np.ascontiguousarray(sources, dtype=np.int32)
+    lo = np.zeros(n, np.int64)
+    hi = np.zeros(n, np.int64)
+    tot = lib().gsofa_oracle_maxid_counts(n, _p(beg, _i32p), _p(end, _i32p), _p(adj, _i32p), adj.shape[0],
+                                          nthreads, _p(src, _i32p), src.shape[0], _p(lo, _i64p), _p(hi, _i64p))
+    if tot < 0:
+        raise ValueError("oracle max-id traversal failed")
+    return int(tot), lo, hi
+
+
+def lists(beg, end, adj, pass_: int, sources, cnt, nthreads: int = 0):
+    """Sorted hi(s) lists of one pass for the listed (distinct) sources, as
+    (ptr int64[k+1], idx int32[]) in the order given; cnt holds the per-line
+    counts of that pass (at least at the listed lines)."""
+    beg, end, adj = _inputs(beg, end, adj)
+    n = beg.shape[0]
+    src = np.ascontiguousarray(sources, dtype=np.int32)
+    ptr = np.zeros(src.shape[0] + 1, np.int64)
+    np.cumsum(np.asarray(cnt)[src], out=ptr[1:])
+    idx = np.zeros(int(ptr[-1]), np.int32)
+    rc = lib().gsofa_oracle_lists(n, _p(beg, _i32p), _p(end, _i32p), _p(adj, _i32p), adj.shape[0], pass_,
+                                  nthreads, _p(src, _i32p), src.shape[0], _p(ptr, _i64p), _p(idx, _i32p))
+    if rc != 0:
+        raise ValueError(f"oracle lists failed (rc={rc})")
+    return ptr, idx
 
 
 def maxid_line(beg, end, adj, s: int):

@@ -110,6 +110,8 @@ static int set_threads(int nthreads)
 #endif
 }
 
+int gsofa_oracle_threads(void) { return set_threads(0); }
+
 int gsofa_oracle_counts(int32_t n, const int32_t *beg, const int32_t *end,
                         const int32_t *adj, int64_t adj_len, int pass,
                         int nthreads, const int32_t *sources, int32_t n_sources,
@@ -138,7 +140,11 @@ int gsofa_oracle_counts(int32_t n, const int32_t *beg, const int32_t *end,
         int32_t *hi = (int32_t *)malloc((size_t)n * sizeof(int32_t));
         if (!stamp || !queue || !hi) failed = 1;
         else {
-#pragma omp for schedule(dynamic, 16)
+            /* One source per scheduling step, in the given order (by default
+             * the highest, heaviest lines first): the threads take the
+             * heavy lines one each instead of one thread taking a block of
+             * them (longest-first list scheduling). */
+#pragma omp for schedule(dynamic, 1)
             for (int32_t i = 0; i < ns; i++) {
                 int32_t s = sources ? sources[i] : (n - 1 - i); /* heavy lines first */
                 int32_t h, o; uint64_t x, e;
@@ -180,7 +186,7 @@ int gsofa_oracle_pattern(int32_t n, const int32_t *beg, const int32_t *end,
         int32_t *hi = (int32_t *)malloc((size_t)n * sizeof(int32_t));
         if (!stamp || !queue || !hi) failed = 1;
         else {
-#pragma omp for schedule(dynamic, 16)
+#pragma omp for schedule(dynamic, 1)
             for (int32_t i = 0; i < n; i++) {
                 int32_t s = n - 1 - i;
                 int32_t h, o; uint64_t x, e;
@@ -188,6 +194,48 @@ int gsofa_oracle_pattern(int32_t n, const int32_t *beg, const int32_t *end,
                 if (ptr[s + 1] - ptr[s] != h) { failed = 1; continue; }
                 qsort(hi, (size_t)h, sizeof(int32_t), cmp_i32);
                 memcpy(idx + ptr[s], hi, (size_t)h * sizeof(int32_t));
+            }
+        }
+        free(stamp); free(queue); free(hi);
+    }
+    free(tb); free(te); free(ta);
+    return failed ? 3 : 0;
+}
+
+int gsofa_oracle_lists(int32_t n, const int32_t *beg, const int32_t *end,
+                       const int32_t *adj, int64_t adj_len, int pass,
+                       int nthreads, const int32_t *sources, int32_t n_sources,
+                       const int64_t *ptr, int32_t *idx)
+{
+    if (validate(n, beg, end, adj, adj_len)) return 1;
+    if (pass != 0 && pass != 1) return 1;
+    if (n_sources < 0 || (n_sources > 0 && (!sources || !ptr || !idx))) return 1;
+    for (int32_t i = 0; i < n_sources; i++)
+        if (sources[i] < 0 || sources[i] >= n) return 1;
+    if (n == 0 || n_sources == 0) return 0;
+    const int32_t *B = beg, *E = end, *A = adj;
+    int32_t *tb = NULL, *te = NULL, *ta = NULL;
+    if (pass == 1) {
+        if (transpose(n, beg, end, adj, &tb, &te, &ta)) return 2;
+        B = tb; E = te; A = ta;
+    }
+    int failed = 0;
+    nthreads = set_threads(nthreads);
+#pragma omp parallel num_threads(nthreads) reduction(| : failed)
+    {
+        int32_t *stamp = (int32_t *)calloc((size_t)n, sizeof(int32_t));
+        int32_t *queue = (int32_t *)malloc((size_t)n * sizeof(int32_t));
+        int32_t *hi = (int32_t *)malloc((size_t)n * sizeof(int32_t));
+        if (!stamp || !queue || !hi) failed = 1;
+        else {
+#pragma omp for schedule(dynamic, 1)
+            for (int32_t i = 0; i < n_sources; i++) {
+                int32_t s = sources[i];
+                int32_t h, o; uint64_t x, e;
+                reach_one(s, B, E, A, stamp, queue, hi, &h, &o, &x, &e);
+                if (ptr[i + 1] - ptr[i] != h) { failed = 1; continue; }
+                qsort(hi, (size_t)h, sizeof(int32_t), cmp_i32);
+                memcpy(idx + ptr[i], hi, (size_t)h * sizeof(int32_t));
             }
         }
         free(stamp); free(queue); free(hi);
@@ -289,13 +337,17 @@ static int64_t maxid_one(int32_t s, const int32_t *beg, const int32_t *end,
     return (int64_t)nout;
 }
 
-int64_t gsofa_oracle_maxid_fills(int32_t n, const int32_t *beg,
-                                 const int32_t *end, const int32_t *adj,
-                                 int64_t adj_len, int nthreads,
-                                 int64_t *fills_lo, int64_t *fills_hi)
+int64_t gsofa_oracle_maxid_counts(int32_t n, const int32_t *beg,
+                                  const int32_t *end, const int32_t *adj,
+                                  int64_t adj_len, int nthreads,
+                                  const int32_t *sources, int32_t n_sources,
+                                  int64_t *fills_lo, int64_t *fills_hi)
 {
     if (validate(n, beg, end, adj, adj_len)) return -1;
     if (n == 0) return 0;
+    const int32_t ns = sources ? n_sources : n;
+    for (int32_t i = 0; sources && i < ns; i++)
+        if (sources[i] < 0 || sources[i] >= n) return -1;
     int64_t total = 0;
     int failed = 0;
     /* A vertex re-enters the FIFO on every improvement of its label, so the
@@ -310,9 +362,10 @@ int64_t gsofa_oracle_maxid_fills(int32_t n, const int32_t *beg,
         int32_t *queue = (int32_t *)malloc((size_t)qcap * sizeof(int32_t));
         if (!cost || !cstamp || !mark || !queue) failed = 1;
         else {
-#pragma omp for schedule(dynamic, 16)
-            for (int32_t i = 0; i < n; i++) {
-                int32_t s = n - 1 - i;
+            /* one source per scheduling step, heaviest (given) order first */
+#pragma omp for schedule(dynamic, 1)
+            for (int32_t i = 0; i < ns; i++) {
+                int32_t s = sources ? sources[i] : (n - 1 - i);
                 int64_t lo = 0, hi = 0;
                 if (maxid_one(s, beg, end, adj, cost, cstamp, mark, queue, qcap,
                               &lo, &hi, NULL) < 0) { failed = 1; continue; }
@@ -324,6 +377,15 @@ int64_t gsofa_oracle_maxid_fills(int32_t n, const int32_t *beg,
         free(cost); free(cstamp); free(mark); free(queue);
     }
     return failed ? -1 : total;
+}
+
+int64_t gsofa_oracle_maxid_fills(int32_t n, const int32_t *beg,
+                                 const int32_t *end, const int32_t *adj,
+                                 int64_t adj_len, int nthreads,
+                                 int64_t *fills_lo, int64_t *fills_hi)
+{
+    return gsofa_oracle_maxid_counts(n, beg, end, adj, adj_len, nthreads, NULL, 0,
+                                     fills_lo, fills_hi);
 }
 
 int32_t gsofa_oracle_maxid_line(int32_t n, const int32_t *beg,

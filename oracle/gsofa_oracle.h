@@ -41,6 +41,10 @@
 extern "C" {
 #endif
 
+/* Threads the OpenMP functions use when given nthreads <= 0 (the OpenMP
+ * default: OMP_NUM_THREADS, else the host's logical cores). */
+int gsofa_oracle_threads(void);
+
 /* Per-line outputs of one reachability pass over G (pass 0) or G^T (pass 1).
  * All arrays have n entries and are caller-allocated; any may be NULL.
  *   cnt[s]   = |hi(s)|               (entries > s in line s of that pass)
@@ -62,6 +66,16 @@ int gsofa_oracle_pattern(int32_t n, const int32_t *beg, const int32_t *end,
                          const int32_t *adj, int64_t adj_len, int pass,
                          int nthreads, const int64_t *ptr, int32_t *idx);
 
+/* The sorted hi(s) lists of one pass for the listed sources only (distinct
+ * ids; a repeated source fails with 3): list i goes to idx[ptr[i] ..
+ * ptr[i+1]), where ptr (n_sources + 1 entries) is the exclusive prefix sum
+ * of those sources' cnt values.  Lets a check cover sampled lines of a
+ * matrix whose whole pattern is too large to hold. */
+int gsofa_oracle_lists(int32_t n, const int32_t *beg, const int32_t *end,
+                       const int32_t *adj, int64_t adj_len, int pass,
+                       int nthreads, const int32_t *sources, int32_t n_sources,
+                       const int64_t *ptr, int32_t *idx);
+
 /* Supernode partition from the per-line upper counts and link flags.
  * Lines s-1 and s are in one supernode iff
  *   (i)   s-1 is in line s  (lnext[s-1] == 1: s is in hi_{G^T}(s-1)),
@@ -82,6 +96,15 @@ int64_t gsofa_oracle_maxid_fills(int32_t n, const int32_t *beg,
                                  const int32_t *end, const int32_t *adj,
                                  int64_t adj_len, int nthreads,
                                  int64_t *fills_lo, int64_t *fills_hi);
+
+/* The same for the listed sources only (NULL: all n, highest first): the
+ * reference's algorithm on a sample of its lines.  fills_lo / fills_hi are
+ * indexed by line and written only at the listed lines. */
+int64_t gsofa_oracle_maxid_counts(int32_t n, const int32_t *beg,
+                                  const int32_t *end, const int32_t *adj,
+                                  int64_t adj_len, int nthreads,
+                                  const int32_t *sources, int32_t n_sources,
+                                  int64_t *fills_lo, int64_t *fills_hi);
 
 /* The fill pattern (both halves, sorted) of the single line s, from the max-id
  * traversal; out must hold n entries.  Returns the number written or -1. */

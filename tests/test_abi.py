@@ -42,12 +42,30 @@ def test_abi_version_and_status_strings():
     assert p.want_pattern == 1 and p.part_count == 1 and p.reuse == -1
 
 
-def test_params_layout_matches_header():
-    # the ctypes mirror must have the C struct's size: 4*i32, 2*i64, 6*i32
-    assert ctypes.sizeof(gsofa_b200.Params) == 4 * 4 + 2 * 8 + 6 * 4
-    assert ctypes.sizeof(gsofa_b200._CResult) == 2 * 4 + 18 * 8 + 8 + 10 * 8
-    # gsofa_supernodal: 2*i32, 2*i64, 6 pointers
-    assert ctypes.sizeof(gsofa_b200._CSupernodal) == 2 * 4 + 2 * 8 + 6 * 8
+def test_params_layout_matches_header(tmp_path):
+    """The ctypes mirrors have the C structs' sizes and field offsets, as the
+    C compiler lays them out from include/gsofa.h."""
+    mirrors = {"gsofa_params": gsofa_b200.Params, "gsofa_result": gsofa_b200._CResult,
+               "gsofa_supernodal": gsofa_b200._CSupernodal, "gsofa_server_config": gsofa_b200.ServerConfig}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "gsofa.h"', "int main(void) {"]
+    for cname, mirror in mirrors.items():
+        lines.append(f'printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for f, _ in mirror._fields_:
+            lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)],
+                   check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        cname, field, val = line.split()
+        got[(cname, field)] = int(val)
+    for cname, mirror in mirrors.items():
+        assert ctypes.sizeof(mirror) == got[(cname, "sizeof")], cname
+        for f, _ in mirror._fields_:
+            assert getattr(mirror, f).offset == got[(cname, f)], f"{cname}.{f}"
 
 
 def test_read_text_matches_fixture(tmp_path):

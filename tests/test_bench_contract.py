@@ -28,6 +28,12 @@ def test_reference_arm_line():
     assert d["config"]["workload"] == "grid2d_64x64_5pt_natural"
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["kind"] == "port" and cb["cores"] >= 1 and cb["sample"]
+    # the sample keeps every thread busy, and the serial run and the max-id
+    # restatement of the reference's algorithm are reported beside it
+    assert cb["sample_sources"] >= min(d["config"]["n"], 8 * cb["cores"])
+    assert "omp_num_threads" in cb and cb["host_cores"] >= 1
+    assert cb["serial"]["value"] > 0 and cb["serial"]["cores"] == 1
+    assert cb["maxid"]["value"] > 0
     e = d["e2e"]
     assert e["value"] == d["value"] and e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
 

@@ -85,6 +85,29 @@ def test_parameters_do_not_change_results(ctx, block, lanes, reuse, chunk, per_s
     assert_same(r, ref, where=f"params {block},{lanes},{reuse},{chunk},{per_sm}")
 
 
+@pytest.mark.parametrize("block,lanes,reuse,chunk,per_sm", [
+    (256, 1, -1, 0, 0), (128, 1, -1, 5, 0), (512, 1, -1, 64, 1), (256, 8, 1, 7, 2),
+    (128, 1, 0, 1, 0), (256, 1, 2, 32, 0), (512, 32, 0, 3, 0), (128, 4, 2, 16, 3)])
+def test_global_state_kernel(ctx, block, lanes, reuse, chunk, per_sm):
+    """Visited bitmaps in global memory: the same results as the oracle, for
+    the paired (exact reuse), adjacency-reuse and no-reuse traversals."""
+    ref = None
+    for g in (matgen.grid3d(14, ordering="nd", drop_frac=0.1, seed=5), matgen.powerlaw(1200, seed=12),
+              random_graph(300, 0.03, 4)):
+        ref = _oracle(g, 8)
+        r = ctx.symbfact(ctx.upload(g), block_size=block, threads_per_source=lanes, reuse=reuse,
+                         src_chunk=chunk, ctas_per_sm=per_sm, max_supernode_size=8,
+                         flags=gsofa_b200.FLAG_GLOBAL_STATE)
+        assert_same(r, ref, where=f"global state {g.name} {block},{lanes},{reuse},{chunk},{per_sm}")
+
+
+def test_state_flags_conflict_is_an_error(ctx):
+    with pytest.raises(gsofa_b200.GsofaError) as e:
+        ctx.symbfact(ctx.upload(bundled()),
+                     flags=gsofa_b200.FLAG_GLOBAL_STATE | gsofa_b200.FLAG_SHARED_STATE)
+    assert e.value.status == 1
+
+
 def test_chain_longer_than_stamp_range(ctx):
     """A path in natural order lets every source reuse its predecessor's
     traversal, so one piece of 65,600 sources is one chain of reuse.  List
@@ -179,9 +202,15 @@ def test_reference_argv_entry(tmp_path):
     files = [str(tmp_path / f) for f in ("b.dat", "e.dat", "c.dat")]
     want = expected()["bundled_11948"]["fill_count"]
     for argv in (["gsofa", *files, "1"], ["gsofa", *files, "6", "1"],
-                 ["gsofa", *files, "264", "5", "128", "1"]):
+                 ["gsofa", *files, "264", "5", "128", "1"],
+                 # a 10 MB pool: fewer concurrent traversals, the same total
+                 ["gsofa", *files, "1", "0.01"], ["gsofa", *files, "6", "0.01", "0", "1"]):
         fills, ms = gsofa_b200.symbfact_min_id(argv)
         assert fills == want and ms > 0
+    # a pool too small for one traversal's state is an out-of-memory status
+    with pytest.raises(gsofa_b200.GsofaError) as e:
+        gsofa_b200.symbfact_min_id(["gsofa", *files, "1", "0.00001"])
+    assert e.value.status == 2
     # the same matrix in the binary form
     bins = [str(tmp_path / f) for f in ("b.bin", "e.bin", "c.bin")]
     gsofa_b200.write_binary(g, *bins)
@@ -275,6 +304,57 @@ def test_autotune_choice_is_cached_and_exact(ctx, tmp_path):
     assert rep2["cached"] and rep2["choice"] == rep["choice"]
     for g, r in zip(gs, ctx.symbfact_batch(ms, best2)):
         assert_same(r, _oracle(g), where=f"autotuned {g.name}")
+
+
+@pytest.mark.parametrize("make,parts", [(lambda: matgen.grid3d(16, ordering="nd", drop_frac=0.1, seed=3), 4),
+                                        (lambda: matgen.powerlaw(1500, seed=9), 3), (bundled, 5)])
+def test_line_range_partitions_keep_reuse_and_sum_to_the_whole(ctx, make, parts):
+    """Contiguous ranges from the work-predicted partitioner: every range
+    keeps traversal reuse, fills exactly its own lines (counts, link flags
+    and, with the pattern, its lists), and the ranges add up to the full
+    factorization."""
+    from gsofa_b200 import distributed, partition_lines
+    g = make()
+    ref = _oracle(g, 8)
+    m = ctx.upload(g)
+    cuts, work = partition_lines(g, parts)
+    assert cuts[0] == 0 and cuts[-1] == g.n and len(work) == parts
+    u = np.zeros(g.n, np.int64); lc = np.zeros(g.n, np.int64); fl = np.zeros(g.n, np.int64); fills = 0
+    for k in range(parts):
+        lo, hi = int(cuts[k]), int(cuts[k + 1])
+        r = ctx.symbfact(m, line_lo=lo, line_hi=hi, max_supernode_size=8)
+        if hi - lo > 2:
+            assert r.reused_sources > 0, (lo, hi)
+        inside = np.zeros(g.n, bool); inside[lo:hi] = True
+        assert np.all(r.u_row_count[~inside] == 0) and np.all(r.l_col_count[~inside] == 0)
+        assert np.array_equal(r.u_row_count[inside], ref["u_row_count"][inside])
+        for s_ in range(lo, hi):
+            assert np.array_equal(r.u_idx[r.u_ptr[s_]:r.u_ptr[s_ + 1]],
+                                  ref["u_idx"][ref["u_ptr"][s_]:ref["u_ptr"][s_ + 1]]), s_
+            assert np.array_equal(r.l_idx[r.l_ptr[s_]:r.l_ptr[s_ + 1]],
+                                  ref["l_idx"][ref["l_ptr"][s_]:ref["l_ptr"][s_ + 1]]), s_
+        u += r.u_row_count; lc += r.l_col_count; fl += r.line_flags; fills += r.fill_count
+    out = distributed.combine(g.n, u, lc, fl, fills, lambda x: x, max_supernode_size=8)
+    assert out["fill_count"] == ref["fill_count"] and out["nnz_lu"] == ref["nnz_lu"]
+    assert np.array_equal(out["sn_start"], ref["sn_start"])
+    # the same through symbfact_sharded, one range per "rank" on this GPU
+    tot = None
+    shares = []
+    for rank in range(parts):
+        p = distributed.rank_params(rank, parts, cuts, max_supernode_size=8)
+        r = ctx.symbfact(m, p)
+        shares.append(np.concatenate([r.u_row_count, r.l_col_count, r.line_flags, [r.fill_count]]).astype(np.int64))
+    tot = np.sum(shares, axis=0)
+    res = distributed.symbfact_sharded(ctx, m, 0, parts, lambda x: tot, max_supernode_size=8, cuts=cuts)
+    assert res["fill_count"] == ref["fill_count"] and np.array_equal(res["sn_start"], ref["sn_start"])
+
+
+def test_line_range_errors(ctx):
+    m = ctx.upload(bundled())
+    with pytest.raises(gsofa_b200.GsofaError):   # with an interleaved partition
+        ctx.symbfact(m, line_lo=0, line_hi=10, part_count=2, part_index=0)
+    with pytest.raises(gsofa_b200.GsofaError):   # on a batch
+        ctx.symbfact_batch([m, m], line_lo=0, line_hi=10)
 
 
 def test_sharded_partitions_assemble_on_one_gpu(ctx):
