@@ -53,10 +53,13 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["nd3d", "plain2d", "circuit", "bundled", "batch", "serve"],
                     default="nd3d")
-    ap.add_argument("--batch-count", type=int, default=256, help="matrices in the batch workload")
+    ap.add_argument("--batch-count", type=int, default=256,
+                    help="matrices in the batch workload (also measured beside the default line; 0: skip)")
     ap.add_argument("--serve-count", type=int, default=120, help="requests in the serving stream")
     ap.add_argument("--serve-nmax", type=int, default=1_000_000, help="largest n of the serving stream")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate (1/s)")
+    ap.add_argument("--serve-compare", type=int, default=120,
+                    help="first requests served again, continuously and one at a time, for the comparison")
     ap.add_argument("--side", type=int, default=80, help="grid side of the nd3d workload")
     ap.add_argument("--reuse", type=int, default=-1,
                     help="reuse traversals along s-1 -> s chains (-1: library default, on)")
@@ -385,19 +388,22 @@ def _make_graph(spec):
 
 def serve_main(args):
     """The serving stream: seeded Poisson arrivals of mixed-kind requests with
-    n log-uniform in [1,000, n_max], served by continuous batching under a
-    120 GB admission budget, then the same stream one request per launch."""
+    n log-uniform in [1,000, n_max], served by continuous batching on the
+    persistent serving kernel under a 120 GB admission budget.  Long streams
+    (the 10,000-request configuration) are generated in a process pool while
+    they are served.  The first --serve-compare requests are then served
+    again, continuously and one request per launch, for the comparison; the
+    results must be identical request by request."""
     import multiprocessing as mp
     import torch
     import gsofa_b200
     from gsofa_b200 import matgen, serve
 
     spec = matgen.mixed_spec(args.serve_count, 1000, args.serve_nmax, matgen.SEEDS["serve"])
-    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
-        graphs = pool.map(_make_graph, spec)
     rng = np.random.default_rng(matgen.SEEDS["serve"] + 1)
-    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, size=len(graphs)))
-    reqs = [serve.Request(i, float(a), g) for i, (a, g) in enumerate(zip(arrivals, graphs))]
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, size=len(spec)))
+    k = min(args.serve_compare, len(spec))
+    pool = mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1))
     torch.cuda.set_device(0)
     ctx = gsofa_b200.Context(0)
     params = gsofa_b200.Params.default(want_pattern=0)
@@ -405,26 +411,39 @@ def serve_main(args):
     oversize = lambda g: ctx.symbfact(ctx.upload(g), params)  # noqa: E731
     cs = serve.ContinuousServer(srv, oversize=oversize, max_n=srv.max_n)
     # warm up on a few small requests
-    cs.run([serve.Request(-1, 0.0, g) for g in sorted(graphs, key=lambda g: g.n)[:4]])
+    warm = [serve.Request(-1 - i, 0.0, matgen.make("grid3d", 2000, i)) for i in range(4)]
+    cs.run(warm)
+    stream = serve.LazyStream(pool, _make_graph, spec, arrivals, ahead=256)
     with ClockSampler(0) as clk:
-        cont = cs.run(reqs)
+        full = cs.run(stream, keep_graphs=k)
+    srv.drain()
+    # the comparison on the first k requests (same arrival times)
+    sub = [serve.Request(r.rid, r.arrival_s, r.graph) for r in stream.reqs[:k]]
+    cont = cs.run(sub)
     srv.drain()
     srv.close()
-    launch = serve.Server(ctx, params, mem_budget_bytes=120 << 30).run(reqs)
-    single = serve.one_at_a_time(ctx, reqs, params)
-    for a, b, c in zip(cont["completions"], single["completions"], launch["completions"]):
+    single = serve.one_at_a_time(ctx, sub, params)
+    pool.close()
+    by_id = {c.rid: c for c in full["completions"]}
+    for a, b in zip(cont["completions"], single["completions"]):
+        c = by_id[a.rid]
         assert (a.result.fill_count, a.result.nnz_lu, a.result.n_supernodes) == \
                (b.result.fill_count, b.result.nnz_lu, b.result.n_supernodes) == \
                (c.result.fill_count, c.result.nnz_lu, c.result.n_supernodes)
-    rep, one = cont["report"], single["report"]
+        assert np.array_equal(a.result.u_row_count, b.result.u_row_count)
+        assert np.array_equal(a.result.sn_start, c.result.sn_start)
+    rep = full["report"]
     line = {
         "metric": "nnz(L+U)/s", "value": rep["nnz_lu_per_s"], "unit": "nnz/s", "n_gpus": 1,
         "steps": 1, "warmup": 1, "ms_per_step": rep["span_s"] * 1000.0, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator)",
-        "config": {"workload": f"serve_{len(reqs)}_poisson_{args.serve_rate:g}hz_n1k-{args.serve_nmax}",
-                   "requests": len(reqs), "admission_budget_gb": 120, "pattern": "counts only",
-                   "seed": matgen.SEEDS["serve"]},
-        "serving": rep, "one_at_a_time": one, "launch_batching": launch["report"],
+        "config": {"workload": f"serve_{len(spec)}_poisson_{args.serve_rate:g}hz_n1k-{args.serve_nmax}",
+                   "requests": len(spec), "admission_budget_gb": 120, "pattern": "counts only",
+                   "seed": matgen.SEEDS["serve"], "generation": "process pool, in arrival order, "
+                   "while serving (a request arrives when both its time and its matrix have come)"},
+        "serving": rep,
+        "comparison": {"requests": k, "continuous": cont["report"], "one_at_a_time": single["report"],
+                       "results_identical": True},
         "serving_kernel_max_n": cs.max_n,
         "factorizations_per_s": rep["factorizations_per_s"],
         "clocks": clk.summary(), "gpu_launches": None,
@@ -507,6 +526,68 @@ def _device_timed(torch, stream, flush, steps, fn):
     e1.record(stream)
     torch.cuda.synchronize()
     return e0.elapsed_time(e1), out
+
+
+def batched_vs_plain(args, ctx, torch, stream, gsofa_b200):
+    """The mixed-size batch (256 matrices, n log-uniform in [2,000, 200,000],
+    2-D natural / 3-D nested-dissection / power-law RCM) in one persistent
+    launch replayed from a CUDA graph, against the plain loop of one launch
+    per matrix on the same GPU; counts and supernodes (the power-law members'
+    patterns hold ~0.25 n^2 entries each).  Also per matrix kind, so the
+    ratio's make-up is visible.  Results are compared matrix by matrix."""
+    import multiprocessing as mp
+    from gsofa_b200 import matgen
+    spec = matgen.config_batch(args.batch_count)
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        graphs = pool.map(_make_graph, spec, chunksize=4)
+    mats = [ctx.upload(g) for g in graphs]
+    flags = {"auto": 0, "global": gsofa_b200.FLAG_GLOBAL_STATE, "shared": gsofa_b200.FLAG_SHARED_STATE}[args.state]
+    p = gsofa_b200.Params.default(want_pattern=0, flags=gsofa_b200.FLAG_NO_DOWNLOAD | flags)
+    pg = gsofa_b200.Params.default(want_pattern=0, flags=gsofa_b200.FLAG_NO_DOWNLOAD | gsofa_b200.FLAG_GRAPH | flags)
+
+    def timed(fn, k):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = None
+        for _ in range(k):
+            out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k, out
+
+    def plain(ms):
+        return [ctx.symbfact(m, p) for m in ms]
+
+    plain(mats)
+    t_plain, rp = timed(lambda: plain(mats), 1)
+    ctx.symbfact_batch(mats, pg)
+    t_batch, rb = timed(lambda: ctx.symbfact_batch(mats, pg), 2)
+    same = all((a.fill_count, a.nnz_lu, a.n_supernodes) == (b.fill_count, b.nnz_lu, b.n_supernodes)
+               for a, b in zip(rp, rb))
+    per_kind = {}
+    for kind in ("grid2d", "grid3d", "powerlaw"):
+        sel = [m for m, (k, _, _) in zip(mats, spec) if k == kind]
+        if not sel:
+            continue
+        tp, _ = timed(lambda: plain(sel), 1)
+        ctx.symbfact_batch(sel, p)
+        tb, _ = timed(lambda: ctx.symbfact_batch(sel, p), 1)
+        per_kind[kind] = {"matrices": len(sel), "lines": int(sum(m.n for m in sel)), "plain_ms": tp,
+                          "batched_ms": tb, "batched_vs_plain": tp / tb}
+    nnz = sum(r.nnz_lu for r in rb)
+    for m in mats:
+        m.free()
+    return {"workload": f"batch_{len(mats)}_mixed_2k-200k", "matrices": len(mats),
+            "lines": int(sum(g.n for g in graphs)), "nnz_lu": int(nnz), "seed": matgen.SEEDS["batch"],
+            "pattern": "counts only", "batched_ms": t_batch, "plain_ms": t_plain,
+            "batched_value": nnz / (t_batch / 1000.0), "plain_value": nnz / (t_plain / 1000.0),
+            "batched_vs_plain": t_plain / t_batch,
+            "batched_factorizations_per_s": len(mats) / (t_batch / 1000.0),
+            "plain_factorizations_per_s": len(mats) / (t_plain / 1000.0),
+            "graph": "one persistent launch replayed from a CUDA graph", "results_identical": same,
+            "per_kind": per_kind}
 
 
 def sharded_main(args, world, rank, local):
@@ -858,6 +939,10 @@ def main():
             "cycles": dict(zip(("seed", "levels", "fold", "count", "lists", "clear", "pair_wait"),
                                res.cycles)), "ctas": res.ctas}
 
+    batched = None
+    if world == 1 and args.batch_count > 0 and args.workload == "nd3d":
+        batched = batched_vs_plain(args, ctx, torch, stream, gsofa_b200)
+
     cpu = None
     parity = None
     if rank == 0:
@@ -886,6 +971,7 @@ def main():
             "factorizations_per_s": facts,
             "other_forms": forms,
             "split_on_one_gpu": split,
+            "batched": batched,
             "e2e": e2e,
             "roofline": roof,
             "cpu_baseline": cpu,

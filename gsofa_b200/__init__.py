@@ -42,6 +42,7 @@ FLAG_DEVICE_TIMING = 0x2
 FLAG_GRAPH = 0x4
 FLAG_GLOBAL_STATE = 0x8    # visited bitmaps in global memory (many traversals per SM, any n)
 FLAG_SHARED_STATE = 0x10   # visited bitmaps in shared memory (at most two per SM)
+FLAG_DIRECT_HOST = 0x20    # symbfact_ranges into host memory: the kernel writes it directly
 
 
 class GsofaError(RuntimeError):
@@ -98,6 +99,7 @@ class ServerConfig(ctypes.Structure):
         ("max_requests", ctypes.c_int32),
         ("idle_exit_us", ctypes.c_int32),
         ("max_n_out", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
     ]
 
 
@@ -605,9 +607,9 @@ class StreamServer:
 
     def __init__(self, device: int = 0, mem_budget_bytes: int = 0, max_n: int = 0,
                  max_supernode_size: int = 0, src_chunk: int = 0, max_requests: int = 0,
-                 idle_exit_us: int = 0):
+                 idle_exit_us: int = 0, flags: int = 0):
         cfg = ServerConfig(device, max_n, mem_budget_bytes, max_supernode_size, src_chunk,
-                           max_requests, idle_exit_us, 0)
+                           max_requests, idle_exit_us, 0, flags)
         h = ctypes.c_void_p()
         _check(lib().gsofa_server_create(ctypes.byref(h), ctypes.byref(cfg)), "gsofa_server_create")
         self._h = h

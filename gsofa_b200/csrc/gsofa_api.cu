@@ -15,6 +15,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <functional>
+#include <thread>
 #include <map>
 #include <unordered_map>
 #include <cmath>
@@ -92,6 +94,10 @@ struct gsofa_ctx {
     // job scratch
     DevBuf queue, cnt, nxt, poff, gptr, lrow, snind, snlist, tiles, misc, pool, out, mats, ranges, stamp;
     DevBuf gstate;            // visited bitmaps of the global-state kernels
+    DevBuf blk;               // streaming: written entries per pool block
+    unsigned int *h_blk = nullptr;   // page-locked mirror of blk
+    size_t h_blk_cap = 0;
+    cudaStream_t s_poll = nullptr, s_copy = nullptr;   // streaming: counter reads, block copies
     DevBuf sn_head, sn_data;  // gsofa_result_supernodal: sizes and offsets; index lists
     std::vector<int64_t> sn_xl, sn_xu;   // supernodal offsets of the result sizes were taken for
     const void *sn_for = nullptr;        // ... that result (its internal record)
@@ -204,6 +210,12 @@ struct ResultInternal {
 struct ExtPool {
     int32_t *dev = nullptr;
     int64_t cap = 0;
+    // streaming to host: per-block written-entry counters the kernel keeps,
+    // and the host loop that copies full blocks out while the kernel runs
+    unsigned int *blk_done = nullptr;
+    int32_t blk_shift = 0;
+    int64_t nblk = 0;
+    std::function<void()> while_running;
 };
 
 int pick_block(int32_t max_n)
@@ -312,6 +324,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     if (ext && (p.want_pattern != 2 || part_count != 1)) return GSOFA_ERR_INVALID_INPUT;
     const int pattern_form = (p.want_pattern != 0 && part_count == 1) ? (ext ? 2 : 1) : 0;
     const bool want_pattern = pattern_form != 0;
+    const bool restrict_tiles = line_range && pattern_form != 1;
     // reuse: -1 (auto) or 1 = paired passes with exact reuse when two bitmaps
     // fit in shared memory, else adjacency chains; 2 = adjacency chains;
     // 0 = every source from scratch.  Interleaved partitions have no
@@ -561,6 +574,11 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         a.sn_list = d_sn;
         a.mat_info = d_minfo;
         a.ntiles = ntiles;
+        // a line range without the CSR form needs its own lines only: the
+        // scans cover its tiles (the totals are its lists' lengths, and no
+        // supernode partition is formed from part of the lines)
+        a.tile_lo = restrict_tiles ? (int64_t)range_lo / TILE : 0;
+        a.tile_hi = restrict_tiles ? ((int64_t)range_hi + TILE - 1) / TILE : ntiles;
         a.tile_sum = d_tiles;
         a.tile_last = d_tiles + 2 * ntiles;
         a.tile_sn = d_tiles + 3 * ntiles;
@@ -569,6 +587,8 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         a.stamp = d_stamp;
         a.stamp_stride = stamp_stride;
         a.gbm = d_gstate;
+        a.blk_done = ext ? ext->blk_done : nullptr;
+        a.blk_shift = ext ? ext->blk_shift : 0;
 
         // The job: descriptor copies, clears and the cooperative launch.  With
         // GSOFA_FLAG_GRAPH it is captured once into a CUDA graph and replayed
@@ -584,6 +604,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
                                         cudaMemcpyHostToDevice, st));
             GS_CUDA(cudaMemsetAsync(d_misc, 0, 256, st));
             GS_CUDA(cudaMemsetAsync(d_lrow, 0, (size_t)L * sizeof(int32_t), st));
+            if (a.blk_done) GS_CUDA(cudaMemsetAsync(a.blk_done, 0, (size_t)ext->nblk * 4, st));
             if (subset) {
                 GS_CUDA(cudaMemsetAsync(d_cnt, 0, (size_t)2 * L * sizeof(int32_t), st));
                 GS_CUDA(cudaMemsetAsync(d_nxt, 0, (size_t)2 * L, st));
@@ -652,6 +673,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
             issue(args, false);
         }
         GS_CUDA(cudaEventRecord(ctx->ev1, st));
+        if (ext && ext->while_running) ext->while_running();
 
         unsigned long long h_misc[25];
         GS_CUDA(cudaMemcpyAsync(h_misc, d_misc, sizeof(h_misc), cudaMemcpyDeviceToHost, st));
@@ -691,10 +713,14 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         s1[count] = tot[1];
         ss[count] = (int64_t)nsn;
         for (int i = count - 1; i >= 0; i--) {
-            if (md[i].n > 0) {
+            if (restrict_tiles) {   // one matrix; its own lines only, no supernodes
+                s0[i] = s1[i] = 0;
+                ss[i] = ss[i + 1] = 0;
+            } else if (md[i].n > 0) {
                 s0[i] = mi[3 * i];
                 s1[i] = mi[3 * i + 1];
-                ss[i] = mi[3 * i + 2];
+                ss[i] = line_range ? 0 : mi[3 * i + 2];
+                if (line_range) ss[i + 1] = 0;
             } else {
                 s0[i] = s0[i + 1];
                 s1[i] = s1[i + 1];
@@ -878,7 +904,7 @@ void gsofa_destroy(gsofa_ctx *c)
     DevBuf *bufs[] = {&c->queue, &c->cnt, &c->nxt, &c->poff, &c->gptr, &c->lrow, &c->snind,
                       &c->snlist, &c->tiles, &c->misc, &c->pool, &c->out, &c->mats, &c->ranges,
                       &c->st_beg, &c->st_end, &c->st_adj, &c->st_tmp, &c->matinfo, &c->stamp,
-                      &c->sn_head, &c->sn_data, &c->gstate};
+                      &c->sn_head, &c->sn_data, &c->gstate, &c->blk};
     for (DevBuf *b : bufs) c->release(*b);
     for (DevBuf &b : c->slabs) cudaFree(b.p);
     c->slabs.clear();
@@ -886,6 +912,9 @@ void gsofa_destroy(gsofa_ctx *c)
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    if (c->s_poll) cudaStreamDestroy(c->s_poll);
+    if (c->s_copy) cudaStreamDestroy(c->s_copy);
+    if (c->h_blk) cudaFreeHost(c->h_blk);
     delete c;
 }
 
@@ -1250,6 +1279,7 @@ gsofa_status gsofa_symbfact_ranges(gsofa_ctx *c, int count, const gsofa_matrix *
         }
         ExtPool ext;
         ext.cap = pool_capacity;
+        int32_t *host_dst = nullptr;   // staged: lists go to a device pool, then here
         if (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) {
             if (at.type == cudaMemoryTypeDevice && at.device != c->device) return GSOFA_ERR_INVALID_INPUT;
             ext.dev = pool;
@@ -1259,11 +1289,73 @@ gsofa_status gsofa_symbfact_ranges(gsofa_ctx *c, int count, const gsofa_matrix *
                 cudaGetLastError();
                 return GSOFA_ERR_INVALID_INPUT;
             }
-            ext.dev = (int32_t *)d;
+            // Staged through device memory when a device pool of the same
+            // capacity fits the budget (the copy engine moves it at full
+            // PCIe speed); else, or with GSOFA_FLAG_DIRECT_HOST, the kernel
+            // writes the lists into host memory itself, so the pattern needs
+            // no device memory at all.
+            const size_t bytes = (size_t)pool_capacity * 4;
+            const bool staged = !(p.flags & GSOFA_FLAG_DIRECT_HOST) && c->held - c->pool.bytes + bytes <= c->budget / 2;
+            if (staged) {
+                ext.dev = (int32_t *)c->grow(c->pool, bytes);
+                host_dst = pool;
+            } else {
+                ext.dev = (int32_t *)d;
+            }
         } else {
             return GSOFA_ERR_INVALID_INPUT;   // pageable host memory
         }
+        // Staged: the kernel counts the entries written into every block of
+        // kStreamShift entries; while it runs, this thread reads the counts
+        // (a small copy on its own stream) and has the copy engine move each
+        // full block to the host, so most of the download overlaps the
+        // traversals.  The partly filled blocks follow when the kernel ends.
+        constexpr int32_t kStreamShift = 22;   // 4M entries (16 MiB) a block
+        std::vector<char> copied;
+        if (host_dst) {
+            if (!c->s_poll) GS_CUDA(cudaStreamCreateWithFlags(&c->s_poll, cudaStreamNonBlocking));
+            if (!c->s_copy) GS_CUDA(cudaStreamCreateWithFlags(&c->s_copy, cudaStreamNonBlocking));
+            ext.blk_shift = kStreamShift;
+            ext.nblk = ((pool_capacity - 1) >> kStreamShift) + 1;
+            ext.blk_done = (unsigned int *)c->grow(c->blk, (size_t)ext.nblk * 4);
+            if (c->h_blk_cap < (size_t)ext.nblk) {
+                if (c->h_blk) cudaFreeHost(c->h_blk);
+                c->h_blk = nullptr;
+                c->h_blk_cap = 0;
+                GS_CUDA(cudaHostAlloc((void **)&c->h_blk, (size_t)ext.nblk * 4, cudaHostAllocDefault));
+                c->h_blk_cap = (size_t)ext.nblk;
+            }
+            copied.assign((size_t)ext.nblk, 0);
+            const int64_t bsz = (int64_t)1 << kStreamShift;
+            ext.while_running = [&]() {
+                for (;;) {
+                    const bool finished = cudaEventQuery(c->ev1) == cudaSuccess;
+                    GS_CUDA(cudaMemcpyAsync(c->h_blk, ext.blk_done, (size_t)ext.nblk * 4, cudaMemcpyDeviceToHost,
+                                            c->s_poll));
+                    GS_CUDA(cudaStreamSynchronize(c->s_poll));
+                    for (int64_t b = 0; b < ext.nblk; b++)
+                        if (!copied[(size_t)b] && (int64_t)c->h_blk[b] == bsz) {
+                            GS_CUDA(cudaMemcpyAsync(host_dst + b * bsz, ext.dev + b * bsz, (size_t)bsz * 4,
+                                                    cudaMemcpyDeviceToHost, c->s_copy));
+                            copied[(size_t)b] = 1;
+                        }
+                    if (finished) break;
+                    std::this_thread::sleep_for(std::chrono::microseconds(50));
+                }
+            };
+        }
         gsofa_status s = run_job(c, count, mats, &p, out, &ext);
+        if (host_dst) {
+            if (s == GSOFA_OK) {
+                const int64_t bsz = (int64_t)1 << kStreamShift, used = out[0].pool_used;
+                for (int64_t b = 0; b < ext.nblk && b * bsz < used; b++)
+                    if (!copied[(size_t)b])
+                        GS_CUDA(cudaMemcpyAsync(host_dst + b * bsz, ext.dev + b * bsz,
+                                                (size_t)(std::min(used, (b + 1) * bsz) - b * bsz) * 4,
+                                                cudaMemcpyDeviceToHost, c->s_copy));
+            }
+            GS_CUDA(cudaStreamSynchronize(c->s_copy));
+        }
         if (s != GSOFA_OK)
             for (int i = 0; i < count; i++) free_result_arrays(&out[i]);
         return s;
@@ -1815,6 +1907,8 @@ extern "C" gsofa_status gsofa_symbfact_counts_noalloc(int device, void *cuda_str
         a.snind = snind;
         a.sn_list = d_sn_start;
         a.ntiles = ntiles;
+        a.tile_lo = 0;
+        a.tile_hi = ntiles;
         a.tile_sum = tiles;
         a.tile_last = tiles + 2 * ntiles;
         a.tile_sn = tiles + 3 * ntiles;
@@ -1911,6 +2005,10 @@ constexpr int32_t kSmallRequest = 65536;   // lines below which a request is cla
 // registers a thread, 768 threads leave 16K registers and 1280 thread slots
 // per SM: two 256-thread upload blocks still run beside the persistent kernel.
 constexpr int kServeBlock = 768;
+// Global-state form: 256-thread CTAs, three per SM (768 threads, 48K of the
+// 64K registers), six traversals per SM.
+constexpr int kServeBlockG = 256;
+constexpr int kServeCtasG = 3;
 
 }  // namespace
 
@@ -1923,6 +2021,8 @@ struct gsofa_server {
     int32_t max_slots = 4096;
     int idle_spins = 10000;
     int block = kServeBlock, ring = 1024, grid = 0;
+    bool gbm = false;               // bitmaps in global memory (d_gstate)
+    uint32_t *d_gstate = nullptr;
     int32_t bitmap_words = 0, state_words = 0;
     size_t smem = 0;
     cudaStream_t run = nullptr, io = nullptr;
@@ -2014,6 +2114,7 @@ gsofa_status server_launch_if_idle_impl(gsofa_server *s)
     a.bitmap_words = s->bitmap_words;
     a.state_words = s->state_words;
     a.ring_size = s->ring;
+    a.gbm = s->d_gstate;
     a.lanes = 1;
     a.reuse = 1;
     a.want_pattern = 0;
@@ -2027,7 +2128,8 @@ gsofa_status server_launch_if_idle_impl(gsofa_server *s)
     sa.slots = s->d_slots;
     sa.slot_done = s->d_done;
     sa.idle_spins = s->idle_spins;
-    serve_kernel<kServeBlock><<<s->grid, kServeBlock, s->smem, s->run>>>(sa);
+    if (s->gbm) serve_kernel<kServeBlockG, true><<<s->grid, kServeBlockG, s->smem, s->run>>>(sa);
+    else serve_kernel<kServeBlock, false><<<s->grid, kServeBlock, s->smem, s->run>>>(sa);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? GSOFA_OK : fail_cuda(e);
 }
@@ -2069,10 +2171,18 @@ gsofa_status gsofa_server_create(gsofa_server **out, gsofa_server_config *cfg)
         // kernel instead of waiting for it to exit.
         const size_t reserve = 12 * 1024;
         const size_t static_smem = 2 * sizeof(SharedState) + 1024 + reserve;
+        if ((cfg->flags & GSOFA_FLAG_GLOBAL_STATE) && (cfg->flags & GSOFA_FLAG_SHARED_STATE)) {
+            delete s;
+            return GSOFA_ERR_INVALID_INPUT;
+        }
+        // the global-state form unless shared memory is asked for
+        s->gbm = !(cfg->flags & GSOFA_FLAG_SHARED_STATE);
+        s->block = s->gbm ? kServeBlockG : kServeBlock;
         const int64_t per_half_words = ((int64_t)(s->optin - static_smem) / 2 - 1024 * 4) / 4;
         const int32_t limit_n =
-            (int32_t)std::min<int64_t>((per_half_words - 64) * 32 / 33 / 128 * 128 * 32, INT32_MAX);
-        s->max_n = cfg->max_n > 0 ? cfg->max_n : limit_n;
+            s->gbm ? (int32_t)(1 << 26)
+                   : (int32_t)std::min<int64_t>((per_half_words - 64) * 32 / 33 / 128 * 128 * 32, INT32_MAX);
+        s->max_n = cfg->max_n > 0 ? cfg->max_n : (s->gbm ? (1 << 20) : limit_n);
         if (s->max_n > limit_n || s->max_n <= 0) { delete s; return GSOFA_ERR_UNSUPPORTED; }
         s->max_sn = cfg->max_supernode_size;
         s->chunk = cfg->src_chunk > 0 ? cfg->src_chunk : 0;
@@ -2080,26 +2190,39 @@ gsofa_status gsofa_server_create(gsofa_server **out, gsofa_server_config *cfg)
         s->idle_spins = std::max(1, (cfg->idle_exit_us > 0 ? cfg->idle_exit_us : 30000000) / 2);
         s->bitmap_words = ((s->max_n + 31) / 32 + 127) / 128 * 128;
         s->state_words = s->bitmap_words + s->bitmap_words / 32 + ((s->bitmap_words / 32 + 31) / 32 + 3) / 4 * 4;
-        // frontier ring: the largest that fits beside the two bitmaps
-        void *kfn = (void *)serve_kernel<kServeBlock>;
+        // frontier ring: the largest that fits beside the two bitmaps (shared
+        // state), or beside two more CTAs' rings (global state)
+        void *kfn = s->gbm ? (void *)serve_kernel<kServeBlockG, true> : (void *)serve_kernel<kServeBlock, false>;
+        const int per_sm = s->gbm ? kServeCtasG : 1;
+        const size_t smem_state = s->gbm ? 0 : (size_t)s->state_words * 4;
         s->ring = 0;
         for (int cand = 8192; cand >= 1024; cand >>= 1) {
-            const size_t sm = 2 * ((size_t)s->state_words * 4 + (size_t)cand * 4);
-            if (sm + static_smem <= s->optin) { s->ring = cand; s->smem = sm; break; }
+            const size_t sm = 2 * (smem_state + (size_t)cand * 4);
+            if ((sm + static_smem - reserve) * per_sm + reserve <= (size_t)prop.sharedMemPerMultiprocessor &&
+                sm + static_smem <= s->optin) {
+                s->ring = cand;
+                s->smem = sm;
+                break;
+            }
         }
         if (!s->ring) { delete s; return GSOFA_ERR_UNSUPPORTED; }
-        GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem));
         int occ = 0;
-        GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, kServeBlock, s->smem));
-        if (occ <= 0) { delete s; return GSOFA_ERR_UNSUPPORTED; }
-        s->grid = s->sms;   // one CTA per SM leaves room for the upload kernels
+        {
+            std::lock_guard<std::mutex> lk(kernel_attr_mutex());
+            GS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem));
+            GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, s->block, s->smem));
+        }
+        if (occ < per_sm) { delete s; return GSOFA_ERR_UNSUPPORTED; }
+        // a fixed number of CTAs per SM leaves room for the upload kernels
+        s->grid = s->sms * per_sm;
         GS_CUDA(cudaStreamCreateWithFlags(&s->run, cudaStreamNonBlocking));
         GS_CUDA(cudaStreamCreateWithFlags(&s->io, cudaStreamNonBlocking));
         size_t fr = 0, tot = 0;
         GS_CUDA(cudaMemGetInfo(&fr, &tot));
         const int64_t budget = cfg->mem_budget_bytes > 0 ? cfg->mem_budget_bytes : (int64_t)(0.9 * (double)fr);
         s->lmax = std::max<int64_t>(4 * (int64_t)s->max_n, 1 << 24);
-        const int64_t fixed = (int64_t)s->grid * 2 * s->max_n * 4 +
+        const int64_t gstate_bytes = s->gbm ? (int64_t)s->grid * 2 * s->state_words * 4 : 0;
+        const int64_t fixed = (int64_t)s->grid * 2 * s->max_n * 4 + gstate_bytes +
                               (int64_t)kServeClasses * s->piece_cap * sizeof(ServePiece) +
                               (int64_t)s->max_slots * (sizeof(MatDesc) + 4) + s->lmax * 10 + 4096;
         s->arena_units = (budget - fixed) / kArenaUnit;
@@ -2115,6 +2238,7 @@ gsofa_status gsofa_server_create(gsofa_server **out, gsofa_server_config *cfg)
         GS_CUDA(cudaMalloc(&s->d_cnt, (size_t)2 * s->lmax * 4));
         GS_CUDA(cudaMalloc(&s->d_nxt, (size_t)2 * s->lmax));
         GS_CUDA(cudaMalloc(&s->d_queue, (size_t)s->grid * 2 * s->max_n * 4));
+        if (s->gbm) GS_CUDA(cudaMalloc(&s->d_gstate, (size_t)gstate_bytes));
         GS_CUDA(cudaMalloc(&s->d_arena, (size_t)s->arena_units * kArenaUnit));
         GS_CUDA(cudaMemsetAsync(s->d_ctl, 0, sizeof(ServeCtl) + 64, s->io));
         GS_CUDA(cudaMemsetAsync(s->d_done, 0, (size_t)s->max_slots * 4, s->io));
@@ -2168,6 +2292,7 @@ void gsofa_server_destroy(gsofa_server *s)
     cudaFree(s->d_cnt);
     cudaFree(s->d_nxt);
     cudaFree(s->d_queue);
+    cudaFree(s->d_gstate);
     cudaFree(s->d_arena);
     if (s->run) cudaStreamDestroy(s->run);
     if (s->io) cudaStreamDestroy(s->io);

@@ -93,6 +93,8 @@ struct JobArgs {
     int64_t *mat_info;         // [nmats][3] at each matrix's first line: pass-0 and
                                // pass-1 CSR offsets, supernodes before it
     int64_t ntiles;
+    int64_t tile_lo, tile_hi;  // the post-traversal phases cover tiles [tile_lo, tile_hi)
+                               // (all of them, unless only a line range was processed)
     int64_t *tile_sum;         // [2][ntiles] then exclusive prefix (in place)
     int64_t *tile_last;        // [ntiles] last supernode-run start, then prefix max
     int64_t *tile_sn;          // [ntiles] then exclusive prefix
@@ -108,6 +110,8 @@ struct JobArgs {
     int64_t stamp_stride;      // the chain index at which each vertex was first set
     uint32_t *gbm;             // global-state kernels: per traversal, state_words
                                // words (bitmap and its summaries) in global memory
+    unsigned int *blk_done;    // ranges form, streamed: entries written into each
+    int32_t blk_shift;         // pool block of 2^blk_shift entries (or null)
 };
 
 constexpr int TILE = 2048;     // lines per tile in the post-traversal phases
@@ -277,6 +281,13 @@ __device__ __forceinline__ void push(const Frontier &f, int *tail, int base, int
     fr_put(f, base + b + (int)g.thread_rank(), w0, m);
 }
 
+// Seeding window: the rows of up to SEED_WIN consecutive sources (SEED_ADJ
+// ids at most), loaded together -- consecutive rows are one stretch of the
+// adjacency array -- so a source's seeding reads shared memory instead of
+// waiting on two dependent L2 round trips.
+constexpr int SEED_WIN = 32;
+constexpr int SEED_ADJ = 512;
+
 struct SharedState {
     long long piece;
     int flag;
@@ -298,16 +309,21 @@ struct SharedState {
     uint16_t *stamp;   // this traversal's stamp row, or null (counts only)
     int chain_s0;      // its first source
     int chain_len;     // its sources so far (the current one included)
-    int chain_idx;     // index of the current source in it
     int64_t chain_total;  // entries of its lists
+    // the seeding window: sources [win_lo, win_hi) of the current piece
+    int win_lo, win_hi;
+    int32_t win_ptr[SEED_WIN + 1];   // their row bounds in adj
+    int32_t win_raw[SEED_WIN];       // their input degrees (work counters)
+    int32_t win_adj[SEED_ADJ];       // adj[win_ptr[0] .. win_ptr[win_hi - win_lo])
 };
 
-// Records that v was first set while the chain's source chain_idx ran.
-// Only vertices above the chain's first source can appear in its lists.
-__device__ __forceinline__ void stamp_set(const SharedState &sh, int32_t v)
+// Records that v was first set while the chain's source `idx` ran (sources
+// of a chain are consecutive, so idx = s - chain_s0).  Only vertices above
+// the chain's first source can appear in its lists.
+__device__ __forceinline__ void stamp_set(const SharedState &sh, int32_t v, int idx, int32_t chain_s0)
 {
     uint16_t *st = sh.stamp;
-    if (st != nullptr && v > sh.chain_s0) st[v] = (uint16_t)sh.chain_idx;
+    if (st != nullptr && v > chain_s0) st[v] = (uint16_t)idx;
 }
 
 // Clears the bitmap words covering vertices [lo, hi]; gtid/GT: the calling
@@ -384,7 +400,7 @@ __device__ __forceinline__ int32_t chain_start(const PassGraph &g, int32_t x, in
         if (test_and_set<GBM>(bm, summ, _m)) {                                        \
             t_lo = min(t_lo, _m);                                               \
             t_hi = max(t_hi, _m);                                               \
-            stamp_set(sh, _m);                                                  \
+            stamp_set(sh, _m, cidx, s - cidx);                                            \
             if (_m < s) push(f, tailp, end, start, _m);                         \
             else nh++;                                                          \
         }                                                                       \
@@ -398,9 +414,16 @@ __device__ __forceinline__ int32_t chain_start(const PassGraph &g, int32_t x, in
 // X(s) and hi(s-1) minus {s} is inside hi(s).
 // END_SYNC: finish with a barrier of the traversal's threads (not needed when
 // the caller's next step is a barrier of the whole CTA).
+//
+// The level counters (tailc, fetch) are zero on entry: the previous source
+// left them so.  s_end: the end of the piece (the seeding window stays within
+// it); stride: the distance between the piece's sources; cidx: the index of
+// s in its chain (every thread tracks it; a chain's sources are consecutive,
+// so it starts at s - cidx).
 template <int GT, bool CG, bool END_SYNC, bool GBM>
 __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
-                               int64_t line, int pass, int32_t s, uint32_t *bm, uint32_t *summ,
+                               int64_t line, int pass, int32_t s, int32_t s_end, int32_t stride,
+                               int cidx, uint32_t *bm, uint32_t *summ,
                                const Frontier &f, SharedState &sh,
                                unsigned long long &edges, const int32_t *rawdeg,
                                unsigned long long &xcnt, unsigned long long &einsp,
@@ -413,28 +436,59 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
     int t_lo = INT32_MAX, t_hi = -1;
 
     long long c0 = 0;
-    if (tid == 0) {
-        c0 = clock64();
-        sh.tailc[0] = sh.tailc[1] = sh.tailc[2] = 0;
-        sh.fetch[0] = sh.fetch[1] = sh.fetch[2] = 0;
-        sh.chain_idx = sh.chain_len;
-        sh.chain_len = sh.chain_idx + 1;
-        if (test_and_set<GBM>(bm, summ, s)) { t_lo = s; t_hi = s; stamp_set(sh, s); }
-        else sh.hcount--;   // s was in hi(s-1): counted, but not above s
+    if (tid == 0) c0 = clock64();
+    // a new seeding window when s is past the current one (consecutive
+    // sources only): row bounds, then the rows themselves, all threads
+    int wlo = sh.win_lo, whi = sh.win_hi;   // stable: set behind earlier barriers
+    if (stride == 1 && (s < wlo || s >= whi)) {
+        const int hi0 = min(s_end, s + SEED_WIN);
+        for (int i = tid; i <= hi0 - s; i += GT) {
+            sh.win_ptr[i] = ld<CG>(g.ptr + s + i);
+            if (i < hi0 - s) sh.win_raw[i] = ld<CG>(rawdeg + s + i);
+        }
+        gsync<GT>(bar);
+        int k = hi0 - s;   // rows that fit
+        while (k > 0 && sh.win_ptr[k] - sh.win_ptr[0] > SEED_ADJ) k--;
+        const int32_t a0 = sh.win_ptr[0], na = sh.win_ptr[k] - a0;
+        for (int i = tid; i < na; i += GT) sh.win_adj[i] = ld<CG>(g.adj + a0 + i);
+        gsync<GT>(bar);
+        wlo = s;
+        whi = s + k;
+        if (tid == 0) { sh.win_lo = wlo; sh.win_hi = whi; }   // read by later sources
     }
-    gsync<GT>(bar);
+    const bool in_win = stride == 1 && s >= wlo && s < whi;
+    if (tid == 0) {
+        sh.chain_len = cidx + 1;
+        if (test_and_set<GBM>(bm, summ, s)) { t_lo = s; t_hi = s; stamp_set(sh, s, cidx, s - cidx); }
+        else atomicAdd(&sh.hcount, -1);   // s was in hi(s-1): counted, but not above s
+    }
+    // No barrier here: seeding pushes onto the zeroed level-0 counter, the
+    // stamps take the thread's own cidx, and s itself (which no neighbour of
+    // s is) is set before the level loop's first barrier.
 
     // seeding: every neighbour of s is structure of line s; level-0 items
     {
-        const int32_t b0 = ld<CG>(g.ptr + s), e0 = ld<CG>(g.ptr + s + 1);
+        int32_t b0, e0;
+        if (in_win) {
+            b0 = sh.win_ptr[s - wlo];
+            e0 = sh.win_ptr[s - wlo + 1];
+        } else {
+            b0 = ld<CG>(g.ptr + s);
+            e0 = ld<CG>(g.ptr + s + 1);
+        }
         if (tid == 0) {
             edges += (unsigned long long)(e0 - b0);
-            if (pass == 0) einsp += (unsigned long long)ld<CG>(rawdeg + s);
+            if (pass == 0) einsp += (unsigned long long)(in_win ? sh.win_raw[s - wlo] : ld<CG>(rawdeg + s));
         }
         int *tailp = &sh.tailc[0];
         const int end = 0, start = 0;
         int nh = 0;
-        for (int32_t k = b0 + tid; k < e0; k += GT) GSOFA_VISIT(ld<CG>(g.adj + k));
+        if (in_win) {
+            const int32_t *wa = sh.win_adj - sh.win_ptr[0];
+            for (int32_t k = b0 + tid; k < e0; k += GT) GSOFA_VISIT(wa[k]);
+        } else {
+            for (int32_t k = b0 + tid; k < e0; k += GT) GSOFA_VISIT(ld<CG>(g.adj + k));
+        }
         nh = (int)__reduce_add_sync(0xffffffffu, (unsigned)nh);
         if (lane == 0 && nh) atomicAdd(&sh.hcount, nh);
     }
@@ -485,7 +539,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                         const bool on = k0 + lane < hd;
                         const int32_t m = on ? ld<CG>(g.adj + hb + k0 + lane) : 0;
                         const bool fresh = on && test_and_set<GBM>(bm, summ, m);
-                        if (fresh) { t_lo = min(t_lo, m); t_hi = max(t_hi, m); stamp_set(sh, m); }
+                        if (fresh) { t_lo = min(t_lo, m); t_hi = max(t_hi, m); stamp_set(sh, m, cidx, s - cidx); }
                         const bool low = fresh && m < s;
                         const unsigned bal = __ballot_sync(0xffffffffu, low);
                         const unsigned bhi = __ballot_sync(0xffffffffu, fresh) & ~bal;
@@ -523,7 +577,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                     if (fresh && sh.stamp != nullptr) {
 #pragma unroll
                         for (int u = 0; u < 8; u++)
-                            if ((fresh >> u) & 1u) stamp_set(sh, buf[u]);
+                            if ((fresh >> u) & 1u) stamp_set(sh, buf[u], cidx, s - cidx);
                     }
                     int incl = nlh;
 #pragma unroll
@@ -591,6 +645,11 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
     // when the chain ends (output_chain); here only the count and the link
     // flag.
     if (tid == 0) {
+        // the next source starts from zeroed level counters (every thread
+        // read this one's last, empty level before leaving the loop; the
+        // counters of that level are zero already)
+        sh.tailc[0] = sh.tailc[1] = sh.tailc[2] = 0;
+        sh.fetch[0] = sh.fetch[1] = sh.fetch[2] = 0;
         const int total = sh.hcount;
         const int64_t slot = (int64_t)pass * a.L + line;
         a.cnt[slot] = (int32_t)total;
@@ -737,6 +796,22 @@ __device__ void output_chain(const JobArgs &a, int64_t line_base, int pass, cons
         if (lane == 0 && pos != cnt) atomicOr(a.status, ERR_COUNT_MISMATCH);
     }
     gsync<GT>(bar);
+    // Streaming: count the chain's entries into the pool blocks they fill.
+    // Every list of the chain is written (the barrier above); one fence makes
+    // those writes visible device-wide before the counts that let the host
+    // copy a full block out while the traversals go on.
+    if (a.blk_done != nullptr && gtid == 0 && sh.chain_total > 0) {
+        const int64_t base = a.poff[row0];
+        if (base >= 0) {
+            __threadfence();
+            const int64_t end = base + sh.chain_total;
+            const int64_t bsz = (int64_t)1 << a.blk_shift;
+            for (int64_t b = base >> a.blk_shift; b <= (end - 1) >> a.blk_shift; b++) {
+                const int64_t lo = max(base, b * bsz), hi = min(end, (b + 1) * bsz);
+                atomicAdd(a.blk_done + b, (unsigned int)(hi - lo));
+            }
+        }
+    }
 }
 
 // Per-thread tallies of one CTA's traversals (summed over the CTA at the
@@ -757,10 +832,14 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
     const int tid = threadIdx.x;
     int prev = -2;
     int idx = 0;
+    // the current chain, tracked by every thread alike (decisions never read
+    // state another thread may be changing): index of the last source in it
+    // (-1: none yet)
+    int cidx = -1;
     for (int32_t s = s_lo; s < s_hi; s += stride, idx++) {
         int reuse = 0;
         // chain indices are 16-bit stamps: a chain ends after 65535 sources
-        if (a.reuse && prev == s - 1 && !(a.want_pattern && sh.chain_len >= 65535)) {
+        if (a.reuse && prev == s - 1 && !(a.want_pattern && cidx + 1 >= 65535)) {
             if (PAIRED) {
                 reuse = pair_flag[(idx - 1) & 1][1 - half];
             } else {
@@ -773,7 +852,7 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
             }
         }
         if (!reuse) {
-            if (a.want_pattern && sh.chain_len > 0) {
+            if (a.want_pattern && cidx >= 0) {
                 const long long co = clock64();
                 output_chain<GT, GBM>(a, md.line_base, pass, bm, summ, sh, gtid, bar);
                 if (gtid == 0) sh.prof[5] += (unsigned long long)(clock64() - co);
@@ -781,18 +860,23 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
             const long long cc = clock64();
             const int clo = sh.chain_lo, chi = sh.chain_hi;
             clear_range<GT>(bm, summ, clo, chi, gtid);
+            // the new chain's counters, in place before the barrier that
+            // precedes its first seeding (which adds to hcount)
+            if (gtid == 0) { sh.hcount = 0; sh.chain_s0 = s; sh.chain_len = 0; sh.chain_total = 0; }
             gsync<GT>(bar);
             if (gtid == 0) {
-                sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0;
-                sh.chain_s0 = s; sh.chain_len = 0; sh.chain_total = 0;
+                sh.chain_lo = INT32_MAX; sh.chain_hi = -1;
                 sh.prof[6] += (unsigned long long)(clock64() - cc);
             }
-        } else if (gtid == 0) {
-            sh.nreuse++;
+            cidx = 0;
+        } else {
+            cidx++;
+            if (gtid == 0) sh.nreuse++;
         }
         // paired: the pass-flag exchange below is a barrier of the whole CTA
-        process_source<GT, CG, !PAIRED, GBM>(a, g, md.n, md.line_base + s, pass, s, bm, summ, fr, sh, acc.edges,
-                           md.rawdeg, acc.xcnt, acc.einsp, sh.prof, gtid, bar);
+        process_source<GT, CG, !PAIRED, GBM>(a, g, md.n, md.line_base + s, pass, s, s_hi, stride, cidx,
+                                             bm, summ, fr, sh, acc.edges, md.rawdeg, acc.xcnt, acc.einsp,
+                                             sh.prof, gtid, bar);
         if (PAIRED) {
             if (gtid == 0) pair_flag[idx & 1][half] = sh.flag;
             const long long cw = clock64();
@@ -803,7 +887,7 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
         if (gtid == 0) sh.nsrc++;
     }
     // the piece's last chain
-    if (a.want_pattern && sh.chain_len > 0) {
+    if (a.want_pattern && cidx >= 0) {
         const long long co = clock64();
         output_chain<GT, GBM>(a, md.line_base, pass, bm, summ, sh, gtid, bar);
         if (gtid == 0) {
@@ -857,9 +941,12 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 1024 ? 1 : 1024 / BLOCK)) fac
     if (gtid == 0) {
         sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0;
         sh.stamp = a.want_pattern ? a.stamp + ((int64_t)blockIdx.x * NS + half) * a.stamp_stride : nullptr;
-        sh.chain_s0 = 0; sh.chain_len = 0; sh.chain_idx = 0; sh.chain_total = 0;
+        sh.chain_s0 = 0; sh.chain_len = 0; sh.chain_total = 0;
         for (int q = 0; q < 8; q++) sh.prof[q] = 0;
         sh.nsrc = sh.nreuse = 0;
+        sh.tailc[0] = sh.tailc[1] = sh.tailc[2] = 0;
+        sh.fetch[0] = sh.fetch[1] = sh.fetch[2] = 0;
+        sh.win_lo = sh.win_hi = 0;
     }
     const Frontier fr{ring, a.queue + ((int64_t)blockIdx.x * NS + half) * a.qcap, a.qcap, a.status,
                       a.ring_size};
@@ -908,7 +995,8 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 1024 ? 1 : 1024 / BLOCK)) fac
             const int clo = sh.chain_lo, chi = sh.chain_hi;
             clear_range<GT>(bm, summ, clo, chi, gtid);
             __syncthreads();
-            if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0; }
+            // the next piece may be another matrix: no seeding window yet
+            if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0; sh.win_lo = sh.win_hi = 0; }
             __syncthreads();
         }
     }
@@ -968,7 +1056,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 1024 ? 1 : 1024 / BLOCK)) fac
     };
 
     // ---- phase 2: tile partial sums ------------------------------------------
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    for (int64_t t = a.tile_lo + blockIdx.x; t < a.tile_hi; t += gridDim.x) {
         int64_t s0 = 0, s1 = 0, last = -1;
         for (int64_t l = t * TILE + tid; l < min(L, (t + 1) * TILE); l += BLOCK) {
             s0 += a.cnt[l];
@@ -990,16 +1078,16 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 1024 ? 1 : 1024 / BLOCK)) fac
     // ---- phase 3: block 0 scans the tile partials -----------------------------
     if (blockIdx.x == 0) {
         int64_t c0 = 0, c1 = 0, cm = -1;
-        for (int64_t base = 0; base < ntiles; base += BLOCK) {
+        for (int64_t base = a.tile_lo; base < a.tile_hi; base += BLOCK) {
             const int64_t t = base + tid;
-            const int64_t v0 = t < ntiles ? a.tile_sum[t] : 0;
-            const int64_t v1 = t < ntiles ? a.tile_sum[ntiles + t] : 0;
-            const int64_t vm = t < ntiles ? a.tile_last[t] : -1;
+            const int64_t v0 = t < a.tile_hi ? a.tile_sum[t] : 0;
+            const int64_t v1 = t < a.tile_hi ? a.tile_sum[ntiles + t] : 0;
+            const int64_t vm = t < a.tile_hi ? a.tile_last[t] : -1;
             int64_t tot0, tot1, totm;
             const int64_t e0 = block_excl_scan<BLOCK>(v0, &tot0, shs[0].warp);
             const int64_t e1 = block_excl_scan<BLOCK>(v1, &tot1, shs[0].warp);
             const int64_t em = block_excl_max<BLOCK>(vm, &totm, shs[0].warp);
-            if (t < ntiles) {
+            if (t < a.tile_hi) {
                 a.tile_sum[t] = c0 + e0;
                 a.tile_sum[ntiles + t] = c1 + e1;
                 a.tile_last[t] = max(cm, em);
@@ -1014,7 +1102,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 1024 ? 1 : 1024 / BLOCK)) fac
     grid.sync();
 
     // ---- phase 4: CSR offsets and supernode starts per tile -------------------
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    for (int64_t t = a.tile_lo + blockIdx.x; t < a.tile_hi; t += gridDim.x) {
         int64_t c0 = a.tile_sum[t], c1 = a.tile_sum[ntiles + t], carry = a.tile_last[t];
         int64_t nsn = 0;
         for (int64_t base = t * TILE; base < min(L, (t + 1) * TILE); base += BLOCK) {
@@ -1047,12 +1135,12 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 1024 ? 1 : 1024 / BLOCK)) fac
     // ---- phase 5: block 0 scans the supernode tile counts ---------------------
     if (blockIdx.x == 0) {
         int64_t c = 0;
-        for (int64_t base = 0; base < ntiles; base += BLOCK) {
+        for (int64_t base = a.tile_lo; base < a.tile_hi; base += BLOCK) {
             const int64_t t = base + tid;
-            int64_t v = t < ntiles ? a.tile_sn[t] : 0;
+            int64_t v = t < a.tile_hi ? a.tile_sn[t] : 0;
             int64_t tot;
             int64_t e = block_excl_scan<BLOCK>(v, &tot, shs[0].warp);
-            if (t < ntiles) a.tile_sn[t] = c + e;
+            if (t < a.tile_hi) a.tile_sn[t] = c + e;
             c += tot;
         }
         if (tid == 0) a.counters[2] = (unsigned long long)c;
@@ -1060,7 +1148,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK >= 1024 ? 1 : 1024 / BLOCK)) fac
     grid.sync();
 
     // ---- phase 6: supernode list, pattern compaction ---------------------------
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    for (int64_t t = a.tile_lo + blockIdx.x; t < a.tile_hi; t += gridDim.x) {
         int64_t c = a.tile_sn[t];
         for (int64_t base = t * TILE; base < min(L, (t + 1) * TILE); base += BLOCK) {
             const int64_t l = base + tid;

@@ -61,10 +61,12 @@ __device__ __forceinline__ T load_cg(const T *p)
     return out;
 }
 
-// At most 64 registers a thread: with 768 threads that leaves a quarter of
-// the SM's registers (and 1280 thread slots) to the upload kernels, which
-// must run beside this kernel while it holds every SM.
-template <int BLOCK>
+// At most 64 registers a thread, so the upload kernels, which must run beside
+// this kernel while it holds every SM, keep registers and thread slots: the
+// shared-state form runs one 768-thread CTA per SM (two traversals, their
+// bitmaps in shared memory); the global-state form (GBM, bitmaps in global
+// memory) three 256-thread CTAs per SM, six traversals of four warps each.
+template <int BLOCK, bool GBM>
 __global__ void __maxnreg__(64) serve_kernel(ServeArgs sa)
 {
     constexpr int GT = BLOCK / 2;
@@ -78,16 +80,20 @@ __global__ void __maxnreg__(64) serve_kernel(ServeArgs sa)
     const int gtid = tid % GT;
     const int bar = 1 + half;
     SharedState &sh = shs[half];
-    uint32_t *bm = smem_dyn + (size_t)half * a.state_words;
+    uint32_t *const state = GBM ? a.gbm + ((int64_t)blockIdx.x * 2) * a.state_words : smem_dyn;
+    uint32_t *bm = state + (size_t)half * a.state_words;
     uint32_t *summ = bm + a.bitmap_words;
-    int32_t *ring = (int32_t *)(smem_dyn + (size_t)2 * a.state_words) + (size_t)half * a.ring_size;
-    for (int w = tid; w < 2 * a.state_words; w += BLOCK) smem_dyn[w] = 0u;
+    int32_t *ring = (int32_t *)(GBM ? smem_dyn : smem_dyn + (size_t)2 * a.state_words) + (size_t)half * a.ring_size;
+    for (int w = tid; w < 2 * a.state_words; w += BLOCK) state[w] = 0u;
     if (gtid == 0) {
         sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0;
         sh.stamp = nullptr;   // counts only: no lists, no stamps
-        sh.chain_s0 = 0; sh.chain_len = 0; sh.chain_idx = 0; sh.chain_total = 0;
+        sh.chain_s0 = 0; sh.chain_len = 0; sh.chain_total = 0;
         for (int q = 0; q < 8; q++) sh.prof[q] = 0;
         sh.nsrc = sh.nreuse = 0;
+        sh.tailc[0] = sh.tailc[1] = sh.tailc[2] = 0;
+        sh.fetch[0] = sh.fetch[1] = sh.fetch[2] = 0;
+        sh.win_lo = sh.win_hi = 0;
     }
     const Frontier fr{ring, a.queue + ((int64_t)blockIdx.x * 2 + half) * a.qcap, a.qcap, a.status,
                       a.ring_size};
@@ -122,13 +128,14 @@ __global__ void __maxnreg__(64) serve_kernel(ServeArgs sa)
         const ServePiece piece =
             load_cg(sa.pieces + (unsigned long long)s_class * sa.piece_cap + (pc % (long long)sa.piece_cap));
         const MatDesc md = load_cg(sa.slots + piece.slot);
-        run_piece<BLOCK, true, true, false>(a, md, md.g[half], half, piece.s_lo, piece.s_hi, 1, bm, summ, fr, sh,
+        run_piece<BLOCK, true, true, GBM>(a, md, md.g[half], half, piece.s_lo, piece.s_hi, 1, bm, summ, fr, sh,
                                      pair_flag, half, gtid, bar, acc);
         {
             const int clo = sh.chain_lo, chi = sh.chain_hi;
             clear_range<GT>(bm, summ, clo, chi, gtid);
             __syncthreads();
-            if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0; }
+            // the next piece may be another request: no seeding window yet
+            if (gtid == 0) { sh.chain_lo = INT32_MAX; sh.chain_hi = -1; sh.hcount = 0; sh.win_lo = sh.win_hi = 0; }
         }
         if (tid == 0) {
             __threadfence();

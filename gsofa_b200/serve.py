@@ -37,7 +37,49 @@ from .matgen import Graph
 class Request:
     rid: int
     arrival_s: float          # offset from the start of the stream
-    graph: Graph
+    graph: object             # a Graph, or a PendingGraph still being generated
+
+
+class PendingGraph:
+    """A request's matrix that a process pool is still generating."""
+
+    def __init__(self, async_result):
+        self._r = async_result
+        self._g = None
+
+    def ready(self) -> bool:
+        return self._g is not None or self._r.ready()
+
+    def get(self) -> Graph:
+        if self._g is None:
+            self._g = self._r.get()
+            self._r = None
+        return self._g
+
+
+class LazyStream:
+    """Generates the matrices of a long request stream in a process pool, in
+    arrival order and at most `ahead` at a time, so a stream of thousands of
+    large requests needs neither the memory nor the wait of building them all
+    first.  Iterate over it for the requests; a request whose matrix is not
+    ready yet arrives when it is (its latency counts from the later time)."""
+
+    def __init__(self, pool, make: Callable, specs: Sequence, arrivals: Sequence[float], ahead: int = 256):
+        self.pool, self.make, self.specs, self.arrivals = pool, make, list(specs), list(arrivals)
+        self.ahead = ahead
+        self.reqs: List[Request] = []
+        self._next = 0
+
+    def __len__(self):
+        return len(self.specs)
+
+    def top_up(self, consumed: int) -> None:
+        """Keeps `ahead` requests generating beyond the first `consumed`."""
+        while self._next < len(self.specs) and self._next < consumed + self.ahead:
+            i = self._next
+            pg = PendingGraph(self.pool.apply_async(self.make, (self.specs[i],)))
+            self.reqs.append(Request(i, float(self.arrivals[i]), pg))
+            self._next += 1
 
 
 @dataclasses.dataclass
@@ -155,23 +197,48 @@ class ContinuousServer:
         self.max_n = max_n
         self.stall_s = stall_s        # no completion for this long while work is in flight: error
 
-    def run(self, requests: Sequence[Request], clock: Callable[[], float] = time.perf_counter,
-            on_result: Optional[Callable[[Completion], None]] = None) -> Dict:
-        reqs = sorted(requests, key=lambda r: r.arrival_s)
+    def run(self, requests, clock: Callable[[], float] = time.perf_counter,
+            on_result: Optional[Callable[[Completion], None]] = None, keep_graphs: int = -1) -> Dict:
+        """Serves the stream (a list of Requests, or a LazyStream); a
+        request's latency runs from its arrival -- or, when its matrix was
+        still being generated then, from the moment it was ready -- to its
+        result on the host.  keep_graphs >= 0: only the first keep_graphs
+        requests keep their matrices after submission (long streams)."""
+        lazy = requests if isinstance(requests, LazyStream) else None
+        if lazy is not None:
+            lazy.top_up(0)
+            reqs = lazy.reqs
+            total = len(lazy)
+        else:
+            reqs = sorted(requests, key=lambda r: r.arrival_s)
+            total = len(reqs)
         t0 = clock()
         now = lambda: clock() - t0  # noqa: E731
         pending = collections.deque(reqs)
+        nxt = len(reqs)
         waiting: collections.deque = collections.deque()
         inflight: Dict[int, Request] = {}
         started: Dict[int, float] = {}
+        arrived: Dict[int, float] = {}
         done: List[Completion] = []
         last_progress = now()
-        while pending or waiting or inflight:
+        while pending or waiting or inflight or (lazy is not None and nxt < total):
             t = now()
             if inflight and t - last_progress > self.stall_s:
                 raise RuntimeError(f"serving stalled: {len(inflight)} requests in flight, "
                                    f"no completion for {self.stall_s:.0f} s")
+            if lazy is not None:
+                lazy.top_up(len(done) + len(inflight) + len(waiting))
+                while nxt < len(lazy.reqs):
+                    pending.append(lazy.reqs[nxt])
+                    nxt += 1
             while pending and pending[0].arrival_s <= t:
+                r = pending[0]
+                if isinstance(r.graph, PendingGraph):
+                    if not r.graph.ready():
+                        break                      # arrives when its matrix exists
+                    r.graph = r.graph.get()
+                arrived[r.rid] = max(r.arrival_s, t)
                 waiting.append(pending.popleft())
             # admit waiting requests in arrival order while they fit
             while waiting:
@@ -183,7 +250,7 @@ class ContinuousServer:
                     self.server.drain()
                     res = self.oversize(r.graph)
                     waiting.popleft()
-                    c = Completion(r.rid, r.arrival_s, st, now(), res)
+                    c = Completion(r.rid, arrived.pop(r.rid, r.arrival_s), st, now(), res)
                     done.append(c)
                     if on_result:
                         on_result(c)
@@ -192,20 +259,24 @@ class ContinuousServer:
                 if rid is None:
                     break
                 waiting.popleft()
+                if 0 <= keep_graphs <= r.rid:
+                    r.graph = None                 # uploaded: the host copy can go
                 inflight[rid] = r
                 started[rid] = st
             for rid in self.server.poll():
                 last_progress = now()
                 res = self.server.result(rid)
                 r = inflight.pop(rid)
-                c = Completion(r.rid, r.arrival_s, started.pop(rid), now(), res)
+                c = Completion(r.rid, arrived.pop(r.rid, r.arrival_s), started.pop(rid), now(), res)
                 done.append(c)
                 if on_result:
                     on_result(c)
             if not waiting and inflight:
                 time.sleep(self.poll_interval)
             elif not inflight and not waiting and pending:
-                time.sleep(max(0.0, min(pending[0].arrival_s - now(), 0.05)))
+                time.sleep(max(0.0005, min(pending[0].arrival_s - now(), 0.05)))
+            elif not inflight and not waiting and not pending:
+                time.sleep(0.001)                  # the next matrix is still being generated
         lat = np.array([c.latency_s for c in done])
         span = max(c.done_s for c in done) - min(c.arrival_s for c in done) if done else 0.0
         report = {

@@ -95,7 +95,10 @@ typedef struct gsofa_params {
                                    (a contiguous partition, see
                                    gsofa_partition_lines; [n, n) is empty);
                                    reuse and the pattern stay available;
-                                   per-line outputs of other lines are zero   */
+                                   per-line outputs of other lines are zero;
+                                   no supernode partition is formed from part
+                                   of the lines (n_supernodes = 0; see
+                                   gsofa_supernodes_from_lines)               */
 } gsofa_params;
 
 #define GSOFA_FLAG_NO_DOWNLOAD 0x1 /* keep per-line arrays on the device only */
@@ -106,6 +109,10 @@ typedef struct gsofa_params {
 #define GSOFA_FLAG_GLOBAL_STATE 0x8 /* keep every traversal's visited bitmap
                                       in global memory (L2): many small
                                       traversals per SM, any n              */
+#define GSOFA_FLAG_DIRECT_HOST 0x20 /* gsofa_symbfact_ranges into host memory:
+                                      the kernel writes the lists there
+                                      itself (no device pool; slower than the
+                                      default staging through device memory) */
 #define GSOFA_FLAG_SHARED_STATE 0x10 /* keep them in shared memory (at most
                                       two per SM; GSOFA_ERR_UNSUPPORTED when
                                       they do not fit).  Neither flag: shared
@@ -237,9 +244,12 @@ void gsofa_result_free(gsofa_result *r);
  * matrices).  No compaction pass runs.
  *
  * `pool` is either device memory on ctx's device or page-locked host memory
- * (cudaHostAlloc, cudaHostRegister): then the lists travel to the host while
- * the traversals run, so the pattern needs no device memory of its own and
- * may be larger than the device.  pool_capacity counts int32 entries.  When
+ * (cudaHostAlloc, cudaHostRegister).  A host pool is staged through a device
+ * pool of the same size when half the context's budget holds it, and copied
+ * at full PCIe speed; otherwise (or with GSOFA_FLAG_DIRECT_HOST) the kernel
+ * writes the lists into host memory while the traversals run, so the pattern
+ * needs no device memory and may be larger than the device.  pool_capacity
+ * counts int32 entries.  When
  * it is too small the call returns GSOFA_ERR_QUEUE_OVERFLOW with
  * out[i].pool_used set to the entries the job needs.  The other result
  * fields are as for gsofa_symbfact.  Results of a device pool can feed
@@ -357,8 +367,7 @@ typedef struct gsofa_server gsofa_server;
 
 typedef struct gsofa_server_config {
     int32_t device;
-    int32_t max_n;              /* largest request; 0: the largest the paired
-                                   kernel's shared memory holds             */
+    int32_t max_n;              /* largest request; 0: see flags            */
     int64_t mem_budget_bytes;   /* device bytes the server may hold; 0: 90%
                                    of the free memory                       */
     int32_t max_supernode_size; /* as in gsofa_params                       */
@@ -370,6 +379,11 @@ typedef struct gsofa_server_config {
                                    itself when nothing is in flight);
                                    0: 30 s                                  */
     int32_t max_n_out;          /* set by gsofa_server_create: the limit    */
+    int32_t flags;              /* GSOFA_FLAG_SHARED_STATE: bitmaps in shared
+                                   memory (two traversals per SM, n up to
+                                   ~800K); default (or _GLOBAL_STATE): in
+                                   global memory, six traversals per SM, max_n
+                                   defaults to 1,048,576                    */
 } gsofa_server_config;
 
 gsofa_status gsofa_server_create(gsofa_server **srv, gsofa_server_config *cfg);

@@ -46,16 +46,17 @@ MATS = [bundled, lambda: matgen.grid3d(16, ordering="nd", drop_frac=0.1, seed=3)
         lambda: matgen.powerlaw(1500, seed=9), lambda: random_graph(400, 0.02, 7)]
 
 
-@pytest.mark.parametrize("where", ["host", "device"])
+@pytest.mark.parametrize("where", ["host", "host-direct", "device"])
 def test_ranges_form_matches_oracle(ctx, where):
     for make in MATS:
         g = make()
         ref = oracle.symbfact(g.beg, g.end, g.adj, max_supernode_size=8)
         need = int(ref["u_idx"].size + ref["l_idx"].size)
         m = ctx.upload(g)
-        if where == "host":
+        if where.startswith("host"):
             pool = _pinned(need)
-            r = ctx.symbfact_ranges(m, pool, max_supernode_size=8)
+            flags = gsofa_b200.FLAG_DIRECT_HOST if where == "host-direct" else 0
+            r = ctx.symbfact_ranges(m, pool, max_supernode_size=8, flags=flags)
             host_pool = pool
         else:
             pool = torch.full((max(need, 1),), -1, dtype=torch.int32, device="cuda")

@@ -18,12 +18,15 @@ def _same(a, b, where):
     assert np.array_equal(a.sn_start, b.sn_start), where
 
 
-def test_stream_server_matches_standalone():
+@pytest.mark.parametrize("flags", [0, gsofa_b200.FLAG_SHARED_STATE])
+def test_stream_server_matches_standalone(flags):
+    """Both kernel forms: bitmaps in global memory (default, six traversals
+    per SM) and in shared memory (two per SM)."""
     reqs = serve.make_stream(40, 200, 6000, rate_hz=2000.0, seed=21, build=matgen.make)
     reqs.append(serve.Request(len(reqs), reqs[-1].arrival_s, bundled()))
     reqs.append(serve.Request(len(reqs), reqs[-1].arrival_s, random_graph(300, 0.02, 4)))
     with gsofa_b200.Context(0) as ctx, gsofa_b200.StreamServer(0, mem_budget_bytes=8 << 30,
-                                                              max_supernode_size=16) as srv:
+                                                              max_supernode_size=16, flags=flags) as srv:
         out = serve.ContinuousServer(srv).run(reqs)
         rep = out["report"]
         assert rep["requests"] == len(reqs) and rep["p50_ms"] <= rep["p99_ms"]
