@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--serve-count", type=int, default=120, help="requests in the serving stream")
     ap.add_argument("--serve-nmax", type=int, default=1_000_000, help="largest n of the serving stream")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate (1/s)")
+    ap.add_argument("--serve-default", type=int, default=240,
+                    help="requests of the short serving stream measured beside the default line (0: skip)")
+    ap.add_argument("--serve-default-rate", type=float, default=60.0, help="its Poisson rate (1/s)")
     ap.add_argument("--serve-compare", type=int, default=120,
                     help="first requests served again, continuously and one at a time, for the comparison")
     ap.add_argument("--side", type=int, default=80, help="grid side of the nd3d workload")
@@ -77,6 +80,8 @@ def parse():
     ap.add_argument("--partitions", type=int, default=4,
                     help="one GPU: also time the matrix as this many work-predicted line ranges, "
                          "one after another (the multi-GPU split, measured on one device; 0: skip)")
+    ap.add_argument("--host-pool-gb", type=float, default=16.0,
+                    help="circuit workload: host buffer the pattern streams into, range by range (0: skip)")
     ap.add_argument("--pattern", type=int, default=-1,
                     help="materialize the L+U pattern (-1: yes except for the circuit workload, "
                          "whose pattern does not fit in memory)")
@@ -386,71 +391,80 @@ def _make_graph(spec):
     return matgen.make(kind, n, seed)
 
 
-def serve_main(args):
-    """The serving stream: seeded Poisson arrivals of mixed-kind requests with
-    n log-uniform in [1,000, n_max], served by continuous batching on the
-    persistent serving kernel under a 120 GB admission budget.  Long streams
-    (the 10,000-request configuration) are generated in a process pool while
-    they are served.  The first --serve-compare requests are then served
-    again, continuously and one request per launch, for the comparison; the
-    results must be identical request by request."""
+def serving_run(ctx, count, nmax, rate, compare, pool_procs=16):
+    """Continuous batching on the persistent serving kernel over a seeded
+    Poisson stream of `count` mixed-kind requests (n log-uniform in [1,000,
+    nmax]) under a 120 GB admission budget, the matrices generated in a
+    process pool while they are served.  The first `compare` requests are then
+    served again, continuously and one request per launch, for the
+    comparison; the results must be identical request by request."""
     import multiprocessing as mp
-    import torch
     import gsofa_b200
     from gsofa_b200 import matgen, serve
 
-    spec = matgen.mixed_spec(args.serve_count, 1000, args.serve_nmax, matgen.SEEDS["serve"])
+    spec = matgen.mixed_spec(count, 1000, nmax, matgen.SEEDS["serve"])
     rng = np.random.default_rng(matgen.SEEDS["serve"] + 1)
-    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, size=len(spec)))
-    k = min(args.serve_compare, len(spec))
-    pool = mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1))
-    torch.cuda.set_device(0)
-    ctx = gsofa_b200.Context(0)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(spec)))
+    k = min(compare, len(spec))
+    pool = mp.get_context("spawn").Pool(min(pool_procs, os.cpu_count() or 1))
     params = gsofa_b200.Params.default(want_pattern=0)
     srv = gsofa_b200.StreamServer(0, mem_budget_bytes=120 << 30)
     oversize = lambda g: ctx.symbfact(ctx.upload(g), params)  # noqa: E731
     cs = serve.ContinuousServer(srv, oversize=oversize, max_n=srv.max_n)
-    # warm up on a few small requests
     warm = [serve.Request(-1 - i, 0.0, matgen.make("grid3d", 2000, i)) for i in range(4)]
     cs.run(warm)
     stream = serve.LazyStream(pool, _make_graph, spec, arrivals, ahead=256)
     with ClockSampler(0) as clk:
         full = cs.run(stream, keep_graphs=k)
     srv.drain()
-    # the comparison on the first k requests (same arrival times)
     sub = [serve.Request(r.rid, r.arrival_s, r.graph) for r in stream.reqs[:k]]
     cont = cs.run(sub)
     srv.drain()
+    max_n = srv.max_n
     srv.close()
     single = serve.one_at_a_time(ctx, sub, params)
     pool.close()
     by_id = {c.rid: c for c in full["completions"]}
+    same = True
     for a, b in zip(cont["completions"], single["completions"]):
         c = by_id[a.rid]
-        assert (a.result.fill_count, a.result.nnz_lu, a.result.n_supernodes) == \
-               (b.result.fill_count, b.result.nnz_lu, b.result.n_supernodes) == \
-               (c.result.fill_count, c.result.nnz_lu, c.result.n_supernodes)
-        assert np.array_equal(a.result.u_row_count, b.result.u_row_count)
-        assert np.array_equal(a.result.sn_start, c.result.sn_start)
-    rep = full["report"]
+        same &= (a.result.fill_count, a.result.nnz_lu, a.result.n_supernodes) == \
+                (b.result.fill_count, b.result.nnz_lu, b.result.n_supernodes) == \
+                (c.result.fill_count, c.result.nnz_lu, c.result.n_supernodes)
+        same &= bool(np.array_equal(a.result.u_row_count, b.result.u_row_count))
+        same &= bool(np.array_equal(a.result.sn_start, c.result.sn_start))
+    return {"workload": f"serve_{len(spec)}_poisson_{rate:g}hz_n1k-{nmax}", "requests": len(spec),
+            "admission_budget_gb": 120, "pattern": "counts only", "seed": matgen.SEEDS["serve"],
+            "serving": full["report"],
+            "comparison": {"requests": k, "continuous": cont["report"], "one_at_a_time": single["report"]},
+            "results_identical": bool(same), "serving_kernel_max_n": max_n, "clocks": clk.summary(),
+            "generation": "process pool, in arrival order, while serving (a request arrives when both "
+                          "its time and its matrix have come)"}
+
+
+def serve_main(args):
+    """The serving configuration as its own line: --serve-count requests
+    (10,000 for the full stream), n up to --serve-nmax, at --serve-rate."""
+    import torch
+    import gsofa_b200
+    torch.cuda.set_device(0)
+    ctx = gsofa_b200.Context(0)
+    out = serving_run(ctx, args.serve_count, args.serve_nmax, args.serve_rate, args.serve_compare)
+    rep = out["serving"]
     line = {
         "metric": "nnz(L+U)/s", "value": rep["nnz_lu_per_s"], "unit": "nnz/s", "n_gpus": 1,
         "steps": 1, "warmup": 1, "ms_per_step": rep["span_s"] * 1000.0, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator)",
-        "config": {"workload": f"serve_{len(spec)}_poisson_{args.serve_rate:g}hz_n1k-{args.serve_nmax}",
-                   "requests": len(spec), "admission_budget_gb": 120, "pattern": "counts only",
-                   "seed": matgen.SEEDS["serve"], "generation": "process pool, in arrival order, "
-                   "while serving (a request arrives when both its time and its matrix have come)"},
-        "serving": rep,
-        "comparison": {"requests": k, "continuous": cont["report"], "one_at_a_time": single["report"],
-                       "results_identical": True},
-        "serving_kernel_max_n": cs.max_n,
+        "config": {k: out[k] for k in ("workload", "requests", "admission_budget_gb", "pattern", "seed",
+                                       "generation")},
+        "serving": rep, "comparison": out["comparison"], "results_identical": out["results_identical"],
+        "serving_kernel_max_n": out["serving_kernel_max_n"],
         "factorizations_per_s": rep["factorizations_per_s"],
-        "clocks": clk.summary(), "gpu_launches": None,
+        "clocks": out["clocks"], "gpu_launches": None,
     }
     print(json.dumps(line), flush=True)
     ctx.close()
-    return 0
+    return 0 if out["results_identical"] else 1
 
 
 def _sha(a, dtype) -> str:
@@ -498,6 +512,24 @@ def check_parity(g, workload_name, res, cs, want_pattern):
                          "n_supernodes"], "mismatched": gm}
     out["mismatches"] = bad
     return out
+
+
+def link_gbs(torch, stream, nbytes=1 << 30):
+    """Device-to-host copy rate of this box's host link: 1 GiB from device
+    memory into page-locked host memory, best of three, CUDA events."""
+    src = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    dst = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    best = None
+    for _ in range(3):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dst.copy_(src, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    return nbytes / (best / 1000.0) / 1e9
 
 
 def _params(gsofa_b200, args, **kw):
@@ -588,6 +620,66 @@ def batched_vs_plain(args, ctx, torch, stream, gsofa_b200):
             "plain_factorizations_per_s": len(mats) / (t_plain / 1000.0),
             "graph": "one persistent launch replayed from a CUDA graph", "results_identical": same,
             "per_kind": per_kind}
+
+
+def streamed_pattern(args, ctx, m, torch, gsofa_b200, g):
+    """The whole pattern of a matrix whose pattern no device holds (the
+    659,033-line power-law matrix: ~1.2e11 entries, ~480 GB), produced in
+    contiguous line ranges, each written as begin/end ranges into one
+    page-locked host buffer of --host-pool-gb while its traversals run (the
+    staged form: full blocks leave the device during the kernel).  The ranges
+    are cut from the exact per-line counts of a counts-only run so that each
+    fills most of the buffer.  A consumer would take each range's lists before
+    the next range overwrites the buffer; here every range's per-line counts
+    are checked against the counts-only run and its lists against the oracle
+    on sampled lines.  Timed end to end (device events around all ranges,
+    copies included)."""
+    import oracle
+    counts = ctx.symbfact(m, want_pattern=0)
+    per_line = counts.u_row_count.astype(np.int64) + counts.l_col_count.astype(np.int64)
+    cum = np.concatenate([[0], np.cumsum(per_line)])
+    need = int(cum[-1])
+    cap = int(args.host_pool_gb * (1 << 30) // 4)
+    if per_line.max() > cap:
+        raise ValueError("one line's lists exceed the host buffer")
+    cuts = [0]
+    while cuts[-1] < g.n:
+        lo = cuts[-1]
+        hi = int(np.searchsorted(cum, cum[lo] + cap, side="right")) - 1
+        cuts.append(max(lo + 1, min(hi, g.n)))
+    hpool = torch.empty(cap, dtype=torch.int32).pin_memory().numpy()
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    bad, checked, written, kms, total_ms = 0, 0, 0, 0.0, 0.0
+    rng = np.random.default_rng(7)
+    for k in range(len(cuts) - 1):
+        lo, hi = cuts[k], cuts[k + 1]
+        p = gsofa_b200.Params.default(line_lo=lo, line_hi=hi)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        r = ctx.symbfact_ranges(m, hpool, p)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        written += r.pool_used
+        kms += r.kernel_ms
+        if not (np.array_equal(r.u_row_count[lo:hi], counts.u_row_count[lo:hi]) and
+                np.array_equal(r.l_col_count[lo:hi], counts.l_col_count[lo:hi])):
+            bad += 1
+        src = np.unique(rng.integers(lo, hi, size=3).astype(np.int32))
+        for pass_, row, cnt in ((0, r.u_row, counts.u_row_count), (1, r.l_col, counts.l_col_count)):
+            rp, ri = oracle.lists(g.beg, g.end, g.adj, pass_, src, cnt)
+            for i, s_ in enumerate(src.tolist()):
+                checked += 1
+                if not np.array_equal(row(s_), ri[rp[i]:rp[i + 1]]):
+                    bad += 1
+    return {"entries": int(written), "expected_entries": need, "ranges": len(cuts) - 1,
+            "host_pool_gb": args.host_pool_gb, "ms": total_ms, "kernel_ms": kms,
+            "value": (written + g.n) / (total_ms / 1000.0), "unit": "nnz/s",
+            "d2h_bytes": int(4 * written), "lists_checked": checked, "mismatches": bad,
+            "note": "the whole pattern produced in host memory range by range, each range's lists "
+                    "streamed out of the device while its traversals ran"}
 
 
 def sharded_main(args, world, rank, local):
@@ -882,7 +974,10 @@ def main():
             d2h += 4 * out.pool_used + 2 * 8 * g.n
         e2e = {"value": world * k2 * nnz_lu / (te / 1000.0), "unit": "nnz/s", "steps": k2,
                "ms_per_step": te / k2, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "form": form, "host_phases": phases, "kernel_ms": out.kernel_ms}
+               "form": form, "host_phases": phases, "kernel_ms": out.kernel_ms,
+               # the step moves d2h bytes over PCIe: their rate against the
+               # host link's copy rate shows how close e2e is to its bound
+               "d2h_gbs": d2h / (te / k2 / 1000.0) / 1e9, "d2h_link_gbs": link_gbs(torch, stream)}
         if want_pattern:
             # the same steps for a consumer of the supernodal structure: the
             # pattern stays on the device and only the per-supernode index
@@ -942,6 +1037,15 @@ def main():
     batched = None
     if world == 1 and args.batch_count > 0 and args.workload == "nd3d":
         batched = batched_vs_plain(args, ctx, torch, stream, gsofa_b200)
+    serving = None
+    if world == 1 and args.workload == "nd3d" and args.serve_default > 0:
+        # a short serving stream beside the headline line (the 10,000-request
+        # stream is its own run: --workload serve --serve-count 10000)
+        serving = serving_run(ctx, args.serve_default, 200_000, args.serve_default_rate,
+                              min(args.serve_default, 120))
+    streamed = None
+    if world == 1 and args.workload == "circuit" and args.host_pool_gb > 0:
+        streamed = streamed_pattern(args, ctx, m, torch, gsofa_b200, g)
 
     cpu = None
     parity = None
@@ -972,6 +1076,8 @@ def main():
             "other_forms": forms,
             "split_on_one_gpu": split,
             "batched": batched,
+            "pattern_streamed_to_host": streamed,
+            "serving": serving,
             "e2e": e2e,
             "roofline": roof,
             "cpu_baseline": cpu,
@@ -985,6 +1091,9 @@ def main():
         dist.destroy_process_group()
     if parity is not None and parity["mismatches"]:
         print(f"parity check failed: {parity}", file=sys.stderr)
+        return 1
+    if streamed is not None and streamed["mismatches"]:
+        print(f"streamed pattern check failed: {streamed}", file=sys.stderr)
         return 1
     return 0
 

@@ -43,6 +43,7 @@ FLAG_GRAPH = 0x4
 FLAG_GLOBAL_STATE = 0x8    # visited bitmaps in global memory (many traversals per SM, any n)
 FLAG_SHARED_STATE = 0x10   # visited bitmaps in shared memory (at most two per SM)
 FLAG_DIRECT_HOST = 0x20    # symbfact_ranges into host memory: the kernel writes it directly
+FLAG_WIDE_REGS = 0x40      # paired passes in 512-thread CTAs with up to 128 registers a thread
 
 
 class GsofaError(RuntimeError):

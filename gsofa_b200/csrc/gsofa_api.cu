@@ -109,7 +109,7 @@ struct gsofa_ctx {
     DevBuf matinfo;
     GraphCache graph;         // last captured job (GSOFA_FLAG_GRAPH)
     // launch shapes already sized: (block, bitmap words) -> (ring, CTAs/SM)
-    struct Shape { int block; int32_t words; bool paired; bool gbm; int ring; int occ; };
+    struct Shape { int block; int32_t words; bool paired; bool gbm; bool wide; int ring; int occ; };
     std::vector<Shape> shapes;
 
     void *grow(DevBuf &b, size_t bytes)
@@ -184,6 +184,7 @@ struct gsofa_matrix {
     int32_t *d_gptr = nullptr, *d_gadj = nullptr;
     int32_t *d_tptr = nullptr, *d_tadj = nullptr;
     int32_t *d_orig_up = nullptr, *d_orig_lo = nullptr, *d_rawdeg = nullptr;
+    int4 *d_gslot = nullptr, *d_tslot = nullptr;   // 32-byte row slots of G and G^T
     void *slab = nullptr;          // one device allocation holding all of the above
     size_t slab_bytes = 0;
     uint64_t orig_up = 0, orig_lo = 0;
@@ -224,15 +225,16 @@ int pick_block(int32_t max_n)
     return 512;
 }
 
-template <int BLOCK, bool PAIRED, bool GBM>
+template <int BLOCK, bool PAIRED, bool GBM, int MINB = (BLOCK >= 1024 ? 1 : 1024 / BLOCK)>
 void *factor_fn()
 {
-    return (void *)factor_kernel<BLOCK, PAIRED, GBM>;
+    return (void *)factor_kernel<BLOCK, PAIRED, GBM, MINB>;
 }
 
 // The factorization kernel for a launch shape: threads per CTA, the two
-// passes side by side (paired), the visited bitmaps in global memory (gbm).
-void *factor_kernel_for(int block, bool paired, bool gbm = false)
+// passes side by side (paired), the visited bitmaps in global memory (gbm),
+// registers budgeted for one CTA per SM (wide: the 512-thread paired form).
+void *factor_kernel_for(int block, bool paired, bool gbm = false, bool wide = false)
 {
     if (gbm) {
         switch (block) {
@@ -242,10 +244,12 @@ void *factor_kernel_for(int block, bool paired, bool gbm = false)
         default: return nullptr;
         }
     }
+    if (wide) return (block == 512 && paired) ? factor_fn<512, true, false, 1>() : nullptr;
     switch (block) {
     case 128: return paired ? nullptr : factor_fn<128, false, false>();
     case 256: return paired ? factor_fn<256, true, false>() : factor_fn<256, false, false>();
     case 512: return paired ? factor_fn<512, true, false>() : factor_fn<512, false, false>();
+    case 768: return paired ? factor_fn<768, true, false>() : factor_fn<768, false, false>();
     case 1024: return paired ? factor_fn<1024, true, false>() : factor_fn<1024, false, false>();
     default: return nullptr;
     }
@@ -354,8 +358,8 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         md[i].n = mats[i]->n;
         md[i].pad = 0;
         md[i].line_base = L;
-        md[i].g[0] = PassGraph{mats[i]->d_gptr, mats[i]->d_gadj};
-        md[i].g[1] = PassGraph{mats[i]->d_tptr, mats[i]->d_tadj};
+        md[i].g[0] = PassGraph{mats[i]->d_gptr, mats[i]->d_gadj, mats[i]->d_gslot};
+        md[i].g[1] = PassGraph{mats[i]->d_tptr, mats[i]->d_tadj, mats[i]->d_tslot};
         md[i].rawdeg = mats[i]->d_rawdeg;
         L += mats[i]->n;
         max_n = std::max(max_n, mats[i]->n);
@@ -379,8 +383,23 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
                      (!(p.flags & GSOFA_FLAG_SHARED_STATE) &&
                       ((want_pair && pair_smem > ctx->smem_optin) || single_smem > ctx->smem_optin));
     const bool paired = want_pair && (gbm || pair_smem <= ctx->smem_optin);
-    int block = p.block_size ? p.block_size : (gbm ? (paired ? 256 : 128) : pick_block(max_n) * (paired ? 2 : 1));
-    void *kfn = factor_kernel_for(block, paired, gbm);
+    // Shared-state pairs past 8K lines hold one CTA per SM (1024 threads at
+    // 64 registers fill its register file): 768 threads with up to 80
+    // registers a thread run without register spills, measured faster than
+    // 1024 threads on the 80^3 stencil with and without the pattern.  (512
+    // threads with up to 128 registers -- GSOFA_FLAG_WIDE_REGS -- are faster
+    // still on latency-bound matrices, counts only, but slower where large
+    // frontiers keep many warps busy, such as dense-fill power-law matrices.)
+    const bool wide = (p.flags & GSOFA_FLAG_WIDE_REGS) != 0;
+    int block = p.block_size;
+    if (wide) block = 512;
+    if (!block) {
+        if (gbm) block = paired ? 256 : 128;
+        else if (paired && max_n > 8192) block = 768;
+        else block = pick_block(max_n) * (paired ? 2 : 1);
+    }
+    if (wide && (!paired || gbm)) return GSOFA_ERR_INVALID_INPUT;
+    void *kfn = factor_kernel_for(block, paired, gbm, wide);
     if (!kfn) return GSOFA_ERR_INVALID_INPUT;
     const int NS = paired ? 2 : 1;
     int lanes = p.threads_per_source ? p.threads_per_source : 1;
@@ -400,7 +419,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     size_t smem = 0;
     bool cached = false;
     for (const auto &sh : ctx->shapes)
-        if (sh.block == block && sh.words == bitmap_words && sh.paired == paired && sh.gbm == gbm) {
+        if (sh.block == block && sh.words == bitmap_words && sh.paired == paired && sh.gbm == gbm && sh.wide == wide) {
             ring = sh.ring; occ = sh.occ; cached = true;
         }
     if (cached) {
@@ -416,7 +435,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
             if (o > occ) { occ = o; ring = cand; smem = sm; }
         }
         if (occ <= 0) return GSOFA_ERR_UNSUPPORTED;
-        ctx->shapes.push_back({block, bitmap_words, paired, gbm, ring, occ});
+        ctx->shapes.push_back({block, bitmap_words, paired, gbm, wide, ring, occ});
     }
     int per_sm = p.ctas_per_sm > 0 ? std::min(p.ctas_per_sm, occ) : occ;
     int grid = per_sm * ctx->sm_count;
@@ -445,8 +464,10 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     // low-numbered sources, so the launch's tail stays short
     int chunk = p.src_chunk;
     if (chunk <= 0) {
-        const int64_t lines = line_range ? (int64_t)(range_hi - range_lo) : L;   // sources per pass
-        const int64_t per = (int64_t)(paired ? 1 : 2) * lines / ((int64_t)8 * grid);
+        // a line range keeps the pieces the whole matrix would have: smaller
+        // ones would start more traversals afresh, and a fresh start costs
+        // most in the separator lines a range of the last lines holds
+        const int64_t per = (int64_t)(paired ? 1 : 2) * L / ((int64_t)8 * grid);
         chunk = reuse ? (int)std::min<int64_t>(512, std::max<int64_t>(32, per)) : 1;
     }
 
@@ -1071,7 +1092,8 @@ gsofa_status gsofa_upload(gsofa_ctx *c, int32_t n, int64_t nnz, const int32_t *b
             auto al = [](size_t b) { return (b + 255) / 256 * 256; };
             const size_t pb = al((size_t)(n + 1) * 4), lb = al(nb);
             const size_t ab = al((size_t)std::max<int64_t>(nnz, 1) * 4);
-            const size_t total = 2 * pb + 3 * lb + 2 * ab;
+            const size_t sb = al((size_t)std::max<int32_t>(n, 1) * 32);
+            const size_t total = 2 * pb + 3 * lb + 2 * ab + 2 * sb;
             char *q = (char *)c->slab_take(total, &m->slab_bytes);
             m->slab = q;
             m->d_gptr = (int32_t *)q; q += pb;
@@ -1079,6 +1101,8 @@ gsofa_status gsofa_upload(gsofa_ctx *c, int32_t n, int64_t nnz, const int32_t *b
             m->d_orig_up = (int32_t *)q; q += lb;
             m->d_orig_lo = (int32_t *)q; q += lb;
             m->d_rawdeg = (int32_t *)q; q += lb;
+            m->d_gslot = (int4 *)q; q += sb;
+            m->d_tslot = (int4 *)q; q += sb;
             m->d_gadj = (int32_t *)q; q += ab;
             m->d_tadj = (int32_t *)q;
         }
@@ -1146,6 +1170,10 @@ gsofa_status gsofa_upload(gsofa_ctx *c, int32_t n, int64_t nnz, const int32_t *b
         GS_CUDA(cudaMemcpyAsync(d_tcur, m->d_tptr, (size_t)(n + 1) * 4, cudaMemcpyDeviceToDevice, st));
         if (n > 0) {
             upload_fill_kernel<<<ugrid, ub, 0, st>>>(u, m->d_gptr, m->d_gadj, d_tcur, m->d_tadj);
+            GS_CUDA(cudaGetLastError());
+            const int sgrid = (int)std::min<int64_t>(((int64_t)n + 255) / 256, (int64_t)c->sm_count * 8);
+            slot_fill_kernel<<<sgrid, 256, 0, st>>>(n, m->d_gptr, m->d_gadj, m->d_gslot);
+            slot_fill_kernel<<<sgrid, 256, 0, st>>>(n, m->d_tptr, m->d_tadj, m->d_tslot);
             GS_CUDA(cudaGetLastError());
         }
         GS_CUDA(cudaStreamSynchronize(st));
@@ -1444,6 +1472,7 @@ size_t gsofa_predict_scratch_bytes(const gsofa_ctx *c, int32_t n, int64_t nnz,
     b += L * (2 * 4 + 2 + 2 * 8 + 4 + 1 + 4);   // cnt, nxt, poff, lrow, snind, sn list
     b += 2 * (L + 1) * 8;                       // gptr
     b += (size_t)(n + 1) * 8 + (size_t)nnz * 8; // G and G^T
+    b += (size_t)n * 64;                        // their 32-byte row slots
     if (p.want_pattern)                         // chain stamps, two traversals a CTA
         b += grid * 2 * ((size_t)(n + 4095) / 4096 * 4096) * 2;
     return b;
@@ -1805,6 +1834,8 @@ extern "C" gsofa_status gsofa_symbfact_counts_noalloc(int device, void *cuda_str
         int32_t *orig_up = lay.take<int32_t>(n);
         int32_t *orig_lo = lay.take<int32_t>(n);
         int32_t *rawdeg = lay.take<int32_t>(n);
+        int4 *gslot = lay.take<int4>((size_t)2 * n);
+        int4 *tslot = lay.take<int4>((size_t)2 * n);
         int64_t *tsum = lay.take<int64_t>(2 * scan_tiles);
         unsigned long long *ucounts = lay.take<unsigned long long>(8);
         int32_t *cnt = lay.take<int32_t>(2 * L);
@@ -1858,14 +1889,16 @@ extern "C" gsofa_status gsofa_symbfact_counts_noalloc(int device, void *cuda_str
         if ((int64_t)hc[2] > nnz || (int64_t)hc[3] > nnz) return GSOFA_ERR_INVALID_INPUT;
         GS_CUDA(cudaMemcpyAsync(tcur, tptr, (size_t)(n + 1) * 4, cudaMemcpyDeviceToDevice, st));
         upload_fill_kernel<<<ugrid, 256, 0, st>>>(u, gptr_g, gadj, tcur, tadj);
+        slot_fill_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, gptr_g, gadj, gslot);
+        slot_fill_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, tptr, tadj, tslot);
         GS_CUDA(cudaGetLastError());
 
         // ---- factorization (counts only) ----
         MatDesc md{};
         md.n = n;
         md.line_base = 0;
-        md.g[0] = PassGraph{gptr_g, gadj};
-        md.g[1] = PassGraph{tptr, tadj};
+        md.g[0] = PassGraph{gptr_g, gadj, gslot};
+        md.g[1] = PassGraph{tptr, tadj, tslot};
         md.rawdeg = rawdeg;
         Range rg{};
         rg.mat = 0;
@@ -2055,7 +2088,8 @@ int64_t server_graph_bytes(int32_t n, int64_t nnz)
 {
     const int64_t a = 256;
     auto r = [&](int64_t b) { return (b + a - 1) / a * a; };
-    return 2 * r(4 * ((int64_t)n + 1)) + 2 * r(4 * std::max<int64_t>(nnz, 1)) + 3 * r(4 * std::max<int32_t>(n, 1));
+    return 2 * r(4 * ((int64_t)n + 1)) + 2 * r(4 * std::max<int64_t>(nnz, 1)) + 3 * r(4 * std::max<int32_t>(n, 1)) +
+           2 * r(32 * std::max<int32_t>(n, 1));
 }
 
 // Upload staging: input copy, degree arrays, scan partials, counters.
@@ -2358,6 +2392,8 @@ gsofa_status gsofa_server_submit(gsofa_server *s, int32_t n, int64_t nnz, const 
         int32_t *orig_up = (int32_t *)take(gb, 4 * (int64_t)n);
         int32_t *orig_lo = (int32_t *)take(gb, 4 * (int64_t)n);
         int32_t *rawdeg = (int32_t *)take(gb, 4 * (int64_t)n);
+        int4 *gslot = (int4 *)take(gb, 32 * (int64_t)n);
+        int4 *tslot = (int4 *)take(gb, 32 * (int64_t)n);
         const int64_t scan_tiles = ((int64_t)n + 1 + 255) / 256 + 1;
         int32_t *d_beg = (int32_t *)take(sb, 4 * (int64_t)n);
         int32_t *d_end = (int32_t *)take(sb, 4 * (int64_t)n);
@@ -2410,14 +2446,19 @@ gsofa_status gsofa_server_submit(gsofa_server *s, int32_t n, int64_t nnz, const 
         r.orig_lo = hc[1];
         GS_CUDA(cudaMemcpyAsync(tcur, tptr, (size_t)(n + 1) * 4, cudaMemcpyDeviceToDevice, st));
         upload_fill_kernel<<<ugrid, 256, 0, st>>>(u, gptr, gadj, tcur, tadj);
+        {
+            const int sgrid = (int)std::min<int64_t>(((int64_t)n + 255) / 256, (int64_t)s->sms * 8);
+            slot_fill_kernel<<<sgrid, 256, 0, st>>>(n, gptr, gadj, gslot);
+            slot_fill_kernel<<<sgrid, 256, 0, st>>>(n, tptr, tadj, tslot);
+        }
         GS_CUDA(cudaGetLastError());
 
         // publish: descriptor, cleared counter, pieces, then the new total
         MatDesc md{};
         md.n = n;
         md.line_base = r.lb;
-        md.g[0] = PassGraph{gptr, gadj};
-        md.g[1] = PassGraph{tptr, tadj};
+        md.g[0] = PassGraph{gptr, gadj, gslot};
+        md.g[1] = PassGraph{tptr, tadj, tslot};
         md.rawdeg = rawdeg;
         GS_CUDA(cudaMemcpyAsync(s->d_slots + r.slot, &md, sizeof(md), cudaMemcpyHostToDevice, st));
         GS_CUDA(cudaMemsetAsync(s->d_done + r.slot, 0, 4, st));

@@ -26,9 +26,16 @@ namespace dev {
 
 namespace cg = cooperative_groups;
 
+// Rows of at most SLOT_NB ids are also kept whole in a 32-byte slot per
+// vertex -- {degree, row offset, up to six ids} -- so expanding a frontier
+// vertex is one L2 round trip instead of two (row bounds, then ids); longer
+// rows take their ids from adj at the slot's offset.
+constexpr int SLOT_NB = 6;
+
 struct PassGraph {
     const int32_t *ptr;  // [n+1]
     const int32_t *adj;  // [ptr[n]]
+    const int4 *slot;    // [2n]: vertex v at slot[2v], slot[2v+1] (or null)
 };
 
 struct MatDesc {
@@ -197,6 +204,13 @@ __device__ __forceinline__ int64_t block_excl_max(int64_t v, int64_t *total,
 // host may rewrite while a persistent kernel runs.
 template <bool CG>
 __device__ __forceinline__ int32_t ld(const int32_t *p)
+{
+    if (CG) return __ldcg(p);
+    return *p;
+}
+
+template <bool CG>
+__device__ __forceinline__ int4 ld4(const int4 *p)
 {
     if (CG) return __ldcg(p);
     return *p;
@@ -522,13 +536,23 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                 if (base >= end) break;
                 const int it = base + lane;
                 int32_t b = 0, d = 0;
+                int4 sl0 = make_int4(0, 0, -1, -1), sl1 = make_int4(-1, -1, -1, -1);
                 if (it < end) {
                     const int32_t v = fr_get(f, it, wstart);
-                    b = ld<CG>(g.ptr + v);
-                    d = ld<CG>(g.ptr + v + 1) - b;
+                    if (g.slot != nullptr) {   // degree, offset and short rows in one 32-byte load
+                        sl0 = ld4<CG>(g.slot + 2 * (int64_t)v);
+                        sl1 = ld4<CG>(g.slot + 2 * (int64_t)v + 1);
+                        d = sl0.x;
+                        b = sl0.y;
+                    } else {
+                        b = ld<CG>(g.ptr + v);
+                        d = ld<CG>(g.ptr + v + 1) - b;
+                    }
                     edges += (unsigned long long)d;
                     if (pass == 0) { xcnt++; einsp += (unsigned long long)ld<CG>(rawdeg + v); }
                 }
+                // the row's ids are in the slot (first step of the id loop)
+                const bool in_slot = g.slot != nullptr && d <= SLOT_NB;
                 unsigned heavy = __ballot_sync(0xffffffffu, d > HEAVY_ROW);
                 while (heavy) {
                     const int src = __ffs(heavy) - 1;
@@ -556,8 +580,14 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
                 const int dmax = __reduce_max_sync(0xffffffffu, dl);
                 for (int k0 = 0; k0 < dmax; k0 += 8) {
                     int32_t buf[8];
+                    if (in_slot) {   // d <= 6 < 8: only this first step has ids
+                        const int32_t sv[SLOT_NB] = {sl0.z, sl0.w, sl1.x, sl1.y, sl1.z, sl1.w};
 #pragma unroll
-                    for (int u = 0; u < 8; u++) buf[u] = (k0 + u < dl) ? ld<CG>(g.adj + b + k0 + u) : -1;
+                        for (int u = 0; u < 8; u++) buf[u] = (u < SLOT_NB && k0 + u < dl) ? sv[u < SLOT_NB ? u : 0] : -1;
+                    } else {
+#pragma unroll
+                        for (int u = 0; u < 8; u++) buf[u] = (k0 + u < dl) ? ld<CG>(g.adj + b + k0 + u) : -1;
+                    }
                     // independent bit tests and sets first, then one enqueue
                     // (warp scan + one shared atomic) for all new low vertices
                     unsigned fresh = 0u;
@@ -914,8 +944,12 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
 // longer bounds how many traversals an SM runs (shared memory holds two
 // bitmaps of at most ~850K lines each), so small CTAs run many traversals per
 // SM side by side, and n is bounded only by device memory.
-template <int BLOCK, bool PAIRED, bool GBM>
-__global__ void __launch_bounds__(BLOCK, (BLOCK >= 1024 ? 1 : 1024 / BLOCK)) factor_kernel(JobArgs a)
+//
+// MINB: resident CTAs per SM the registers are budgeted for (the default
+// fills the SM with 1024 threads; 1 gives a 512-thread CTA up to 128
+// registers a thread, for launches that hold one CTA per SM anyway).
+template <int BLOCK, bool PAIRED, bool GBM, int MINB = (BLOCK >= 1024 ? 1 : 1024 / BLOCK)>
+__global__ void __launch_bounds__(BLOCK, MINB) factor_kernel(JobArgs a)
 {
     constexpr int GT = PAIRED ? BLOCK / 2 : BLOCK;
     constexpr int NS = PAIRED ? 2 : 1;
@@ -1312,6 +1346,20 @@ __global__ void upload_fill_kernel(UploadArgs u, const int32_t *gptr, int32_t *g
             }
             out += __popc(bal);
         }
+    }
+}
+
+// Fills the 32-byte slot of every vertex of one pass graph: {degree, row
+// offset, the first SLOT_NB ids (-1 past the degree)}.
+__global__ void slot_fill_kernel(int32_t n, const int32_t *ptr, const int32_t *adj, int4 *slot)
+{
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t b = ptr[v], d = ptr[v + 1] - b;
+        int32_t x[SLOT_NB];
+#pragma unroll
+        for (int u = 0; u < SLOT_NB; u++) x[u] = u < d ? adj[b + u] : -1;
+        slot[2 * v] = make_int4(d, b, x[0], x[1]);
+        slot[2 * v + 1] = make_int4(x[2], x[3], x[4], x[5]);
     }
 }
 

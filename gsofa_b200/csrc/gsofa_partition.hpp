@@ -26,11 +26,18 @@
 namespace gsofa {
 namespace part {
 
-// Per-traversal and per-list-entry costs (SM cycles, from the factorization
-// kernel's own tallies on the 80^3 nested-dissection matrix: ~7K cycles per
-// source and pass, ~2.6 cycles per list entry).
+// Per-traversal, per-list-entry and per-edge costs (SM cycles, from the
+// factorization kernel's own tallies on the 80^3 nested-dissection matrix:
+// ~7K cycles per source and pass, ~2.6 cycles per list entry, ~3.2 cycles per
+// inspected edge of a traversal that starts afresh).  A traversal starts
+// afresh at the first source of every work piece and then expands all of
+// X(s), whose size is bounded by s's descendants in the elimination tree of
+// A + A^T.  Work pieces are n / (8 x 148) sources long on a 148-SM GPU,
+// between 32 and 512, whether the kernel runs the whole matrix or a range.
 constexpr double kCostPerSource = 7000.0;
 constexpr double kCostPerEntry = 2.6;
+constexpr double kCostPerEdge = 3.2;
+inline double piece_len(int32_t n) { return std::min(512.0, std::max(32.0, (double)n / 1184.0)); }
 
 struct Sym {
     std::vector<int64_t> ptr;   // [n+1]
@@ -182,10 +189,20 @@ inline void partition(int32_t n, const int32_t *beg, const int32_t *end, const i
     const std::vector<int32_t> parent = etree(n, s);
     const std::vector<int32_t> post = postorder(n, parent);
     const std::vector<int64_t> cc = column_counts(n, s, parent, post);
+    // descendants in the elimination tree, with their symmetric degrees: the
+    // edges a fresh traversal of v would inspect at most
+    std::vector<double> sub((size_t)n, 0.0);
+    for (int32_t v = 0; v < n; v++) sub[(size_t)v] = (double)(s.ptr[(size_t)v + 1] - s.ptr[(size_t)v]);
+    for (int32_t v = 0; v < n; v++)    // parent[v] > v: children first
+        if (parent[(size_t)v] != -1) sub[(size_t)parent[(size_t)v]] += sub[(size_t)v];
     std::vector<double> pre((size_t)n + 1, 0.0);
-    for (int32_t v = 0; v < n; v++)
+    const double kPieceLen = piece_len(n);
+    for (int32_t v = 0; v < n; v++) {
+        const double fresh = (sub[(size_t)v] - (double)(s.ptr[(size_t)v + 1] - s.ptr[(size_t)v])) / 2.0;
         pre[(size_t)v + 1] = pre[(size_t)v] + 2.0 * kCostPerSource +
-                             kCostPerEntry * 2.0 * (double)std::max<int64_t>(cc[(size_t)v] - 1, 0);
+                             kCostPerEntry * 2.0 * (double)std::max<int64_t>(cc[(size_t)v] - 1, 0) +
+                             2.0 * kCostPerEdge * fresh / kPieceLen;
+    }
     const double total = pre[(size_t)n];
     cuts[0] = 0;
     for (int32_t p = 1; p < parts; p++) {

@@ -65,7 +65,8 @@ typedef struct gsofa_matrix gsofa_matrix; /* device-resident G and G^T     */
 typedef struct gsofa_params {
     int32_t src_chunk;          /* consecutive sources per work item; 0: 32 to
                                    512, about eight pieces per resident CTA  */
-    int32_t block_size;         /* threads per CTA: 128, 256, 512 or 1024     */
+    int32_t block_size;         /* threads per CTA: 128, 256, 512, 768 (the
+                                   two passes side by side only) or 1024      */
     int32_t threads_per_source; /* lanes expanding one frontier vertex:
                                    1 (default: one thread per vertex, a warp
                                    for rows longer than 32), 4, 8, 16 or 32   */
@@ -109,6 +110,11 @@ typedef struct gsofa_params {
 #define GSOFA_FLAG_GLOBAL_STATE 0x8 /* keep every traversal's visited bitmap
                                       in global memory (L2): many small
                                       traversals per SM, any n              */
+#define GSOFA_FLAG_WIDE_REGS 0x40  /* the two passes side by side in 512-thread
+                                      CTAs with up to 128 registers a thread
+                                      (one CTA per SM): fastest on
+                                      latency-bound matrices (small frontiers),
+                                      slower on dense-fill ones               */
 #define GSOFA_FLAG_DIRECT_HOST 0x20 /* gsofa_symbfact_ranges into host memory:
                                       the kernel writes the lists there
                                       itself (no device pool; slower than the

@@ -76,7 +76,8 @@ def test_empty_and_tiny(ctx):
 @pytest.mark.parametrize("block,lanes,reuse,chunk,per_sm", [
     (128, 4, 0, 1, 0), (256, 8, 1, 7, 1), (512, 16, 1, 32, 0), (1024, 32, 0, 3, 0),
     (256, 32, 1, 1, 2), (512, 8, 1, 200, 0), (128, 1, 0, 1, 0), (1024, 1, 1, 16, 1),
-    (512, 1, 2, 32, 0), (256, 1, 2, 5, 0), (1024, 1, 2, 64, 1), (512, 1, -1, 3, 2)])
+    (512, 1, 2, 32, 0), (256, 1, 2, 5, 0), (1024, 1, 2, 64, 1), (512, 1, -1, 3, 2),
+    (768, 1, -1, 0, 0), (768, 8, 1, 40, 0), (768, 1, 0, 1, 0)])
 def test_parameters_do_not_change_results(ctx, block, lanes, reuse, chunk, per_sm):
     g = matgen.grid3d(14, ordering="nd", drop_frac=0.1, seed=5)
     ref = _oracle(g, 8)
@@ -99,6 +100,17 @@ def test_global_state_kernel(ctx, block, lanes, reuse, chunk, per_sm):
                          src_chunk=chunk, ctas_per_sm=per_sm, max_supernode_size=8,
                          flags=gsofa_b200.FLAG_GLOBAL_STATE)
         assert_same(r, ref, where=f"global state {g.name} {block},{lanes},{reuse},{chunk},{per_sm}")
+
+
+def test_wide_register_kernel(ctx):
+    for g in (matgen.grid3d(20, ordering="nd", drop_frac=0.1, seed=2), matgen.powerlaw(12000, seed=5)):
+        for pattern in (0, 1):
+            r = ctx.symbfact(ctx.upload(g), want_pattern=pattern, max_supernode_size=8,
+                             flags=gsofa_b200.FLAG_WIDE_REGS)
+            assert_same(r, _oracle(g, 8, pattern=bool(pattern)), pattern=bool(pattern),
+                        where=f"wide registers {g.name} pattern={pattern}")
+    with pytest.raises(gsofa_b200.GsofaError):
+        ctx.symbfact(ctx.upload(bundled()), reuse=0, flags=gsofa_b200.FLAG_WIDE_REGS)
 
 
 def test_state_flags_conflict_is_an_error(ctx):
