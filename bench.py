@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--wide-regs", action="store_true",
+                    help="512-thread CTAs with up to 128 registers a thread (GSOFA_FLAG_WIDE_REGS)")
     ap.add_argument("--form", choices=["ranges", "csr"], default="ranges",
                     help="pattern form: begin/end ranges into a pool (no compaction) or CSR")
     ap.add_argument("--state", choices=["auto", "global", "shared"], default="auto",
@@ -410,7 +412,9 @@ def serving_run(ctx, count, nmax, rate, compare, pool_procs=16):
     params = gsofa_b200.Params.default(want_pattern=0)
     srv = gsofa_b200.StreamServer(0, mem_budget_bytes=120 << 30)
     oversize = lambda g: ctx.symbfact(ctx.upload(g), params)  # noqa: E731
-    cs = serve.ContinuousServer(srv, oversize=oversize, max_n=srv.max_n)
+    # size classes: small requests share the persistent serving kernel, large
+    # ones run alone on the factorization kernel
+    cs = serve.ContinuousServer(srv, oversize=oversize, max_n=min(srv.max_n, serve.LARGE_REQUEST_N - 1))
     warm = [serve.Request(-1 - i, 0.0, matgen.make("grid3d", 2000, i)) for i in range(4)]
     cs.run(warm)
     stream = serve.LazyStream(pool, _make_graph, spec, arrivals, ahead=256)
@@ -437,7 +441,10 @@ def serving_run(ctx, count, nmax, rate, compare, pool_procs=16):
             "admission_budget_gb": 120, "pattern": "counts only", "seed": matgen.SEEDS["serve"],
             "serving": full["report"],
             "comparison": {"requests": k, "continuous": cont["report"], "one_at_a_time": single["report"]},
-            "results_identical": bool(same), "serving_kernel_max_n": max_n, "clocks": clk.summary(),
+            "results_identical": bool(same), "serving_kernel_max_n": max_n,
+            "size_classes": {"serving_kernel": f"n < {serve.LARGE_REQUEST_N}",
+                             "alone_on_factorization_kernel": f"n >= {serve.LARGE_REQUEST_N}"},
+            "clocks": clk.summary(),
             "generation": "process pool, in arrival order, while serving (a request arrives when both "
                           "its time and its matrix have come)"}
 
@@ -535,6 +542,8 @@ def link_gbs(torch, stream, nbytes=1 << 30):
 def _params(gsofa_b200, args, **kw):
     """Library parameters from the command line (plus overrides)."""
     flags = {"auto": 0, "global": gsofa_b200.FLAG_GLOBAL_STATE, "shared": gsofa_b200.FLAG_SHARED_STATE}[args.state]
+    if args.wide_regs:
+        flags |= gsofa_b200.FLAG_WIDE_REGS
     base = dict(reuse=args.reuse, block_size=args.block, src_chunk=args.chunk, threads_per_source=args.lanes,
                 ctas_per_sm=args.ctas_per_sm, flags=flags)
     extra_flags = kw.pop("flags", 0)
@@ -1064,14 +1073,16 @@ def main():
         line = {
             "metric": "nnz(L+U)/s", "value": value, "unit": "nnz/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded generator)",
             "config": dict(cfg, nnz_lu=int(nnz_lu), fill_count=int(res.fill_count),
                            supernodes=int(res.n_supernodes),
                            pattern={"ranges": "begin/end ranges into a device pool", "csr": "CSR on the device",
                                     "counts": "counts only"}[form],
                            state=args.state, reuse=args.reuse, l2="flushed between steps (256 MiB write)",
-                           parallelism=f"independent factorization per rank x{world}"),
+                           parallelism=("one matrix on one GPU (--gpus N splits it into N contiguous "
+                                        "work-predicted line ranges)" if world == 1 else
+                                        f"independent factorization per rank x{world}")),
             "factorizations_per_s": facts,
             "other_forms": forms,
             "split_on_one_gpu": split,

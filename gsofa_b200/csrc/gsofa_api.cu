@@ -386,16 +386,21 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     // Shared-state pairs past 8K lines hold one CTA per SM (1024 threads at
     // 64 registers fill its register file): 768 threads with up to 80
     // registers a thread run without register spills, measured faster than
-    // 1024 threads on the 80^3 stencil with and without the pattern.  (512
-    // threads with up to 128 registers -- GSOFA_FLAG_WIDE_REGS -- are faster
-    // still on latency-bound matrices, counts only, but slower where large
-    // frontiers keep many warps busy, such as dense-fill power-law matrices.)
+    // 1024 threads on the 80^3 stencil with and without the pattern.  Counts
+    // of matrices with long rows (no row slots: mean degree above SLOT_NB)
+    // take 1024 threads: their large frontiers keep every warp busy (9%
+    // faster on the 659K-line power-law matrix).  512 threads with up to 128
+    // registers -- GSOFA_FLAG_WIDE_REGS -- are faster still on latency-bound
+    // matrices, counts only, but slower where large frontiers keep many warps
+    // busy.
     const bool wide = (p.flags & GSOFA_FLAG_WIDE_REGS) != 0;
+    bool long_rows = false;
+    for (int i = 0; i < count; i++) long_rows |= mats[i]->n > 0 && mats[i]->d_gslot == nullptr;
     int block = p.block_size;
     if (wide) block = 512;
     if (!block) {
         if (gbm) block = paired ? 256 : 128;
-        else if (paired && max_n > 8192) block = 768;
+        else if (paired && max_n > 8192) block = (!want_pattern && long_rows) ? 1024 : 768;
         else block = pick_block(max_n) * (paired ? 2 : 1);
     }
     if (wide && (!paired || gbm)) return GSOFA_ERR_INVALID_INPUT;
@@ -464,10 +469,15 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     // low-numbered sources, so the launch's tail stays short
     int chunk = p.src_chunk;
     if (chunk <= 0) {
-        // a line range keeps the pieces the whole matrix would have: smaller
-        // ones would start more traversals afresh, and a fresh start costs
-        // most in the separator lines a range of the last lines holds
-        const int64_t per = (int64_t)(paired ? 1 : 2) * L / ((int64_t)8 * grid);
+        // a line range keeps the pieces the whole matrix would have (smaller
+        // ones start more traversals afresh, and a fresh start costs most in
+        // the separator lines a range of the last lines holds) while every
+        // CTA still gets about four pieces; shorter ranges take the length
+        // that gives every CTA four, or eight, pieces
+        const int64_t mult = paired ? 1 : 2;
+        const int64_t lines = line_range ? (int64_t)(range_hi - range_lo) : L;
+        const int64_t per = std::max(mult * lines / ((int64_t)8 * grid),
+                                     std::min(mult * L / ((int64_t)8 * grid), mult * lines / ((int64_t)4 * grid)));
         chunk = reuse ? (int)std::min<int64_t>(512, std::max<int64_t>(32, per)) : 1;
     }
 
@@ -1092,7 +1102,10 @@ gsofa_status gsofa_upload(gsofa_ctx *c, int32_t n, int64_t nnz, const int32_t *b
             auto al = [](size_t b) { return (b + 255) / 256 * 256; };
             const size_t pb = al((size_t)(n + 1) * 4), lb = al(nb);
             const size_t ab = al((size_t)std::max<int64_t>(nnz, 1) * 4);
-            const size_t sb = al((size_t)std::max<int32_t>(n, 1) * 32);
+            // row slots only where most rows fit one (mean off-diagonal
+            // degree of the input at most SLOT_NB)
+            const bool slots = nnz - (int64_t)n <= (int64_t)SLOT_NB * n;
+            const size_t sb = slots ? al((size_t)std::max<int32_t>(n, 1) * 32) : 0;
             const size_t total = 2 * pb + 3 * lb + 2 * ab + 2 * sb;
             char *q = (char *)c->slab_take(total, &m->slab_bytes);
             m->slab = q;
@@ -1101,8 +1114,8 @@ gsofa_status gsofa_upload(gsofa_ctx *c, int32_t n, int64_t nnz, const int32_t *b
             m->d_orig_up = (int32_t *)q; q += lb;
             m->d_orig_lo = (int32_t *)q; q += lb;
             m->d_rawdeg = (int32_t *)q; q += lb;
-            m->d_gslot = (int4 *)q; q += sb;
-            m->d_tslot = (int4 *)q; q += sb;
+            m->d_gslot = sb ? (int4 *)q : nullptr; q += sb;
+            m->d_tslot = sb ? (int4 *)q : nullptr; q += sb;
             m->d_gadj = (int32_t *)q; q += ab;
             m->d_tadj = (int32_t *)q;
         }
@@ -1171,10 +1184,12 @@ gsofa_status gsofa_upload(gsofa_ctx *c, int32_t n, int64_t nnz, const int32_t *b
         if (n > 0) {
             upload_fill_kernel<<<ugrid, ub, 0, st>>>(u, m->d_gptr, m->d_gadj, d_tcur, m->d_tadj);
             GS_CUDA(cudaGetLastError());
-            const int sgrid = (int)std::min<int64_t>(((int64_t)n + 255) / 256, (int64_t)c->sm_count * 8);
-            slot_fill_kernel<<<sgrid, 256, 0, st>>>(n, m->d_gptr, m->d_gadj, m->d_gslot);
-            slot_fill_kernel<<<sgrid, 256, 0, st>>>(n, m->d_tptr, m->d_tadj, m->d_tslot);
-            GS_CUDA(cudaGetLastError());
+            if (m->d_gslot != nullptr) {
+                const int sgrid = (int)std::min<int64_t>(((int64_t)n + 255) / 256, (int64_t)c->sm_count * 8);
+                slot_fill_kernel<<<sgrid, 256, 0, st>>>(n, m->d_gptr, m->d_gadj, m->d_gslot);
+                slot_fill_kernel<<<sgrid, 256, 0, st>>>(n, m->d_tptr, m->d_tadj, m->d_tslot);
+                GS_CUDA(cudaGetLastError());
+            }
         }
         GS_CUDA(cudaStreamSynchronize(st));
     } catch (CudaFail &f) {

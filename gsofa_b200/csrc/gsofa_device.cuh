@@ -29,7 +29,9 @@ namespace cg = cooperative_groups;
 // Rows of at most SLOT_NB ids are also kept whole in a 32-byte slot per
 // vertex -- {degree, row offset, up to six ids} -- so expanding a frontier
 // vertex is one L2 round trip instead of two (row bounds, then ids); longer
-// rows take their ids from adj at the slot's offset.
+// rows take their ids from adj at the slot's offset.  Matrices whose mean
+// off-diagonal degree is above SLOT_NB have no slots (slot == nullptr): most
+// of their rows would pay the 32-byte slot load and still read adj.
 constexpr int SLOT_NB = 6;
 
 struct PassGraph {
@@ -305,12 +307,14 @@ constexpr int SEED_ADJ = 512;
 struct SharedState {
     long long piece;
     int flag;
-    int tailc[3];     // entries pushed for level L live in tailc[L % 3]
-    int fetch[3];     // dynamic fetch counter of level L in fetch[L % 3]
+    int tailc[3];     // level entry counts by phase (barrier-synchronised levels)
+    int fetch[3];     // dynamic fetch counters by phase
     int chain_lo;     // lowest vertex set in the bitmap since the last clear
     int chain_hi;     // highest vertex set since the last clear
     int seg[2];       // piece boundaries after chain alignment
-    int64_t warp[32];
+    int stail;        // entries of the next level, counted while warp 0 runs levels alone
+    int solo_start, solo_wstart, solo_count;   // where such a run ended
+    int64_t warp[32]; // per-warp entry counts of a chain's last list (list output)
     // tallies kept by the half's first thread only: levels, then cycles of
     // seeding, level loop, range fold, count and link flag, list output (per
     // chain), bitmap clearing, wait for the other pass; sources; reused
@@ -509,124 +513,179 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
     long long cs = 0;
     if (tid == 0) { cs = clock64(); prof[1] += (unsigned long long)(cs - c0); }
 
-    // level-synchronous expansion through vertices < s, one barrier a level
-    int start = 0, wstart = 0;
-    for (int L = 0;; L++) {
-        gsync<GT>(bar);
-        const int end = start + sh.tailc[L % 3];
-        if (end == start) {
-            if (tid == 0) prof[0] += (unsigned long long)L;
-            break;
+    // One warp's step of a level (one thread per vertex): items base ..
+    // base + 31 of the level [start, end), whose entries were written while
+    // the level starting at wstart ran; new vertices below s go to the next
+    // level through tailp.  Each lane loads its row bounds and then up to
+    // eight adjacency ids at once (independent loads in flight hide the L2
+    // latency).  The id loop runs to the warp's longest light row so every
+    // step is warp-uniform and new vertices below s are enqueued with one
+    // ballot and one shared atomic.  Rows longer than HEAVY_ROW are expanded
+    // by the whole warp.
+    auto warp_step = [&](const int base, const int start, const int end, const int wstart, int *const tailp) {
+        const int it = base + lane;
+        int32_t b = 0, d = 0;
+        int4 sl0 = make_int4(0, 0, -1, -1), sl1 = make_int4(-1, -1, -1, -1);
+        if (it < end) {
+            const int32_t v = fr_get(f, it, wstart);
+            if (g.slot != nullptr) {   // degree, offset and short rows in one 32-byte load
+                sl0 = ld4<CG>(g.slot + 2 * (int64_t)v);
+                sl1 = ld4<CG>(g.slot + 2 * (int64_t)v + 1);
+                d = sl0.x;
+                b = sl0.y;
+            } else {
+                b = ld<CG>(g.ptr + v);
+                d = ld<CG>(g.ptr + v + 1) - b;
+            }
+            edges += (unsigned long long)d;
+            if (pass == 0) { xcnt++; einsp += (unsigned long long)ld<CG>(rawdeg + v); }
         }
-        if (tid == 0) { sh.tailc[(L + 2) % 3] = 0; sh.fetch[(L + 1) % 3] = 0; }
-        int *tailp = &sh.tailc[(L + 1) % 3];
-        int *fetchp = &sh.fetch[L % 3];
+        // the row's ids are in the slot (first step of the id loop)
+        const bool in_slot = g.slot != nullptr && d <= SLOT_NB;
+        unsigned heavy = __ballot_sync(0xffffffffu, d > HEAVY_ROW);
+        while (heavy) {
+            const int src = __ffs(heavy) - 1;
+            heavy &= heavy - 1u;
+            const int32_t hb = __shfl_sync(0xffffffffu, b, src);
+            const int32_t hd = __shfl_sync(0xffffffffu, d, src);
+            for (int32_t k0 = 0; k0 < hd; k0 += 32) {
+                const bool on = k0 + lane < hd;
+                const int32_t m = on ? ld<CG>(g.adj + hb + k0 + lane) : 0;
+                const bool fresh = on && test_and_set<GBM>(bm, summ, m);
+                if (fresh) { t_lo = min(t_lo, m); t_hi = max(t_hi, m); stamp_set(sh, m, cidx, s - cidx); }
+                const bool low = fresh && m < s;
+                const unsigned bal = __ballot_sync(0xffffffffu, low);
+                const unsigned bhi = __ballot_sync(0xffffffffu, fresh) & ~bal;
+                if (lane == 0 && bhi) atomicAdd(&sh.hcount, __popc(bhi));
+                if (bal) {
+                    int pb = 0;
+                    if (lane == 0) pb = atomicAdd(tailp, __popc(bal));
+                    pb = __shfl_sync(0xffffffffu, pb, 0);
+                    if (low) fr_put(f, end + pb + __popc(bal & ((1u << lane) - 1u)), start, m);
+                }
+            }
+        }
+        const int dl = d > HEAVY_ROW ? 0 : d;
+        const int dmax = __reduce_max_sync(0xffffffffu, dl);
+        for (int k0 = 0; k0 < dmax; k0 += 8) {
+            int32_t buf[8];
+            if (in_slot) {   // d <= 6 < 8: only this first step has ids
+                const int32_t sv[SLOT_NB] = {sl0.z, sl0.w, sl1.x, sl1.y, sl1.z, sl1.w};
+#pragma unroll
+                for (int u = 0; u < 8; u++) buf[u] = (u < SLOT_NB && k0 + u < dl) ? sv[u < SLOT_NB ? u : 0] : -1;
+            } else {
+#pragma unroll
+                for (int u = 0; u < 8; u++) buf[u] = (k0 + u < dl) ? ld<CG>(g.adj + b + k0 + u) : -1;
+            }
+            // independent bit tests and sets first, then one enqueue
+            // (warp scan + one shared atomic) for all new low vertices
+            unsigned fresh = 0u;
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+                if (buf[u] >= 0 && test_and_set<GBM>(bm, summ, buf[u])) fresh |= 1u << u;
+            // new vertices below s in the low 16 bits, above s in
+            // the high ones (a warp step finds at most 256)
+            int nlh = 0;
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+                if ((fresh >> u) & 1u) {
+                    t_lo = min(t_lo, buf[u]);
+                    t_hi = max(t_hi, buf[u]);
+                    nlh += buf[u] < s ? 1 : 0x10000;
+                }
+            if (fresh && sh.stamp != nullptr) {
+#pragma unroll
+                for (int u = 0; u < 8; u++)
+                    if ((fresh >> u) & 1u) stamp_set(sh, buf[u], cidx, s - cidx);
+            }
+            int incl = nlh;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int wsum = __shfl_sync(0xffffffffu, incl, 31);
+            const int wtot = wsum & 0xffff;
+            if (lane == 0 && (wsum >> 16)) atomicAdd(&sh.hcount, wsum >> 16);
+            if (wtot) {
+                int pb = 0;
+                if (lane == 0) pb = atomicAdd(tailp, wtot);
+                pb = __shfl_sync(0xffffffffu, pb, 0) + ((incl - nlh) & 0xffff);
+#pragma unroll
+                for (int u = 0; u < 8; u++)
+                    if (((fresh >> u) & 1u) && buf[u] < s) fr_put(f, end + pb++, start, buf[u]);
+            }
+        }
+    };
+
+    // level-synchronous expansion through vertices < s, one barrier a level.
+    // A level of at most 32 vertices (one per lane) is run by warp 0 alone
+    // (solo), and so are the small levels after it, with warp barriers only,
+    // while the traversal's other warps wait at the next barrier.  The
+    // barrier-synchronised levels count their entries in tailc[] by phase c:
+    // the current level's count in tailc[c % 3], the next level's in
+    // tailc[(c + 1) % 3] (zero when the level starts), fetch counter
+    // fetch[c % 3] (zero too).  Solo levels count in sh.stail only, touched by
+    // lane 0 alone, and hand over through sh.solo_* after the next barrier:
+    // the phase and its counters are then as they were when the run began.
+    int start = 0, wstart = 0, c = 0;
+    bool relay = false;   // warp 0 ran levels alone: take up its position
+    for (;;) {
+        gsync<GT>(bar);
+        int end;
+        if (relay) {
+            start = sh.solo_start;
+            wstart = sh.solo_wstart;
+            end = start + sh.solo_count;
+            relay = false;
+        } else {
+            end = start + sh.tailc[c % 3];
+        }
+        if (end == start) break;
+        const bool solo = lanes == 1 && end - start <= 32;
+        if (solo && tid >= 32) {
+            relay = true;
+            continue;
+        }
+        if (tid == 0) prof[0]++;   // levels
+        if (!solo && tid == 0) { sh.tailc[(c + 2) % 3] = 0; sh.fetch[(c + 1) % 3] = 0; }
+        int *const tailp = solo ? &sh.stail : &sh.tailc[(c + 1) % 3];
+        int *const fetchp = &sh.fetch[c % 3];
         if (lanes == 1) {
-            // One thread per vertex: a warp takes 32 queue items with one
-            // shared atomic; each lane loads its row bounds and then up to
-            // eight adjacency ids at once (independent loads in flight hide
-            // the L2 latency).  The id loop runs to the warp's longest light
-            // row so every step is warp-uniform and new vertices below s are
-            // enqueued with one ballot and one shared atomic.  Rows longer
-            // than HEAVY_ROW are expanded by the whole warp.
+            // a warp takes 32 queue items with one shared atomic; solo, warp
+            // 0 takes the whole level, then the next while it is small
             for (;;) {
-                int base = 0;
-                if (lane == 0) base = atomicAdd(fetchp, 32);
-                base = __shfl_sync(0xffffffffu, base, 0) + start;
-                if (base >= end) break;
-                const int it = base + lane;
-                int32_t b = 0, d = 0;
-                int4 sl0 = make_int4(0, 0, -1, -1), sl1 = make_int4(-1, -1, -1, -1);
-                if (it < end) {
-                    const int32_t v = fr_get(f, it, wstart);
-                    if (g.slot != nullptr) {   // degree, offset and short rows in one 32-byte load
-                        sl0 = ld4<CG>(g.slot + 2 * (int64_t)v);
-                        sl1 = ld4<CG>(g.slot + 2 * (int64_t)v + 1);
-                        d = sl0.x;
-                        b = sl0.y;
-                    } else {
-                        b = ld<CG>(g.ptr + v);
-                        d = ld<CG>(g.ptr + v + 1) - b;
-                    }
-                    edges += (unsigned long long)d;
-                    if (pass == 0) { xcnt++; einsp += (unsigned long long)ld<CG>(rawdeg + v); }
+                int base = start;
+                if (solo) {
+                    if (lane == 0) sh.stail = 0;
+                } else {
+                    if (lane == 0) base = atomicAdd(fetchp, 32);
+                    base = __shfl_sync(0xffffffffu, base, 0) + start;
+                    if (base >= end) break;
                 }
-                // the row's ids are in the slot (first step of the id loop)
-                const bool in_slot = g.slot != nullptr && d <= SLOT_NB;
-                unsigned heavy = __ballot_sync(0xffffffffu, d > HEAVY_ROW);
-                while (heavy) {
-                    const int src = __ffs(heavy) - 1;
-                    heavy &= heavy - 1u;
-                    const int32_t hb = __shfl_sync(0xffffffffu, b, src);
-                    const int32_t hd = __shfl_sync(0xffffffffu, d, src);
-                    for (int32_t k0 = 0; k0 < hd; k0 += 32) {
-                        const bool on = k0 + lane < hd;
-                        const int32_t m = on ? ld<CG>(g.adj + hb + k0 + lane) : 0;
-                        const bool fresh = on && test_and_set<GBM>(bm, summ, m);
-                        if (fresh) { t_lo = min(t_lo, m); t_hi = max(t_hi, m); stamp_set(sh, m, cidx, s - cidx); }
-                        const bool low = fresh && m < s;
-                        const unsigned bal = __ballot_sync(0xffffffffu, low);
-                        const unsigned bhi = __ballot_sync(0xffffffffu, fresh) & ~bal;
-                        if (lane == 0 && bhi) atomicAdd(&sh.hcount, __popc(bhi));
-                        if (bal) {
-                            int pb = 0;
-                            if (lane == 0) pb = atomicAdd(tailp, __popc(bal));
-                            pb = __shfl_sync(0xffffffffu, pb, 0);
-                            if (low) fr_put(f, end + pb + __popc(bal & ((1u << lane) - 1u)), start, m);
+                warp_step(base, start, end, wstart, tailp);
+                if (solo) {
+                    __syncwarp();   // the level's queue entries, for every lane
+                    int nn = 0;
+                    if (lane == 0) nn = sh.stail;
+                    nn = __shfl_sync(0xffffffffu, nn, 0);
+                    wstart = start;
+                    start = end;
+                    end += nn;
+                    if (nn == 0 || nn > 32) {
+                        if (lane == 0) {
+                            sh.solo_start = start;
+                            sh.solo_wstart = wstart;
+                            sh.solo_count = nn;
                         }
+                        break;
                     }
+                    if (lane == 0) prof[0]++;
                 }
-                const int dl = d > HEAVY_ROW ? 0 : d;
-                const int dmax = __reduce_max_sync(0xffffffffu, dl);
-                for (int k0 = 0; k0 < dmax; k0 += 8) {
-                    int32_t buf[8];
-                    if (in_slot) {   // d <= 6 < 8: only this first step has ids
-                        const int32_t sv[SLOT_NB] = {sl0.z, sl0.w, sl1.x, sl1.y, sl1.z, sl1.w};
-#pragma unroll
-                        for (int u = 0; u < 8; u++) buf[u] = (u < SLOT_NB && k0 + u < dl) ? sv[u < SLOT_NB ? u : 0] : -1;
-                    } else {
-#pragma unroll
-                        for (int u = 0; u < 8; u++) buf[u] = (k0 + u < dl) ? ld<CG>(g.adj + b + k0 + u) : -1;
-                    }
-                    // independent bit tests and sets first, then one enqueue
-                    // (warp scan + one shared atomic) for all new low vertices
-                    unsigned fresh = 0u;
-#pragma unroll
-                    for (int u = 0; u < 8; u++)
-                        if (buf[u] >= 0 && test_and_set<GBM>(bm, summ, buf[u])) fresh |= 1u << u;
-                    // new vertices below s in the low 16 bits, above s in
-                    // the high ones (a warp step finds at most 256)
-                    int nlh = 0;
-#pragma unroll
-                    for (int u = 0; u < 8; u++)
-                        if ((fresh >> u) & 1u) {
-                            t_lo = min(t_lo, buf[u]);
-                            t_hi = max(t_hi, buf[u]);
-                            nlh += buf[u] < s ? 1 : 0x10000;
-                        }
-                    if (fresh && sh.stamp != nullptr) {
-#pragma unroll
-                        for (int u = 0; u < 8; u++)
-                            if ((fresh >> u) & 1u) stamp_set(sh, buf[u], cidx, s - cidx);
-                    }
-                    int incl = nlh;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                        if (lane >= o) incl += y;
-                    }
-                    const int wsum = __shfl_sync(0xffffffffu, incl, 31);
-                    const int wtot = wsum & 0xffff;
-                    if (lane == 0 && (wsum >> 16)) atomicAdd(&sh.hcount, wsum >> 16);
-                    if (wtot) {
-                        int pb = 0;
-                        if (lane == 0) pb = atomicAdd(tailp, wtot);
-                        pb = __shfl_sync(0xffffffffu, pb, 0) + ((incl - nlh) & 0xffff);
-#pragma unroll
-                        for (int u = 0; u < 8; u++)
-                            if (((fresh >> u) & 1u) && buf[u] < s) fr_put(f, end + pb++, start, buf[u]);
-                    }
-                }
+            }
+            if (solo) {
+                relay = true;
+                continue;
             }
         } else {
             // groups of `lanes` threads per vertex
@@ -652,6 +711,7 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
         }
         wstart = start;
         start = end;
+        c++;
     }
     long long ce = 0;
     if (tid == 0) { ce = clock64(); prof[2] += (unsigned long long)(ce - cs); }
@@ -693,23 +753,45 @@ __device__ void process_source(const JobArgs &a, const PassGraph g, int32_t n,
 }
 #undef GSOFA_VISIT
 
+// Lane's bitmap word of chunk cc, without the bits below word w0 and below
+// first_mask in word w0.
+template <bool GBM>
+__device__ __forceinline__ uint32_t last_word(const uint32_t *bm, const uint32_t *summ, int cc, int lane, int w0,
+                                              uint32_t first_mask)
+{
+    const int w = (cc << 5) + lane;
+    uint32_t x = ((bm_word<GBM>(summ + cc) >> lane) & 1u) ? bm_word<GBM>(bm + w) : 0u;
+    if (w < w0) x = 0u;
+    if (w == w0) x &= first_mask;
+    return x;
+}
+
 // Writes the lists of the chain that just ended -- sources chain_s0 ..
 // chain_s0 + chain_len - 1, which shared one bitmap -- while the bitmap still
 // holds the last source's traversal.  Bits are only ever added along a chain,
 // so the bits above source i of the chain that were set by the time it
 // finished are its list: hi(s_i) = { v > s_i : v set, stamp(v) <= i }.  One
-// pool range holds all of the chain's lists; each warp then writes whole
-// lists on its own, in increasing order, with no barrier per source.  Lists
-// of pass G^T (columns of L) also count their entries into the L row
-// histogram (fire-and-forget reductions that overlap other traversals).
+// pool range holds all of the chain's lists.
+//
+// The last source's list is every set bit above it: all warps write it at
+// once from the bitmap (each a share of its chunks, offsets from a count
+// pass), into the pool and into `scratch` (this traversal's frontier spill
+// array, free once the traversal is done).  Every earlier list i is then the
+// chain's own later sources that it reached, followed by the last list's
+// entries of stamp <= i: a warp streams the last list from scratch (several
+// coalesced loads and their stamps in flight at once) and keeps its entries
+// by ballot -- no per-list walk of the bitmap.  Lists of pass G^T (columns
+// of L) also count their entries into the L row histogram (fire-and-forget
+// reductions that overlap other traversals).
 template <int GT, bool GBM>
 __device__ void output_chain(const JobArgs &a, int64_t line_base, int pass, const uint32_t *bm,
-                             const uint32_t *summ, SharedState &sh, int gtid, int bar)
+                             const uint32_t *summ, SharedState &sh, int32_t *scratch, int gtid, int bar)
 {
     const int64_t line0 = line_base + sh.chain_s0;
     int32_t *const lrow = pass ? a.lrow + line_base : nullptr;
     constexpr int NWARP = GT / 32;
     const int lane = gtid & 31, wid = gtid >> 5;
+    const unsigned below = (1u << lane) - 1u;
     const int s0 = sh.chain_s0, len = sh.chain_len;
     const int64_t row0 = (int64_t)pass * a.L + line0;   // cnt / poff entry of s0
     // warp 0: one pool range for the chain, then every list's offset
@@ -745,84 +827,135 @@ __device__ void output_chain(const JobArgs &a, int64_t line_base, int pass, cons
     }
     gsync<GT>(bar);
 
+    // the last source's list: set bits in words from w0 on (first_mask on
+    // w0), chunks [c_lo, c_hi) shared out among the warps
+    const int s_last = s0 + len - 1;
+    const int64_t off_last = a.poff[row0 + len - 1];
+    const int cnt_last = a.cnt[row0 + len - 1];
+    const int chain_hi = sh.chain_hi;
+    const bool write = off_last >= 0;   // else the pool is short: nothing is written
     const uint32_t *summ2 = summ + bm_summary_words(bm, summ);
-    const int cend = sh.chain_hi >= 0 ? (sh.chain_hi >> 10) + 1 : 0;   // chunks holding set bits
-    const uint16_t *stamp = sh.stamp;
-    for (int i = wid; i < len; i += NWARP) {
-        const int s = s0 + i;
-        const int64_t off = a.poff[row0 + i];
-        const int cnt = a.cnt[row0 + i];
-        if (off < 0 || cnt == 0) continue;
-        int32_t *out = a.pool + off;
-        const int w0 = (s + 1) >> 5;
-        const uint32_t first_mask = ~0u << ((s + 1) & 31);
-        const bool last = (i == len - 1);   // every set bit was set by then
-        int pos = 0;
-        for_nonzero_chunks<GBM>(summ2, w0 >> 5, cend, [&](int cc) {
-            const int w = (cc << 5) + lane;
-            uint32_t x = ((bm_word<GBM>(summ + cc) >> lane) & 1u) ? bm_word<GBM>(bm + w) : 0u;
-            if (w < w0) x = 0u;
-            if (w == w0) x &= first_mask;
-            if (x != 0u && !last) {
-                // stamps of this word's 32 vertices: four 16-byte loads
-                const uint4 *sp = reinterpret_cast<const uint4 *>(stamp + ((int64_t)w << 5));
-                uint32_t keep = 0u;
+    const int w0 = (s_last + 1) >> 5;
+    const uint32_t first_mask = ~0u << ((s_last + 1) & 31);
+    const int c_lo = w0 >> 5;
+    const int c_hi = chain_hi > s_last ? (chain_hi >> 10) + 1 : c_lo;
+    const int share = (max(c_hi - c_lo, 0) + NWARP - 1) / NWARP;
+    const int my_lo = c_lo + wid * share, my_hi = min(c_hi, my_lo + share);
+    int mine = 0;
+    if (write && my_lo < my_hi)
+        for_nonzero_chunks<GBM>(summ2, my_lo, my_hi, [&](int cc) {
+            mine += __popc(last_word<GBM>(bm, summ, cc, lane, w0, first_mask));
+        });
+    mine = (int)__reduce_add_sync(0xffffffffu, (unsigned)mine);
+    if (lane == 0) sh.warp[wid] = mine;
+    gsync<GT>(bar);
+    if (write) {
+        int pos = 0, all = 0;
+        for (int k = 0; k < NWARP; k++) {
+            const int c = (int)sh.warp[k];
+            pos += k < wid ? c : 0;
+            all += c;
+        }
+        if (gtid == 0 && all != cnt_last) atomicOr(a.status, ERR_COUNT_MISMATCH);
+        int32_t *const out = a.pool + off_last;
+        if (my_lo < my_hi)
+            for_nonzero_chunks<GBM>(summ2, my_lo, my_hi, [&](int cc) {
+                uint32_t x = last_word<GBM>(bm, summ, cc, lane, w0, first_mask);
+                const int pc = __popc(x);
+                int incl = pc;
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    if ((x >> (8 * q)) & 0xffu) {
-                        const uint4 v = sp[q];
-                        const uint32_t h[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-                        for (int e = 0; e < 4; e++) {
-                            keep |= (uint32_t)((int)(h[e] & 0xffffu) <= i) << (8 * q + 2 * e);
-                            keep |= (uint32_t)((int)(h[e] >> 16) <= i) << (8 * q + 2 * e + 1);
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                const int excl = incl - pc;
+                const int wbase = cc << 5;
+                // at most two entries a word: a word per lane; denser chunks
+                // a word at a time across the warp (lane = bit), one
+                // coalesced run per store.  Nothing lands past the list's
+                // own cnt_last entries.
+                if (__reduce_max_sync(0xffffffffu, (unsigned)pc) <= 2u) {
+                    int at = pos + excl;
+                    while (x) {
+                        const int bit = __ffs(x) - 1;
+                        x &= x - 1u;
+                        const int32_t v = ((wbase + lane) << 5) + bit;
+                        if (at < cnt_last) {
+                            out[at] = v;
+                            scratch[at] = v;
+                            if (lrow) atomicAdd(lrow + v, 1);
+                        }
+                        at++;
+                    }
+                } else {
+                    unsigned nzw = __ballot_sync(0xffffffffu, x != 0u);
+                    while (nzw) {
+                        const int j = __ffs(nzw) - 1;
+                        nzw &= nzw - 1u;
+                        const uint32_t xj = __shfl_sync(0xffffffffu, x, j);
+                        const int pj = __shfl_sync(0xffffffffu, excl, j);
+                        const int at = pos + pj + __popc(xj & below);
+                        if (((xj >> lane) & 1u) && at < cnt_last) {
+                            const int32_t v = ((wbase + j) << 5) + lane;
+                            out[at] = v;
+                            scratch[at] = v;
+                            if (lrow) atomicAdd(lrow + v, 1);
                         }
                     }
                 }
-                x &= keep;
+                pos += __shfl_sync(0xffffffffu, incl, 31);
+            });
+    }
+    gsync<GT>(bar);
+
+    // every earlier list i: its later chain sources (s_i, s_last] that were
+    // reached by then, then the last list's entries of stamp <= i (all above
+    // s_last, so the list stays sorted)
+    const uint16_t *stamp = sh.stamp;
+    for (int i = wid; write && i < len - 1; i += NWARP) {
+        const int s = s0 + i;
+        const int64_t off = a.poff[row0 + i];
+        const int cnt = a.cnt[row0 + i];
+        if (cnt == 0) continue;
+        int32_t *const out = a.pool + off;
+        int pos = 0;
+        for (int k0 = s + 1; k0 <= s_last; k0 += 32) {
+            const int v = k0 + lane;
+            const bool in = v <= s_last && ((bm_word<GBM>(bm + (v >> 5)) >> (v & 31)) & 1u) && (int)stamp[v] <= i;
+            const unsigned bal = __ballot_sync(0xffffffffu, in);
+            const int at = pos + __popc(bal & below);
+            if (in && at < cnt) {
+                out[at] = v;
+                if (lrow) atomicAdd(lrow + v, 1);
             }
-            const int pc = __popc(x);
-            int incl = pc;
+            pos += __popc(bal);
+        }
+        // UNR loads of the last list and their stamps in flight at once (two
+        // where 64 registers a thread must do)
+        constexpr int UNR = GT > 384 ? 2 : 4;
+        for (int k0 = 0; k0 < cnt_last; k0 += 32 * UNR) {
+            int32_t e[UNR];
+            int t[UNR];
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += y;
+            for (int u = 0; u < UNR; u++) {
+                const int k = k0 + 32 * u + lane;
+                e[u] = k < cnt_last ? __ldcg(scratch + k) : -1;
             }
-            const int excl = incl - pc;
-            const int wbase = cc << 5;
-            // at most two entries a word: a word per lane; denser chunks a
-            // word at a time across the warp (lane = bit), one coalesced run
-            // per store.  Nothing lands past the list's own `cnt` entries.
-            if (__reduce_max_sync(0xffffffffu, (unsigned)pc) <= 2u) {
-                int at = pos + excl;
-                while (x) {
-                    const int bit = __ffs(x) - 1;
-                    x &= x - 1u;
-                    const int32_t v = ((wbase + lane) << 5) + bit;
-                    if (at < cnt) {
-                        out[at] = v;
-                        if (lrow) atomicAdd(lrow + v, 1);
-                    }
-                    at++;
+#pragma unroll
+            for (int u = 0; u < UNR; u++)   // only vertices of the last list (s_last, chain_hi] are read
+                t[u] = (e[u] > s_last && e[u] <= chain_hi) ? (int)stamp[e[u]] : INT32_MAX;
+#pragma unroll
+            for (int u = 0; u < UNR; u++) {
+                const bool in = t[u] <= i;
+                const unsigned bal = __ballot_sync(0xffffffffu, in);
+                const int at = pos + __popc(bal & below);
+                if (in && at < cnt) {
+                    out[at] = e[u];
+                    if (lrow) atomicAdd(lrow + e[u], 1);
                 }
-            } else {
-                unsigned nzw = __ballot_sync(0xffffffffu, x != 0u);
-                const uint32_t below = (1u << lane) - 1u;
-                while (nzw) {
-                    const int j = __ffs(nzw) - 1;
-                    nzw &= nzw - 1u;
-                    const uint32_t xj = __shfl_sync(0xffffffffu, x, j);
-                    const int pj = __shfl_sync(0xffffffffu, excl, j);
-                    const int at = pos + pj + __popc(xj & below);
-                    if (((xj >> lane) & 1u) && at < cnt) {
-                        const int32_t v = ((wbase + j) << 5) + lane;
-                        out[at] = v;
-                        if (lrow) atomicAdd(lrow + v, 1);
-                    }
-                }
+                pos += __popc(bal);
             }
-            pos += __shfl_sync(0xffffffffu, incl, 31);
-        });
+        }
         if (lane == 0 && pos != cnt) atomicOr(a.status, ERR_COUNT_MISMATCH);
     }
     gsync<GT>(bar);
@@ -884,7 +1017,7 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
         if (!reuse) {
             if (a.want_pattern && cidx >= 0) {
                 const long long co = clock64();
-                output_chain<GT, GBM>(a, md.line_base, pass, bm, summ, sh, gtid, bar);
+                output_chain<GT, GBM>(a, md.line_base, pass, bm, summ, sh, fr.spill, gtid, bar);
                 if (gtid == 0) sh.prof[5] += (unsigned long long)(clock64() - co);
             }
             const long long cc = clock64();
@@ -919,7 +1052,7 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
     // the piece's last chain
     if (a.want_pattern && cidx >= 0) {
         const long long co = clock64();
-        output_chain<GT, GBM>(a, md.line_base, pass, bm, summ, sh, gtid, bar);
+        output_chain<GT, GBM>(a, md.line_base, pass, bm, summ, sh, fr.spill, gtid, bar);
         if (gtid == 0) {
             sh.prof[5] += (unsigned long long)(clock64() - co);
             sh.chain_len = 0;

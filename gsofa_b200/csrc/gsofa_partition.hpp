@@ -32,12 +32,17 @@ namespace part {
 // inspected edge of a traversal that starts afresh).  A traversal starts
 // afresh at the first source of every work piece and then expands all of
 // X(s), whose size is bounded by s's descendants in the elimination tree of
-// A + A^T.  Work pieces are n / (8 x 148) sources long on a 148-SM GPU,
-// between 32 and 512, whether the kernel runs the whole matrix or a range.
+// A + A^T.  Work pieces of a range of r lines of an n-line matrix are
+// max(r / 8G, min(n / 8G, r / 4G)) sources long on a GPU of G = 148 SMs,
+// between 32 and 512.
 constexpr double kCostPerSource = 7000.0;
 constexpr double kCostPerEntry = 2.6;
 constexpr double kCostPerEdge = 3.2;
-inline double piece_len(int32_t n) { return std::min(512.0, std::max(32.0, (double)n / 1184.0)); }
+inline double piece_len(int32_t n, int32_t parts)
+{
+    const double r = (double)n / (double)std::max(parts, 1), g8 = 8.0 * 148.0;
+    return std::min(512.0, std::max(32.0, std::max(r / g8, std::min((double)n / g8, 2.0 * r / g8))));
+}
 
 struct Sym {
     std::vector<int64_t> ptr;   // [n+1]
@@ -196,7 +201,7 @@ inline void partition(int32_t n, const int32_t *beg, const int32_t *end, const i
     for (int32_t v = 0; v < n; v++)    // parent[v] > v: children first
         if (parent[(size_t)v] != -1) sub[(size_t)parent[(size_t)v]] += sub[(size_t)v];
     std::vector<double> pre((size_t)n + 1, 0.0);
-    const double kPieceLen = piece_len(n);
+    const double kPieceLen = piece_len(n, parts);
     for (int32_t v = 0; v < n; v++) {
         const double fresh = (sub[(size_t)v] - (double)(s.ptr[(size_t)v + 1] - s.ptr[(size_t)v])) / 2.0;
         pre[(size_t)v + 1] = pre[(size_t)v] + 2.0 * kCostPerSource +

@@ -1,9 +1,14 @@
 """Serving loops: symbolic factorizations as a request stream on one GPU.
 
-ContinuousServer (the serving path) drives the persistent kernel of
-StreamServer: each request is uploaded and published as soon as it arrives
-and fits, and its work pieces run on whichever CTAs free up, overlapping
-with every request already on the device.
+ContinuousServer (the serving path) serves by size class.  Small requests
+(fewer than LARGE_REQUEST_N lines) go to the persistent kernel of
+StreamServer: each is uploaded and published as soon as it arrives and fits,
+and its work pieces run on whichever CTAs free up, overlapping with every
+request already on the device -- many small matrices share the GPU, where
+alone each would leave most SMs idle.  A large request fills the GPU on its
+own: it runs alone on the factorization kernel (shared-memory state, all
+warps of an SM on two traversals) once the requests on the device finish,
+instead of inside the serving kernel's smaller global-state traversals.
 
 Server batches at launch granularity instead: whenever the GPU finishes a
 persistent launch, every request that has arrived in the meantime and fits
@@ -31,6 +36,12 @@ import numpy as np
 
 from . import Context, Params, Result
 from .matgen import Graph
+
+
+# Lines from which a request runs alone on the factorization kernel instead of
+# sharing the persistent serving kernel (the serving kernel's own priority
+# classes split at the same size).
+LARGE_REQUEST_N = 65536
 
 
 @dataclasses.dataclass
@@ -186,7 +197,10 @@ class ContinuousServer:
     """Serves a request stream on the persistent kernel (StreamServer):
     every request is published as soon as it arrives and fits, and runs
     alongside whatever is already on the device.  Requests that do not fit
-    wait (admission by device bytes) until finished ones are fetched."""
+    wait (admission by device bytes) until finished ones are fetched.
+    Requests of more than max_n lines (the large class) run alone through
+    `oversize` once the device is drained; later requests wait behind them in
+    arrival order."""
 
     def __init__(self, server, poll_interval_s: float = 0.0005,
                  oversize: Optional[Callable[[Graph], Result]] = None, max_n: Optional[int] = None,
@@ -221,6 +235,7 @@ class ContinuousServer:
         started: Dict[int, float] = {}
         arrived: Dict[int, float] = {}
         done: List[Completion] = []
+        alone = 0                                  # large-class requests run on their own
         last_progress = now()
         while pending or waiting or inflight or (lazy is not None and nxt < total):
             t = now()
@@ -249,6 +264,7 @@ class ContinuousServer:
                         break                      # finish what runs, then take it alone
                     self.server.drain()
                     res = self.oversize(r.graph)
+                    alone += 1
                     waiting.popleft()
                     c = Completion(r.rid, arrived.pop(r.rid, r.arrival_s), st, now(), res)
                     done.append(c)
@@ -287,6 +303,7 @@ class ContinuousServer:
             "factorizations_per_s": len(done) / span if span > 0 else None,
             "nnz_lu_per_s": sum(c.result.nnz_lu for c in done) / span if span > 0 else None,
             "span_s": span,
+            "run_alone": alone,
         }
         return {"report": report, "completions": sorted(done, key=lambda c: c.rid)}
 
