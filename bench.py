@@ -465,7 +465,7 @@ def serve_main(args):
         "config": {k: out[k] for k in ("workload", "requests", "admission_budget_gb", "pattern", "seed",
                                        "generation")},
         "serving": rep, "comparison": out["comparison"], "results_identical": out["results_identical"],
-        "serving_kernel_max_n": out["serving_kernel_max_n"],
+        "serving_kernel_max_n": out["serving_kernel_max_n"], "size_classes": out["size_classes"],
         "factorizations_per_s": rep["factorizations_per_s"],
         "clocks": out["clocks"], "gpu_launches": None,
     }
