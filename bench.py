@@ -696,8 +696,9 @@ def sharded_main(args, world, rank, local):
     ranges of equal predicted work (gsofa_partition_lines), each rank
     factorizing its range with traversal reuse; the per-line arrays are then
     summed over NCCL (distributed.symbfact_sharded).  Total work is fixed as N
-    grows: strong scaling.  value = factorizations of the whole matrix per
-    second, timed on the device as the max over ranks."""
+    grows: strong scaling.  value = nnz(L+U) of the whole matrix per second
+    (whole-matrix factorizations x nnz(L+U)), timed on the device as the max
+    over ranks."""
     import torch
     import torch.distributed as dist
     import gsofa_b200
