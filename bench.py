@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["nd3d", "plain2d", "circuit", "bundled", "batch", "serve"],
+    ap.add_argument("--workload", choices=["nd3d", "plain2d", "circuit", "bundled", "batch", "serve", "order"],
                     default="nd3d")
     ap.add_argument("--batch-count", type=int, default=256,
                     help="matrices in the batch workload (also measured beside the default line; 0: skip)")
@@ -411,7 +411,7 @@ def serving_run(ctx, count, nmax, rate, compare, pool_procs=16):
     pool = mp.get_context("spawn").Pool(min(pool_procs, os.cpu_count() or 1))
     params = gsofa_b200.Params.default(want_pattern=0)
     srv = gsofa_b200.StreamServer(0, mem_budget_bytes=120 << 30)
-    oversize = lambda g: ctx.symbfact(ctx.upload(g), params)  # noqa: E731
+    oversize = lambda g: serve.run_alone(ctx, g, params)  # noqa: E731
     # size classes: small requests share the persistent serving kernel, large
     # ones run alone on the factorization kernel
     cs = serve.ContinuousServer(srv, oversize=oversize, max_n=min(srv.max_n, serve.LARGE_REQUEST_N - 1))
@@ -447,6 +447,63 @@ def serving_run(ctx, count, nmax, rate, compare, pool_procs=16):
             "clocks": clk.summary(),
             "generation": "process pool, in arrival order, while serving (a request arrives when both "
                           "its time and its matrix have come)"}
+
+
+def order_main(args):
+    """The step before the path: reverse Cuthill-McKee on the GPU
+    (gsofa_order_rcm) of the power-law circuit pattern before it is ordered
+    (n = 659,033, the same shuffle the circuit workload's generator orders
+    with scipy), timed end to end through the public call (host arrays in,
+    permutation out), against the oracle's sequential restatement on one
+    host core; parity is bit-exact, and the ordered pattern is factorized
+    (counts) to report the fill the ordering leaves."""
+    import torch
+    import gsofa_b200
+    import oracle
+    from gsofa_b200 import matgen
+    torch.cuda.set_device(0)
+    g = matgen.powerlaw(659_033, seed=matgen.SEEDS["circuit"], ordering="random")
+    ctx = gsofa_b200.Context(0)
+    for _ in range(args.warmup):
+        perm = ctx.order_rcm(g)
+    times = []
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            perm = ctx.order_rcm(g)
+            times.append((time.perf_counter() - t0) * 1000.0)
+    t_cpu = time.perf_counter()
+    want = oracle.rcm(g.beg, g.end, g.adj)
+    t_cpu = (time.perf_counter() - t_cpu) * 1000.0
+    same = bool(np.array_equal(perm, want))
+    inv = np.empty(g.n, np.int64)
+    inv[perm] = np.arange(g.n)
+    rows = np.repeat(np.arange(g.n), g.end - g.beg)
+    band_in = int(np.abs(rows - g.adj.astype(np.int64)).max())
+    band_out = int(np.abs(inv[rows] - inv[g.adj]).max())
+    h = gsofa_b200.permute_lines(g, perm)
+    with ctx.upload(h) as m:
+        ordered = ctx.symbfact(m, gsofa_b200.Params.default(want_pattern=0, flags=gsofa_b200.FLAG_NO_DOWNLOAD))
+    ms = float(np.median(times))
+    line = {
+        "metric": "ordering time", "value": ms, "unit": "ms", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator)",
+        "config": {"workload": f"rcm_{g.name}", "n": g.n, "nnz": g.nnz,
+                   "ordering": "reverse Cuthill-McKee of A + A^T, George-Liu start, (degree, id) ties"},
+        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": int(4 * (2 * g.n + g.nnz)),
+                "d2h_bytes_per_step": int(4 * g.n)},
+        "cpu_baseline": {"value": t_cpu, "unit": "ms", "cores": 1, "kind": "port",
+                         "sample": "the whole matrix, once (sequential restatement)"},
+        "parity": {"perm_identical_to_oracle": same},
+        "bandwidth": {"input": band_in, "ordered": band_out},
+        "fill_after_ordering": {"nnz_lu": int(ordered.nnz_lu), "fill_count": int(ordered.fill_count),
+                                "factorization_kernel_ms": float(ordered.kernel_ms)},
+        "clocks": clk.summary(), "gpu_launches": None,
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0 if same else 1
 
 
 def serve_main(args):
@@ -817,6 +874,8 @@ def main():
         return batch_main(args)
     if args.workload == "serve":
         return serve_main(args)
+    if args.workload == "order":
+        return order_main(args)
 
     import torch
     import torch.distributed as dist

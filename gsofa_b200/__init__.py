@@ -264,6 +264,11 @@ def lib():
     L.gsofa_partition_lines.argtypes = [ctypes.c_int32, ctypes.c_int64, _i32p, _i32p, _i32p, ctypes.c_int32,
                                         _i32p, ctypes.POINTER(ctypes.c_double)]
     L.gsofa_partition_lines.restype = ctypes.c_int
+    L.gsofa_order_rcm.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, _i32p, _i32p, _i32p, _i32p]
+    L.gsofa_order_rcm.restype = ctypes.c_int
+    L.gsofa_permute_lines.argtypes = [ctypes.c_int32, ctypes.c_int64, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p,
+                                      _i32p]
+    L.gsofa_permute_lines.restype = ctypes.c_int
     L.gsofa_supernodes_from_lines.argtypes = [ctypes.c_int32, _i32p, ctypes.POINTER(ctypes.c_uint8),
                                               ctypes.c_int32, _i32p]
     L.gsofa_supernodes_from_lines.restype = ctypes.c_int32
@@ -363,6 +368,17 @@ class Matrix:
         if self._h:
             lib().gsofa_matrix_free(self._h)
             self._h = None
+            mats = self._ctx._mats
+            if mats and mats[-1] is self:
+                mats.pop()
+            elif self in mats:
+                mats.remove(self)
+
+    def __enter__(self) -> "Matrix":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.free()
 
     @property
     def handle(self):
@@ -420,6 +436,18 @@ class Context:
         m = Matrix(self, h, int(beg.shape[0]), int(adj.shape[0]))
         self._mats.append(m)
         return m
+
+    def order_rcm(self, g: Graph) -> np.ndarray:
+        """Reverse Cuthill-McKee order of A + A^T computed on the GPU
+        (gsofa_order_rcm): perm[new] = old, int32[n]."""
+        beg = np.ascontiguousarray(g.beg, dtype=np.int32)
+        end = np.ascontiguousarray(g.end, dtype=np.int32)
+        adj = np.ascontiguousarray(g.adj if g.nnz else np.zeros(1, np.int32), dtype=np.int32)
+        perm = np.zeros(max(g.n, 1), np.int32)
+        _check(lib().gsofa_order_rcm(self._h, int(g.n), int(g.nnz), beg.ctypes.data_as(_i32p),
+                                     end.ctypes.data_as(_i32p), adj.ctypes.data_as(_i32p),
+                                     perm.ctypes.data_as(_i32p)), "gsofa_order_rcm")
+        return perm[:g.n]
 
     def symbfact(self, m: Matrix, params: Optional[Params] = None, **kw) -> Result:
         p = params if params is not None else Params.default(**kw)
@@ -752,6 +780,26 @@ def partition_lines(g: Graph, parts: int):
     return cuts, work
 
 
+def permute_lines(g: Graph, perm) -> Graph:
+    """The symmetric permutation P A P^T (gsofa_permute_lines, host): new
+    line k is old line perm[k], ids renamed, lines sorted and packed."""
+    beg = np.ascontiguousarray(g.beg, dtype=np.int32)
+    end = np.ascontiguousarray(g.end, dtype=np.int32)
+    adj = np.ascontiguousarray(g.adj if g.nnz else np.zeros(1, np.int32), dtype=np.int32)
+    p = np.ascontiguousarray(perm, dtype=np.int32)
+    if p.shape != (g.n,):
+        raise GsofaError(1, "perm must have n entries")
+    total = int((end.astype(np.int64) - beg).sum()) if g.n else 0
+    ob = np.zeros(max(g.n, 1), np.int32)
+    oe = np.zeros(max(g.n, 1), np.int32)
+    oa = np.zeros(max(total, 1), np.int32)
+    _check(lib().gsofa_permute_lines(int(g.n), int(g.nnz), beg.ctypes.data_as(_i32p), end.ctypes.data_as(_i32p),
+                                     adj.ctypes.data_as(_i32p), p.ctypes.data_as(_i32p), ob.ctypes.data_as(_i32p),
+                                     oe.ctypes.data_as(_i32p), oa.ctypes.data_as(_i32p)), "gsofa_permute_lines")
+    name = f"{g.name}_perm" if getattr(g, "name", "") else "permuted"
+    return Graph(g.n, ob[:g.n], oe[:g.n], oa[:total], name)
+
+
 def predict_line_counts(g: Graph) -> np.ndarray:
     """Upper bound on every line's |U row| and |L column| from the symmetric
     structure A + A^T (exact for symmetric patterns); host-only."""
@@ -790,7 +838,7 @@ def exported_symbols() -> List[str]:
             "gsofa_result_supernodal_sizes", "gsofa_result_supernodal_fetch",
             "gsofa_predict_scratch_bytes",
             "gsofa_symbfact_counts_noalloc", "gsofa_supernodes_from_lines", "gsofa_partition_lines",
-            "gsofa_predict_line_counts",
+            "gsofa_predict_line_counts", "gsofa_order_rcm", "gsofa_permute_lines",
             "gsofa_server_create",
             "gsofa_server_destroy", "gsofa_server_request_bytes", "gsofa_server_submit",
             "gsofa_server_poll", "gsofa_server_result", "gsofa_server_drain"]

@@ -10,6 +10,7 @@
 #include "gsofa_server.cuh"
 #include "gsofa_supernodal.cuh"
 #include "gsofa_partition.hpp"
+#include "gsofa_order.cuh"
 
 #include <cuda_runtime.h>
 
@@ -95,6 +96,7 @@ struct gsofa_ctx {
     DevBuf queue, cnt, nxt, poff, gptr, lrow, snind, snlist, tiles, misc, pool, out, mats, ranges, stamp;
     DevBuf gstate;            // visited bitmaps of the global-state kernels
     DevBuf blk;               // streaming: written entries per pool block
+    DevBuf order;             // gsofa_order_rcm: symmetric structure, levels, sort space
     unsigned int *h_blk = nullptr;   // page-locked mirror of blk
     size_t h_blk_cap = 0;
     cudaStream_t s_poll = nullptr, s_copy = nullptr;   // streaming: counter reads, block copies
@@ -109,7 +111,7 @@ struct gsofa_ctx {
     DevBuf matinfo;
     GraphCache graph;         // last captured job (GSOFA_FLAG_GRAPH)
     // launch shapes already sized: (block, bitmap words) -> (ring, CTAs/SM)
-    struct Shape { int block; int32_t words; bool paired; bool gbm; bool wide; int ring; int occ; };
+    struct Shape { int block; int32_t words; bool paired; bool gbm; bool wide; bool lists; int ring; int occ; };
     std::vector<Shape> shapes;
 
     void *grow(DevBuf &b, size_t bytes)
@@ -225,17 +227,26 @@ int pick_block(int32_t max_n)
     return 512;
 }
 
-template <int BLOCK, bool PAIRED, bool GBM, int MINB = (BLOCK >= 1024 ? 1 : 1024 / BLOCK)>
+template <int BLOCK, bool PAIRED, bool GBM, int MINB = (BLOCK >= 1024 ? 1 : 1024 / BLOCK), bool LISTS = true>
 void *factor_fn()
 {
-    return (void *)factor_kernel<BLOCK, PAIRED, GBM, MINB>;
+    return (void *)factor_kernel<BLOCK, PAIRED, GBM, MINB, LISTS>;
 }
 
 // The factorization kernel for a launch shape: threads per CTA, the two
 // passes side by side (paired), the visited bitmaps in global memory (gbm),
 // registers budgeted for one CTA per SM (wide: the 512-thread paired form).
-void *factor_kernel_for(int block, bool paired, bool gbm = false, bool wide = false)
+// lists: the job writes the pattern.  Counts-only jobs of the shapes that
+// large matrices take run an instantiation without the list output (fewer
+// registers: no spills where the list output's code would cause them).
+void *factor_kernel_for(int block, bool paired, bool gbm = false, bool wide = false, bool lists = true)
 {
+    if (!lists && paired) {
+        if (gbm && block == 256) return factor_fn<256, true, true, 4, false>();
+        if (wide && block == 512) return factor_fn<512, true, false, 1, false>();
+        if (!gbm && !wide && block == 768) return factor_fn<768, true, false, 1, false>();
+        if (!gbm && !wide && block == 1024) return factor_fn<1024, true, false, 1, false>();
+    }
     if (gbm) {
         switch (block) {
         case 128: return paired ? factor_fn<128, true, true>() : factor_fn<128, false, true>();
@@ -404,7 +415,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
         else block = pick_block(max_n) * (paired ? 2 : 1);
     }
     if (wide && (!paired || gbm)) return GSOFA_ERR_INVALID_INPUT;
-    void *kfn = factor_kernel_for(block, paired, gbm, wide);
+    void *kfn = factor_kernel_for(block, paired, gbm, wide, want_pattern != 0);
     if (!kfn) return GSOFA_ERR_INVALID_INPUT;
     const int NS = paired ? 2 : 1;
     int lanes = p.threads_per_source ? p.threads_per_source : 1;
@@ -424,7 +435,8 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
     size_t smem = 0;
     bool cached = false;
     for (const auto &sh : ctx->shapes)
-        if (sh.block == block && sh.words == bitmap_words && sh.paired == paired && sh.gbm == gbm && sh.wide == wide) {
+        if (sh.block == block && sh.words == bitmap_words && sh.paired == paired && sh.gbm == gbm && sh.wide == wide &&
+            sh.lists == (want_pattern != 0)) {
             ring = sh.ring; occ = sh.occ; cached = true;
         }
     if (cached) {
@@ -440,7 +452,7 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
             if (o > occ) { occ = o; ring = cand; smem = sm; }
         }
         if (occ <= 0) return GSOFA_ERR_UNSUPPORTED;
-        ctx->shapes.push_back({block, bitmap_words, paired, gbm, wide, ring, occ});
+        ctx->shapes.push_back({block, bitmap_words, paired, gbm, wide, want_pattern != 0, ring, occ});
     }
     int per_sm = p.ctas_per_sm > 0 ? std::min(p.ctas_per_sm, occ) : occ;
     int grid = per_sm * ctx->sm_count;
@@ -935,7 +947,7 @@ void gsofa_destroy(gsofa_ctx *c)
     DevBuf *bufs[] = {&c->queue, &c->cnt, &c->nxt, &c->poff, &c->gptr, &c->lrow, &c->snind,
                       &c->snlist, &c->tiles, &c->misc, &c->pool, &c->out, &c->mats, &c->ranges,
                       &c->st_beg, &c->st_end, &c->st_adj, &c->st_tmp, &c->matinfo, &c->stamp,
-                      &c->sn_head, &c->sn_data, &c->gstate, &c->blk};
+                      &c->sn_head, &c->sn_data, &c->gstate, &c->blk, &c->order};
     for (DevBuf *b : bufs) c->release(*b);
     for (DevBuf &b : c->slabs) cudaFree(b.p);
     c->slabs.clear();
@@ -1444,6 +1456,207 @@ gsofa_status gsofa_partition_lines(int32_t n, int64_t nnz, const int32_t *beg, c
     if (parts <= 0 || !cuts || !valid_lines(n, nnz, beg, end, adj)) return GSOFA_ERR_INVALID_INPUT;
     try {
         gsofa::part::partition(n, beg, end, adj, parts, cuts, work);
+    } catch (std::bad_alloc &) {
+        return GSOFA_ERR_OOM;
+    }
+    return GSOFA_OK;
+}
+
+gsofa_status gsofa_order_rcm(gsofa_ctx *c, int32_t n, int64_t nnz, const int32_t *beg, const int32_t *end,
+                             const int32_t *adj, int32_t *perm)
+{
+    if (!c || (n > 0 && !perm) || !valid_lines(n, nnz, beg, end, adj)) return GSOFA_ERR_INVALID_INPUT;
+    if (n == 0) return GSOFA_OK;
+    try {
+        GS_CUDA(cudaSetDevice(c->device));
+        cudaStream_t st = c->stream;
+        // key slots: two per entry of every line's range
+        std::vector<int64_t> off((size_t)n + 1);
+        off[0] = 0;
+        for (int32_t v = 0; v < n; v++) off[(size_t)v + 1] = off[(size_t)v] + 2 * (int64_t)(end[v] - beg[v]);
+        const int64_t total = off[(size_t)n];
+        if (total > INT32_MAX) return GSOFA_ERR_UNSUPPORTED;   // one radix sort holds at most 2^31 keys
+        const int64_t nk = std::max<int64_t>(std::max<int64_t>(total, n), 1);
+        size_t sort_tmp = 0, uniq_tmp = 0;
+        GS_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, sort_tmp, (unsigned long long *)nullptr,
+                                               (unsigned long long *)nullptr, (int)nk, 0, 64, st));
+        GS_CUDA(cub::DeviceSelect::Unique(nullptr, uniq_tmp, (unsigned long long *)nullptr,
+                                          (unsigned long long *)nullptr, (int *)nullptr, (int)nk, st));
+        const size_t tmp_bytes = std::max(sort_tmp, uniq_tmp);
+        // one scratch block: every part 256-byte aligned
+        size_t at = 0;
+        auto take = [&](size_t bytes) { const size_t o = at; at += (bytes + 255) / 256 * 256; return o; };
+        const size_t o_beg = take((size_t)n * 4), o_end = take((size_t)n * 4),
+                     o_adj = take((size_t)std::max<int64_t>(nnz, 1) * 4), o_off = take(((size_t)n + 1) * 8),
+                     o_ka = take((size_t)nk * 8), o_kb = take((size_t)nk * 8), o_sp = take(((size_t)n + 1) * 8),
+                     o_sa = take((size_t)nk * 4), o_ord = take((size_t)n * 4), o_pord = take((size_t)n * 4),
+                     o_rank = take((size_t)n * 4), o_bykey = take((size_t)n * 4), o_cm = take((size_t)n * 4),
+                     o_q = take((size_t)n * 4), o_next = take((size_t)n * 4), o_claim = take((size_t)n * 4),
+                     o_gen = take((size_t)n * 4), o_ctr = take(64), o_tmp = take(tmp_bytes);
+        char *base = (char *)c->grow(c->order, at);
+        int32_t *d_beg = (int32_t *)(base + o_beg), *d_end = (int32_t *)(base + o_end);
+        int32_t *d_adj = (int32_t *)(base + o_adj);
+        int64_t *d_off = (int64_t *)(base + o_off);
+        unsigned long long *ka = (unsigned long long *)(base + o_ka), *kb = (unsigned long long *)(base + o_kb);
+        int64_t *d_sp = (int64_t *)(base + o_sp);
+        int32_t *d_sa = (int32_t *)(base + o_sa), *d_ord = (int32_t *)(base + o_ord);
+        int32_t *d_pord = (int32_t *)(base + o_pord), *d_rank = (int32_t *)(base + o_rank);
+        int32_t *d_bykey = (int32_t *)(base + o_bykey), *d_cm = (int32_t *)(base + o_cm);
+        int32_t *d_q = (int32_t *)(base + o_q), *d_next = (int32_t *)(base + o_next);
+        uint32_t *d_claim = (uint32_t *)(base + o_claim), *d_gen = (uint32_t *)(base + o_gen);
+        unsigned long long *d_ctr = (unsigned long long *)(base + o_ctr);   // [0] tail, [1] count
+        int32_t *d_small = (int32_t *)(d_ctr + 4);                           // [0] zeros / start / least rank
+        void *d_tmp = base + o_tmp;
+        const int gridc = c->sm_count * 8;
+        auto blocks = [&](int64_t items, int per) {
+            return (unsigned)std::max<int64_t>(1, std::min<int64_t>((items + per - 1) / per, gridc));
+        };
+        auto read_ull = [&](const unsigned long long *d) {
+            unsigned long long h = 0;
+            GS_CUDA(cudaMemcpyAsync(&h, d, 8, cudaMemcpyDeviceToHost, st));
+            GS_CUDA(cudaStreamSynchronize(st));
+            return h;
+        };
+        auto read_i32 = [&](const int32_t *d) {
+            int32_t h = 0;
+            GS_CUDA(cudaMemcpyAsync(&h, d, 4, cudaMemcpyDeviceToHost, st));
+            GS_CUDA(cudaStreamSynchronize(st));
+            return h;
+        };
+
+        GS_CUDA(cudaMemcpyAsync(d_beg, beg, (size_t)n * 4, cudaMemcpyHostToDevice, st));
+        GS_CUDA(cudaMemcpyAsync(d_end, end, (size_t)n * 4, cudaMemcpyHostToDevice, st));
+        if (nnz > 0) GS_CUDA(cudaMemcpyAsync(d_adj, adj, (size_t)nnz * 4, cudaMemcpyHostToDevice, st));
+        GS_CUDA(cudaMemcpyAsync(d_off, off.data(), ((size_t)n + 1) * 8, cudaMemcpyHostToDevice, st));
+        // S = A + A^T: sorted distinct (row, column) keys, the diagonal last
+        int64_t count = 0;
+        if (total > 0) {
+            order_edge_keys_kernel<<<blocks((int64_t)n * 32, 256), 256, 0, st>>>(n, d_beg, d_end, d_adj, d_off, ka);
+            GS_CUDA(cudaGetLastError());
+            size_t tb = tmp_bytes;
+            GS_CUDA(cub::DeviceRadixSort::SortKeys(d_tmp, tb, ka, kb, (int)total, 0, 64, st));
+            tb = tmp_bytes;
+            GS_CUDA(cub::DeviceSelect::Unique(d_tmp, tb, kb, ka, (int *)(d_ctr + 1), (int)total, st));
+            count = (int64_t)(int32_t)(read_ull(d_ctr + 1) & 0xffffffffu);
+            if (count > 0 && read_ull(ka + count - 1) == ~0ull) count--;
+        }
+        order_rows_kernel<<<blocks(count + 1, 256), 256, 0, st>>>(n, ka, count, d_sp, d_sa);
+        GS_CUDA(cudaGetLastError());
+        // ranks by (degree, id); degree-0 vertices placed first
+        order_init_kernel<<<blocks(n, 256), 256, 0, st>>>(n, d_sp, kb, d_ord, d_pord, d_claim, d_gen);
+        GS_CUDA(cudaGetLastError());
+        {
+            size_t tb = tmp_bytes;
+            GS_CUDA(cub::DeviceRadixSort::SortKeys(d_tmp, tb, kb, ka, (int)n, 0, 64, st));
+        }
+        GS_CUDA(cudaMemsetAsync(d_small, 0, 4, st));
+        order_ranks_kernel<<<blocks(n, 256), 256, 0, st>>>(n, ka, d_bykey, d_rank, d_ord, d_cm, d_small);
+        GS_CUDA(cudaGetLastError());
+        std::vector<int32_t> bykey((size_t)n);
+        GS_CUDA(cudaMemcpyAsync(bykey.data(), d_bykey, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
+        int32_t pos = read_i32(d_small), cursor = pos;
+        uint32_t g = 0;
+
+        // breadth-first search from r over the unordered vertices: returns
+        // its eccentricity and the vertex of least key in its last level
+        auto bfs = [&](int32_t r, int32_t *last_min) -> int32_t {
+            ++g;
+            GS_CUDA(cudaMemcpyAsync(d_q, &r, 4, cudaMemcpyHostToDevice, st));
+            GS_CUDA(cudaMemcpyAsync(d_gen + r, &g, 4, cudaMemcpyHostToDevice, st));
+            const unsigned long long one = 1;
+            GS_CUDA(cudaMemcpyAsync(d_ctr, &one, 8, cudaMemcpyHostToDevice, st));
+            int64_t f0 = 0, f1 = 1;
+            int32_t ecc = 0;
+            for (;;) {
+                order_bfs_kernel<<<blocks((f1 - f0) * 32, 256), 256, 0, st>>>(f0, f1, d_q, d_sp, d_sa, d_ord, d_gen, g,
+                                                                           d_ctr);
+                GS_CUDA(cudaGetLastError());
+                const int64_t t = (int64_t)read_ull(d_ctr);
+                if (t == f1) break;
+                f0 = f1;
+                f1 = t;
+                ecc++;
+            }
+            const int32_t big = INT32_MAX;
+            GS_CUDA(cudaMemcpyAsync(d_small, &big, 4, cudaMemcpyHostToDevice, st));
+            order_min_rank_kernel<<<blocks(f1 - f0, 256), 256, 0, st>>>(f0, f1, d_q, d_rank, d_small);
+            GS_CUDA(cudaGetLastError());
+            *last_min = bykey[(size_t)read_i32(d_small)];
+            return ecc;
+        };
+
+        while (pos < n) {
+            order_find_start_kernel<<<1, 1024, 0, st>>>(n, d_bykey, d_ord, cursor, d_small);
+            GS_CUDA(cudaGetLastError());
+            cursor = read_i32(d_small);
+            if (cursor >= n) throw CudaFail{cudaErrorUnknown};   // cannot happen: pos < n leaves a vertex
+            // George-Liu pseudo-peripheral vertex of the component
+            int32_t r = bykey[(size_t)cursor], cnd = -1;
+            int32_t ecc = bfs(r, &cnd);
+            for (;;) {
+                int32_t c2 = -1;
+                const int32_t ecc_c = bfs(cnd, &c2);
+                if (ecc_c <= ecc) break;
+                r = cnd;
+                ecc = ecc_c;
+                cnd = c2;
+            }
+            // Cuthill-McKee levels from r
+            GS_CUDA(cudaMemcpyAsync(d_ord + r, &pos, 4, cudaMemcpyHostToDevice, st));
+            GS_CUDA(cudaMemcpyAsync(d_cm + pos, &r, 4, cudaMemcpyHostToDevice, st));
+            int32_t l0 = pos, l1 = pos + 1;
+            pos++;
+            for (;;) {
+                GS_CUDA(cudaMemsetAsync(d_ctr, 0, 8, st));
+                order_cm_kernel<<<blocks((int64_t)(l1 - l0) * 32, 256), 256, 0, st>>>(l0, l1, d_cm, d_sp, d_sa, d_ord,
+                                                                                    d_pord, d_claim, d_next, d_ctr);
+                GS_CUDA(cudaGetLastError());
+                const int64_t m = (int64_t)read_ull(d_ctr);
+                if (m == 0) break;
+                order_level_keys_kernel<<<blocks(m, 256), 256, 0, st>>>(m, d_next, d_pord, d_rank, ka);
+                GS_CUDA(cudaGetLastError());
+                size_t tb = tmp_bytes;
+                GS_CUDA(cub::DeviceRadixSort::SortKeys(d_tmp, tb, ka, kb, (int)m, 0, 64, st));
+                order_place_kernel<<<blocks(m, 256), 256, 0, st>>>(m, kb, d_bykey, pos, d_ord, d_cm);
+                GS_CUDA(cudaGetLastError());
+                l0 = pos;
+                pos += (int32_t)m;
+                l1 = pos;
+            }
+        }
+        std::vector<int32_t> cm((size_t)n);
+        GS_CUDA(cudaMemcpyAsync(cm.data(), d_cm, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
+        GS_CUDA(cudaStreamSynchronize(st));
+        for (int32_t k = 0; k < n; k++) perm[k] = cm[(size_t)(n - 1 - k)];
+    } catch (CudaFail &f) {
+        return fail_cuda(f.e);
+    } catch (std::bad_alloc &) {
+        return GSOFA_ERR_OOM;
+    }
+    return GSOFA_OK;
+}
+
+gsofa_status gsofa_permute_lines(int32_t n, int64_t nnz, const int32_t *beg, const int32_t *end,
+                                 const int32_t *adj, const int32_t *perm, int32_t *out_beg, int32_t *out_end,
+                                 int32_t *out_adj)
+{
+    if ((n > 0 && (!perm || !out_beg || !out_end)) || !valid_lines(n, nnz, beg, end, adj))
+        return GSOFA_ERR_INVALID_INPUT;
+    try {
+        std::vector<int32_t> inv((size_t)n, -1);
+        for (int32_t k = 0; k < n; k++) {
+            if (perm[k] < 0 || perm[k] >= n || inv[(size_t)perm[k]] >= 0) return GSOFA_ERR_INVALID_INPUT;
+            inv[(size_t)perm[k]] = k;
+        }
+        int64_t w = 0;
+        for (int32_t k = 0; k < n; k++) {
+            const int32_t v = perm[k];
+            if (end[v] > beg[v] && !out_adj) return GSOFA_ERR_INVALID_INPUT;
+            out_beg[k] = (int32_t)w;
+            for (int32_t j = beg[v]; j < end[v]; j++) out_adj[w++] = inv[(size_t)adj[j]];
+            std::sort(out_adj + out_beg[k], out_adj + w);
+            out_end[k] = (int32_t)w;
+        }
     } catch (std::bad_alloc &) {
         return GSOFA_ERR_OOM;
     }

@@ -315,6 +315,8 @@ struct SharedState {
     int stail;        // entries of the next level, counted while warp 0 runs levels alone
     int solo_start, solo_wstart, solo_count;   // where such a run ended
     int64_t warp[32]; // per-warp entry counts of a chain's last list (list output)
+    int64_t last_off; // pool offset of a chain's last list (-1: pool short)
+    int last_cnt;     // its entries
     // tallies kept by the half's first thread only: levels, then cycles of
     // seeding, level loop, range fold, count and link flag, list output (per
     // chain), bitmap clearing, wait for the other pass; sources; reused
@@ -794,14 +796,27 @@ __device__ void output_chain(const JobArgs &a, int64_t line_base, int pass, cons
     const unsigned below = (1u << lane) - 1u;
     const int s0 = sh.chain_s0, len = sh.chain_len;
     const int64_t row0 = (int64_t)pass * a.L + line0;   // cnt / poff entry of s0
-    // warp 0: one pool range for the chain, then every list's offset
+
+    // The last source's list: set bits in words from w0 on (first_mask on
+    // w0), chunks [c_lo, c_hi) shared out among the warps.  Every warp counts
+    // its share (shared memory only) while warp 0 also takes the chain's pool
+    // range and writes every list's offset; one barrier then covers both.
+    const int s_last = s0 + len - 1;
+    const int chain_hi = sh.chain_hi;
+    const uint32_t *summ2 = summ + bm_summary_words(bm, summ);
+    const int w0 = (s_last + 1) >> 5;
+    const uint32_t first_mask = ~0u << ((s_last + 1) & 31);
+    const int c_lo = w0 >> 5;
+    const int c_hi = chain_hi > s_last ? (chain_hi >> 10) + 1 : c_lo;
+    const int share = (max(c_hi - c_lo, 0) + NWARP - 1) / NWARP;
+    const int my_lo = c_lo + wid * share, my_hi = min(c_hi, my_lo + share);
     if (wid == 0) {
+        // one exact range per chain (one global atomic per chain of sources,
+        // so the pool holds the lists with no gaps); past the capacity the
+        // chain's lists are not written, the tail still advances, and its
+        // final value is the capacity the job needs
         long long base = -1;
         if (lane == 0) {
-            // one exact range per chain (one global atomic per chain of
-            // sources, so the pool holds the lists with no gaps); past the
-            // capacity the chain's lists are not written, the tail still
-            // advances, and its final value is the capacity the job needs
             const int64_t total = sh.chain_total;
             base = 0;
             if (total > 0) {
@@ -821,34 +836,26 @@ __device__ void output_chain(const JobArgs &a, int64_t line_base, int pass, cons
                 const long long y = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= o) incl += y;
             }
-            if (i < len) a.poff[row0 + i] = base >= 0 ? base + carry + incl - c : -1;
+            const long long off = base >= 0 ? base + carry + incl - c : -1;
+            if (i < len) a.poff[row0 + i] = off;
+            if (i == len - 1) {
+                sh.last_off = off;
+                sh.last_cnt = (int)c;
+            }
             carry += __shfl_sync(0xffffffffu, incl, 31);
         }
     }
-    gsync<GT>(bar);
-
-    // the last source's list: set bits in words from w0 on (first_mask on
-    // w0), chunks [c_lo, c_hi) shared out among the warps
-    const int s_last = s0 + len - 1;
-    const int64_t off_last = a.poff[row0 + len - 1];
-    const int cnt_last = a.cnt[row0 + len - 1];
-    const int chain_hi = sh.chain_hi;
-    const bool write = off_last >= 0;   // else the pool is short: nothing is written
-    const uint32_t *summ2 = summ + bm_summary_words(bm, summ);
-    const int w0 = (s_last + 1) >> 5;
-    const uint32_t first_mask = ~0u << ((s_last + 1) & 31);
-    const int c_lo = w0 >> 5;
-    const int c_hi = chain_hi > s_last ? (chain_hi >> 10) + 1 : c_lo;
-    const int share = (max(c_hi - c_lo, 0) + NWARP - 1) / NWARP;
-    const int my_lo = c_lo + wid * share, my_hi = min(c_hi, my_lo + share);
     int mine = 0;
-    if (write && my_lo < my_hi)
+    if (my_lo < my_hi)
         for_nonzero_chunks<GBM>(summ2, my_lo, my_hi, [&](int cc) {
             mine += __popc(last_word<GBM>(bm, summ, cc, lane, w0, first_mask));
         });
     mine = (int)__reduce_add_sync(0xffffffffu, (unsigned)mine);
     if (lane == 0) sh.warp[wid] = mine;
     gsync<GT>(bar);
+    const int64_t off_last = sh.last_off;
+    const int cnt_last = sh.last_cnt;
+    const bool write = off_last >= 0;   // else the pool is short: nothing is written
     if (write) {
         int pos = 0, all = 0;
         for (int k = 0; k < NWARP; k++) {
@@ -985,7 +992,7 @@ struct Tally {
 
 // The sources s_lo, s_lo + stride, ... < s_hi of one work piece, in order,
 // each starting from the previous source's state whenever that is valid.
-template <int BLOCK, bool PAIRED, bool CG, bool GBM>
+template <int BLOCK, bool PAIRED, bool CG, bool GBM, bool LISTS = true>
 __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &g, int pass,
                           int32_t s_lo, int32_t s_hi, int32_t stride, uint32_t *bm, uint32_t *summ,
                           const Frontier &fr, SharedState &sh, int (*pair_flag)[2], int half,
@@ -1015,7 +1022,7 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
             }
         }
         if (!reuse) {
-            if (a.want_pattern && cidx >= 0) {
+            if (LISTS && a.want_pattern && cidx >= 0) {
                 const long long co = clock64();
                 output_chain<GT, GBM>(a, md.line_base, pass, bm, summ, sh, fr.spill, gtid, bar);
                 if (gtid == 0) sh.prof[5] += (unsigned long long)(clock64() - co);
@@ -1050,7 +1057,7 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
         if (gtid == 0) sh.nsrc++;
     }
     // the piece's last chain
-    if (a.want_pattern && cidx >= 0) {
+    if (LISTS && a.want_pattern && cidx >= 0) {
         const long long co = clock64();
         output_chain<GT, GBM>(a, md.line_base, pass, bm, summ, sh, fr.spill, gtid, bar);
         if (gtid == 0) {
@@ -1081,7 +1088,9 @@ __device__ void run_piece(const JobArgs &a, const MatDesc &md, const PassGraph &
 // MINB: resident CTAs per SM the registers are budgeted for (the default
 // fills the SM with 1024 threads; 1 gives a 512-thread CTA up to 128
 // registers a thread, for launches that hold one CTA per SM anyway).
-template <int BLOCK, bool PAIRED, bool GBM, int MINB = (BLOCK >= 1024 ? 1 : 1024 / BLOCK)>
+// LISTS: the list output is compiled in; counts-only jobs run an
+// instantiation without it, whose registers go to the traversal alone.
+template <int BLOCK, bool PAIRED, bool GBM, int MINB = (BLOCK >= 1024 ? 1 : 1024 / BLOCK), bool LISTS = true>
 __global__ void __launch_bounds__(BLOCK, MINB) factor_kernel(JobArgs a)
 {
     constexpr int GT = PAIRED ? BLOCK / 2 : BLOCK;
@@ -1155,7 +1164,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) factor_kernel(JobArgs a)
             s_lo = sh.seg[0];
             s_hi = sh.seg[1];
         }
-        run_piece<BLOCK, PAIRED, false, GBM>(a, md, g, pass, s_lo, s_hi, rg.stride, bm, summ, fr, sh, pair_flag,
+        run_piece<BLOCK, PAIRED, false, GBM, LISTS>(a, md, g, pass, s_lo, s_hi, rg.stride, bm, summ, fr, sh, pair_flag,
                                         half, gtid, bar, acc);
         // the next piece starts from an empty bitmap
         {

@@ -128,7 +128,7 @@ __global__ void __maxnreg__(64) serve_kernel(ServeArgs sa)
         const ServePiece piece =
             load_cg(sa.pieces + (unsigned long long)s_class * sa.piece_cap + (pc % (long long)sa.piece_cap));
         const MatDesc md = load_cg(sa.slots + piece.slot);
-        run_piece<BLOCK, true, true, GBM>(a, md, md.g[half], half, piece.s_lo, piece.s_hi, 1, bm, summ, fr, sh,
+        run_piece<BLOCK, true, true, GBM, false>(a, md, md.g[half], half, piece.s_lo, piece.s_hi, 1, bm, summ, fr, sh,
                                      pair_flag, half, gtid, bar, acc);
         {
             const int clo = sh.chain_lo, chi = sh.chain_hi;

@@ -227,11 +227,12 @@ def powerlaw(n: int, alpha: float = 2.1, cap: int = 4000, local_frac: float = 0.
     diag = np.arange(n, dtype=np.int64)
     rows = np.concatenate([rows, diag])
     cols = np.concatenate([cols, diag])
-    if ordering == "rcm":
+    if ordering in ("rcm", "random"):
         perm = rng.permutation(n).astype(np.int64)      # new_id after the shuffle
         rows, cols = perm[rows], perm[cols]
-        new_id = rcm_order(n, rows, cols)
-        rows, cols = new_id[rows], new_id[cols]
+        if ordering == "rcm":
+            new_id = rcm_order(n, rows, cols)
+            rows, cols = new_id[rows], new_id[cols]
     elif ordering != "natural":
         raise ValueError(f"unknown ordering {ordering!r}")
     return _csr_from_pairs(n, rows, cols, f"powerlaw_{n}_{ordering}")

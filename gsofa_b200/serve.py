@@ -308,6 +308,13 @@ class ContinuousServer:
         return {"report": report, "completions": sorted(done, key=lambda c: c.rid)}
 
 
+def run_alone(ctx: Context, g: Graph, params: Optional[Params] = None) -> Result:
+    """One request alone on the factorization kernel (the large class):
+    upload, factorize, free the matrix."""
+    with ctx.upload(g) as m:
+        return ctx.symbfact(m, params if params is not None else Params.default(want_pattern=0))
+
+
 def one_at_a_time(ctx: Context, requests: Sequence[Request], params: Optional[Params] = None,
                   clock: Callable[[], float] = time.perf_counter) -> Dict:
     """The same stream served one request per launch (no batching)."""

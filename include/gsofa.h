@@ -355,6 +355,27 @@ gsofa_status gsofa_predict_line_counts(int32_t n, int64_t nnz, const int32_t *be
                                        const int32_t *end, const int32_t *adj,
                                        int64_t *counts);
 
+/* Fill-reducing ordering on the GPU, the step before the factorization (the
+ * reference takes its colbeg/colend/csr input already ordered): reverse
+ * Cuthill-McKee on the symmetric structure A + A^T of the host triple.  The
+ * order is exactly the sequential algorithm's with every tie broken by
+ * (degree, vertex id): each component (taken in that key order) starts at
+ * George and Liu's pseudo-peripheral vertex, each vertex's unordered
+ * neighbours follow it in key order, and the whole sequence is reversed.
+ * perm (n entries) receives perm[new] = old.  Uses the context's device and
+ * stream; scratch (about 40 bytes per entry and 60 per line) counts against
+ * its budget.  GSOFA_ERR_UNSUPPORTED past 2^30 entries. */
+gsofa_status gsofa_order_rcm(gsofa_ctx *ctx, int32_t n, int64_t nnz, const int32_t *colbeg,
+                             const int32_t *colend, const int32_t *csr, int32_t *perm);
+
+/* The symmetric permutation P A P^T of a host triple: new line k is old line
+ * perm[k] with every id v renamed to the new position of v, each line sorted,
+ * packed in order (out_colbeg[k] .. out_colend[k] in out_csr, which holds
+ * the sum of the input lines' lengths).  Host-only. */
+gsofa_status gsofa_permute_lines(int32_t n, int64_t nnz, const int32_t *colbeg, const int32_t *colend,
+                                 const int32_t *csr, const int32_t *perm, int32_t *out_colbeg,
+                                 int32_t *out_colend, int32_t *out_csr);
+
 /* Device scratch bytes a factorization of an n-line, nnz-entry matrix needs
  * with these parameters, excluding the pattern pool (admission control). */
 size_t gsofa_predict_scratch_bytes(const gsofa_ctx *ctx, int32_t n, int64_t nnz,

@@ -62,6 +62,8 @@ def lib():
         L.gsofa_oracle_maxid_line.argtypes = [ctypes.c_int32, _i32p, _i32p, _i32p, ctypes.c_int64,
                                               ctypes.c_int32, _i32p]
         L.gsofa_oracle_maxid_line.restype = ctypes.c_int32
+        L.gsofa_oracle_rcm.argtypes = [ctypes.c_int32, _i32p, _i32p, _i32p, ctypes.c_int64, _i32p]
+        L.gsofa_oracle_rcm.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -208,3 +210,15 @@ def symbfact(beg, end, adj, want_pattern: bool = True, max_supernode_size: int =
         res.update(u_ptr=uptr, u_idx=uidx, l_ptr=lptr, l_idx=lidx)
         res["l_row_count"] = np.bincount(lidx, minlength=n).astype(np.int32)
     return res
+
+
+def rcm(beg, end, adj):
+    """Reverse Cuthill-McKee order of A + A^T (perm[new] = old), with the
+    tie-breaking rules of gsofa_oracle.c."""
+    beg, end, adj = _inputs(beg, end, adj)
+    n = beg.shape[0]
+    perm = np.zeros(n, np.int32)
+    rc = lib().gsofa_oracle_rcm(n, _p(beg, _i32p), _p(end, _i32p), _p(adj, _i32p), adj.shape[0], _p(perm, _i32p))
+    if rc != 0:
+        raise ValueError(f"oracle rcm failed (rc={rc})")
+    return perm

@@ -407,3 +407,137 @@ int32_t gsofa_oracle_maxid_line(int32_t n, const int32_t *beg,
     free(cost); free(cstamp); free(mark); free(queue);
     return (int32_t)r;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Reverse Cuthill-McKee ordering (the step before the path: the reference
+ * takes its input already ordered).  Restates the published algorithms --
+ * Cuthill and McKee (1969), breadth-first levels with each vertex's unvisited
+ * neighbours appended by increasing degree; George and Liu (1979), the
+ * pseudo-peripheral start vertex; the order reversed at the end -- with every
+ * tie broken by vertex id, so the result is one well-defined permutation:
+ *
+ *   S = A + A^T without the diagonal and duplicates; deg(v) = |S(v)|; the
+ *   key of v is (deg(v), v).
+ *   While vertices remain: start = the unordered vertex of least key.
+ *     George-Liu: r = start; repeat { BFS from r; c = the vertex of least key
+ *     in the last level; if ecc(c) > ecc(r) then r = c else stop }.
+ *     Cuthill-McKee from r: a FIFO queue; each dequeued vertex appends its
+ *     unordered neighbours in key order.
+ *   perm[k] = the (n-1-k)-th vertex of the whole Cuthill-McKee sequence.
+ *
+ * perm[new] = old.  Returns 0, or nonzero on invalid input or allocation
+ * failure. */
+static int32_t *g_rcm_deg;   /* key order for qsort (single-threaded) */
+static int cmp_key(const void *a, const void *b)
+{
+    const int32_t x = *(const int32_t *)a, y = *(const int32_t *)b;
+    if (g_rcm_deg[x] != g_rcm_deg[y]) return g_rcm_deg[x] < g_rcm_deg[y] ? -1 : 1;
+    return (x > y) - (x < y);
+}
+
+/* BFS from r over the unordered vertices (ord < 0), levels into lev[];
+ * returns the eccentricity and the vertex of least key in the last level. */
+static int32_t rcm_bfs(int32_t r, const int64_t *sp, const int32_t *sa, const int32_t *deg,
+                       const int32_t *ord, int32_t *lev, int32_t *queue, int32_t *last_min)
+{
+    int64_t head = 0, tail = 0;
+    queue[tail++] = r;
+    lev[r] = 0;
+    int32_t ecc = 0;
+    while (head < tail) {
+        const int32_t v = queue[head++];
+        for (int64_t k = sp[v]; k < sp[v + 1]; k++) {
+            const int32_t u = sa[k];
+            if (ord[u] >= 0 || lev[u] >= 0) continue;
+            lev[u] = lev[v] + 1;
+            if (lev[u] > ecc) ecc = lev[u];
+            queue[tail++] = u;
+        }
+    }
+    int32_t best = -1;
+    for (int64_t i = 0; i < tail; i++) {
+        const int32_t v = queue[i];
+        if (lev[v] == ecc && (best < 0 || deg[v] < deg[best] || (deg[v] == deg[best] && v < best))) best = v;
+    }
+    for (int64_t i = 0; i < tail; i++) lev[queue[i]] = -1;
+    *last_min = best;
+    return ecc;
+}
+
+int gsofa_oracle_rcm(int32_t n, const int32_t *beg, const int32_t *end, const int32_t *adj,
+                     int64_t adj_len, int32_t *perm)
+{
+    if (validate(n, beg, end, adj, adj_len) || (n > 0 && !perm)) return 1;
+    if (n == 0) return 0;
+    /* S: both directions of every off-diagonal entry, each row sorted and
+     * without duplicates */
+    int64_t *cnt = (int64_t *)calloc((size_t)n + 1, sizeof(int64_t));
+    if (!cnt) return 2;
+    for (int32_t v = 0; v < n; v++)
+        for (int32_t k = beg[v]; k < end[v]; k++)
+            if (adj[k] != v) { cnt[v + 1]++; cnt[adj[k] + 1]++; }
+    for (int32_t v = 0; v < n; v++) cnt[v + 1] += cnt[v];
+    int32_t *sa = (int32_t *)malloc(((size_t)cnt[n] + 1) * sizeof(int32_t));
+    int64_t *at = (int64_t *)malloc(((size_t)n + 1) * sizeof(int64_t));
+    int64_t *sp = (int64_t *)malloc(((size_t)n + 1) * sizeof(int64_t));
+    int32_t *deg = (int32_t *)malloc((size_t)n * sizeof(int32_t));
+    int32_t *ord = (int32_t *)malloc((size_t)n * sizeof(int32_t));
+    int32_t *lev = (int32_t *)malloc((size_t)n * sizeof(int32_t));
+    int32_t *queue = (int32_t *)malloc((size_t)n * sizeof(int32_t));
+    int32_t *bykey = (int32_t *)malloc((size_t)n * sizeof(int32_t));
+    int32_t *cm = (int32_t *)malloc((size_t)n * sizeof(int32_t));
+    int32_t *buf = (int32_t *)malloc((size_t)n * sizeof(int32_t));
+    int rc = 0;
+    if (!sa || !at || !sp || !deg || !ord || !lev || !queue || !bykey || !cm || !buf) { rc = 2; goto done; }
+    for (int32_t v = 0; v < n; v++) at[v] = cnt[v];
+    for (int32_t v = 0; v < n; v++)
+        for (int32_t k = beg[v]; k < end[v]; k++)
+            if (adj[k] != v) { sa[at[v]++] = adj[k]; sa[at[adj[k]]++] = v; }
+    sp[0] = 0;
+    for (int32_t v = 0; v < n; v++) {
+        const int64_t b = cnt[v], e = cnt[v + 1];
+        qsort(sa + b, (size_t)(e - b), sizeof(int32_t), cmp_i32);
+        int64_t w = sp[v];
+        for (int64_t k = b; k < e; k++)
+            if (k == b || sa[k] != sa[k - 1]) sa[w++] = sa[k];
+        sp[v + 1] = w;
+        deg[v] = (int32_t)(w - sp[v]);
+    }
+    /* compacted rows: sa[sp[v] .. sp[v+1]) (sp[v] <= cnt[v], writes trail reads) */
+    for (int32_t v = 0; v < n; v++) { ord[v] = -1; lev[v] = -1; bykey[v] = v; }
+    g_rcm_deg = deg;
+    qsort(bykey, (size_t)n, sizeof(int32_t), cmp_key);
+    {
+        int32_t pos = 0, cursor = 0;
+        while (pos < n) {
+            while (ord[bykey[cursor]] >= 0) cursor++;
+            int32_t r = bykey[cursor], c = -1;
+            int32_t ecc = rcm_bfs(r, sp, sa, deg, ord, lev, queue, &c);
+            for (;;) {
+                int32_t c2 = -1;
+                const int32_t ecc_c = rcm_bfs(c, sp, sa, deg, ord, lev, queue, &c2);
+                if (ecc_c <= ecc) break;
+                r = c;
+                ecc = ecc_c;
+                c = c2;
+            }
+            /* Cuthill-McKee from r */
+            int32_t head = pos;
+            cm[pos] = r;
+            ord[r] = pos++;
+            while (head < pos) {
+                const int32_t v = cm[head++];
+                int32_t m = 0;
+                for (int64_t k = sp[v]; k < sp[v + 1]; k++)
+                    if (ord[sa[k]] < 0) { buf[m++] = sa[k]; ord[sa[k]] = n; }   /* taken */
+                qsort(buf, (size_t)m, sizeof(int32_t), cmp_key);
+                for (int32_t i = 0; i < m; i++) { cm[pos] = buf[i]; ord[buf[i]] = pos++; }
+            }
+        }
+    }
+    for (int32_t k = 0; k < n; k++) perm[k] = cm[n - 1 - k];
+done:
+    free(cnt); free(sa); free(at); free(sp); free(deg); free(ord); free(lev); free(queue);
+    free(bykey); free(cm); free(buf);
+    return rc;
+}

@@ -112,6 +112,16 @@ int32_t gsofa_oracle_maxid_line(int32_t n, const int32_t *beg,
                                 const int32_t *end, const int32_t *adj,
                                 int64_t adj_len, int32_t s, int32_t *out);
 
+/* Reverse Cuthill-McKee ordering of the symmetric structure A + A^T (the
+ * step before the path; the reference takes its input already ordered, so
+ * this restates the published algorithms: Cuthill-McKee breadth-first levels,
+ * George-Liu pseudo-peripheral start, ties broken by (degree, vertex id); the
+ * rules are spelled out in gsofa_oracle.c).  perm[new] = old.  No reference
+ * output exists for it: the GPU ordering is compared with this one bit for
+ * bit, and its quality (bandwidth) with scipy's reverse_cuthill_mckee. */
+int gsofa_oracle_rcm(int32_t n, const int32_t *beg, const int32_t *end, const int32_t *adj,
+                     int64_t adj_len, int32_t *perm);
+
 #ifdef __cplusplus
 }
 #endif

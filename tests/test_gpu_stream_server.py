@@ -83,3 +83,22 @@ def test_stream_server_rejects_oversize_and_bad_input():
             done = srv.poll()
         assert done == [rid]
         srv.result(rid)
+
+
+def test_size_classes_match_standalone_and_free_large_requests():
+    """Requests above max_n run alone on the factorization kernel (the large
+    class), the rest on the serving kernel; every result equals a standalone
+    factorization, and the large requests' matrices are freed."""
+    reqs = serve.make_stream(24, 200, 4000, rate_hz=2000.0, seed=23, build=matgen.make)
+    with gsofa_b200.Context(0) as ctx, gsofa_b200.StreamServer(0, mem_budget_bytes=8 << 30,
+                                                              max_supernode_size=16) as srv:
+        params = gsofa_b200.Params.default(want_pattern=0, max_supernode_size=16)
+        cs = serve.ContinuousServer(srv, oversize=lambda g: serve.run_alone(ctx, g, params), max_n=1500)
+        out = cs.run(reqs)
+        assert out["report"]["run_alone"] == sum(1 for r in reqs if r.graph.n > 1500) > 0
+        assert ctx._mats == []
+        for c in out["completions"]:
+            g = reqs[c.rid].graph
+            with ctx.upload(g) as m:
+                _same(c.result, ctx.symbfact(m, params), f"request {c.rid} (n={g.n})")
+        assert ctx._mats == []
