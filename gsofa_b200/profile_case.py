@@ -6,7 +6,9 @@ into a device pool in the ranges form twice, then once each counts only,
 unpaired with adjacency reuse, with global-memory state and with the
 supernodal structure.  ``python -m gsofa_b200.profile_case serve`` serves one
 request through the persistent serving kernel with a 2 ms idle exit, so a
-replaying profiler never waits on an idle kernel.
+replaying profiler never waits on an idle kernel.  ``python -m
+gsofa_b200.profile_case order`` orders a shuffled 50,000-line power-law
+pattern by reverse Cuthill-McKee on the GPU.
 """
 import sys
 import time
@@ -47,8 +49,14 @@ def serve(side: int = 48) -> None:
         srv.close()
 
 
+def order(side: int = 48) -> None:
+    g = matgen.powerlaw(50_000, seed=7, ordering="random")
+    with gsofa_b200.Context(0) as ctx:
+        ctx.order_rcm(g)
+
+
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "factor"
     side = int(sys.argv[2]) if len(sys.argv) > 2 else 48
-    {"factor": factor, "serve": serve}[which](side)
+    {"factor": factor, "serve": serve, "order": order}[which](side)
     print("ok", which)
