@@ -1581,7 +1581,9 @@ gsofa_status gsofa_order_rcm(gsofa_ctx *c, int32_t n, int64_t nnz, const int32_t
             GS_CUDA(cudaMemcpyAsync(d_small, &big, 4, cudaMemcpyHostToDevice, st));
             order_min_rank_kernel<<<blocks(f1 - f0, 256), 256, 0, st>>>(f0, f1, d_q, d_rank, d_small);
             GS_CUDA(cudaGetLastError());
-            *last_min = bykey[(size_t)read_i32(d_small)];
+            const int32_t least = read_i32(d_small);
+            if (least < 0 || least >= n) throw CudaFail{cudaErrorUnknown};   // cannot happen: the level is not empty
+            *last_min = bykey[(size_t)least];
             return ecc;
         };
 
@@ -1613,6 +1615,7 @@ gsofa_status gsofa_order_rcm(gsofa_ctx *c, int32_t n, int64_t nnz, const int32_t
                 GS_CUDA(cudaGetLastError());
                 const int64_t m = (int64_t)read_ull(d_ctr);
                 if (m == 0) break;
+                if (m > (int64_t)n - pos) throw CudaFail{cudaErrorUnknown};   // cannot happen: each vertex is queued once
                 order_level_keys_kernel<<<blocks(m, 256), 256, 0, st>>>(m, d_next, d_pord, d_rank, ka);
                 GS_CUDA(cudaGetLastError());
                 size_t tb = tmp_bytes;
