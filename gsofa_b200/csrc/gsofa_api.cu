@@ -515,7 +515,10 @@ gsofa_status run_job(gsofa_ctx *ctx, int count, const gsofa_matrix *const *mats,
             if (r.nj <= 0) continue;
         }
         r.piece_base = npieces;
-        r.npieces = (paired ? 1 : 2) * (((int64_t)r.nj + chunk - 1) / chunk);
+        // the bottom eighth in quarter-length pieces (the last handed out)
+        r.tail = (reuse && chunk >= 64) ? r.nj / 8 : 0;
+        r.small = r.tail ? std::max(32, chunk / 4) : chunk;
+        r.npieces = (paired ? 1 : 2) * pieces_per_pass(r);
         npieces += r.npieces;
         ranges.push_back(r);
     }
@@ -2134,6 +2137,8 @@ extern "C" gsofa_status gsofa_symbfact_counts_noalloc(int device, void *cuda_str
         Range rg{};
         rg.mat = 0;
         rg.chunk = 32;
+        rg.small = 32;
+        rg.tail = 0;
         rg.nj = n;
         rg.stride = 1;
         rg.offset = 0;

@@ -49,19 +49,45 @@ struct MatDesc {
 };
 
 // The sources of one matrix, s = offset + stride * j for j in [0, nj), cut
-// into pieces of `chunk` consecutive j.  Piece k of a range covers pass k & 1
-// and chunk k >> 1 counted from the top (the highest sources, which carry the
-// largest traversals, are handed out first).
+// into pieces of consecutive j.  Piece k of a range covers pass k & 1 (one
+// pass per piece unless paired) and piece k >> 1 (k, paired) counted from the
+// top: the highest sources, which carry the largest traversals, are handed
+// out first.  The top nj - tail sources go in pieces of `chunk`, the bottom
+// `tail` ones in pieces of `small`, handed out last, so a launch ends on
+// short pieces instead of waiting for a long one.
 struct Range {
     int32_t mat;
     int32_t chunk;
     int32_t nj;
     int32_t stride;
     int32_t offset;
+    int32_t small;       // piece length of the bottom `tail` sources
+    int32_t tail;
     int32_t pad;
     int64_t piece_base;  // first global piece index of this range
-    int64_t npieces;     // 2 * ceil(nj / chunk)
+    int64_t npieces;     // pieces of both passes
 };
+
+// Sources [j0, j1) of piece c of a range, counted from its top.
+__host__ __device__ inline void piece_bounds(const Range &rg, int64_t c, int64_t &j0, int64_t &j1)
+{
+    const int64_t top = (int64_t)rg.nj - rg.tail;
+    const int64_t nb = (top + rg.chunk - 1) / rg.chunk;
+    if (c < nb) {
+        j1 = (int64_t)rg.nj - c * rg.chunk;
+        j0 = j1 - rg.chunk > (int64_t)rg.tail ? j1 - rg.chunk : (int64_t)rg.tail;
+    } else {
+        j1 = (int64_t)rg.tail - (c - nb) * rg.small;
+        j0 = j1 - rg.small > 0 ? j1 - rg.small : 0;
+    }
+}
+
+// Pieces of one pass of a range.
+__host__ __device__ inline int64_t pieces_per_pass(const Range &rg)
+{
+    const int64_t top = (int64_t)rg.nj - rg.tail;
+    return (top + rg.chunk - 1) / rg.chunk + ((int64_t)rg.tail + rg.small - 1) / rg.small;
+}
 
 // Error bits reported through JobArgs::status.
 enum : uint32_t {
@@ -1145,8 +1171,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) factor_kernel(JobArgs a)
         const int64_t k = pc - rg.piece_base;
         const int pass = PAIRED ? half : (int)(k & 1);
         const int64_t c = PAIRED ? k : (k >> 1);
-        const int64_t j1 = (int64_t)rg.nj - c * rg.chunk;
-        const int64_t j0 = max((int64_t)0, j1 - rg.chunk);
+        int64_t j0, j1;
+        piece_bounds(rg, c, j0, j1);
         const MatDesc md = a.mats[rg.mat];
         const PassGraph g = md.g[pass];
         int32_t s_lo = rg.offset + (int32_t)j0 * rg.stride;
