@@ -240,7 +240,6 @@ def test_batch_matches_one_by_one(ctx):
 
 
 def test_exhaustive_n4_in_one_batch(ctx):
-    import itertools
     pairs = [(i, j) for i in range(4) for j in range(4) if i != j]
     gs, ms = [], []
     for mask in range(0, 1 << len(pairs), 3):   # every third pattern: 1,366 matrices

@@ -4,7 +4,6 @@ The oracle holds two restatements of the fill computation: the reference's
 max-id label propagation, and the two-pass reachability form the GPU library
 implements.  Both are pinned to the reference's logged fill total on its
 bundled matrix before either is trusted as the GPU's checker."""
-import itertools
 
 import numpy as np
 import pytest
