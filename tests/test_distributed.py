@@ -129,3 +129,16 @@ def test_host_supernode_scan_matches_oracle():
         for ms in (0, 5):
             want = oracle.supernodes(ref["u_row_count"], ref["u_next"], ref["l_next"], ms)
             assert np.array_equal(supernodes_from_lines(ref["u_row_count"], flags, ms), want)
+
+
+def test_partition_cuts_are_monotone_for_any_part_count():
+    import gsofa_b200
+    from tests.common import random_graph
+    for g in (matgen.grid2d(10), random_graph(40, 0.05, 3)):
+        for parts in (1, 3, g.n, g.n + 5):
+            cuts, work = gsofa_b200.partition_lines(g, parts)
+            assert cuts[0] == 0 and cuts[-1] == g.n and len(cuts) == parts + 1
+            assert np.all(np.diff(cuts) >= 0)
+            if parts <= g.n:
+                assert np.all(np.diff(cuts) >= 1)    # no empty part while lines remain for each
+            assert np.all(work >= 0)

@@ -126,3 +126,26 @@ def test_permute_lines_is_the_symmetric_permutation():
         assert np.array_equal(h.adj[h.beg[k]:h.end[k]], np.sort(inv[g.adj[g.beg[v]:g.end[v]]]))
     with pytest.raises(gsofa_b200.GsofaError):
         gsofa_b200.permute_lines(g, np.zeros(g.n, np.int32))   # not a permutation
+
+
+def test_permute_lines_edge_cases():
+    import gsofa_b200
+    # identity: every line sorted, ids unchanged
+    g = random_graph(60, 0.05, 2)
+    h = gsofa_b200.permute_lines(g, np.arange(g.n, dtype=np.int32))
+    for v in range(g.n):
+        assert np.array_equal(h.adj[h.beg[v]:h.end[v]], np.sort(g.adj[g.beg[v]:g.end[v]]))
+    # one line, and no lines
+    one = matgen.Graph(1, np.zeros(1, np.int32), np.ones(1, np.int32), np.zeros(1, np.int32), "one")
+    h1 = gsofa_b200.permute_lines(one, np.zeros(1, np.int32))
+    assert h1.n == 1 and h1.adj.tolist() == [0]
+    empty = matgen.Graph(0, np.zeros(0, np.int32), np.zeros(0, np.int32), np.zeros(0, np.int32), "empty")
+    assert gsofa_b200.permute_lines(empty, np.zeros(0, np.int32)).n == 0
+    # wrong length, out-of-range and repeated entries are errors
+    with pytest.raises(gsofa_b200.GsofaError):
+        gsofa_b200.permute_lines(g, np.arange(g.n - 1, dtype=np.int32))
+    bad = np.arange(g.n, dtype=np.int32)
+    bad[3] = g.n
+    with pytest.raises(gsofa_b200.GsofaError):
+        gsofa_b200.permute_lines(g, bad)
+
