@@ -307,7 +307,7 @@ def reference_arm(args):
     line = {
         "metric": "nnz(L+U)/s", "value": value, "unit": "nnz/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * wall / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded generator)", "impl": "reference",
         "config": dict(cfg, sample=cs["desc"]),
         "cpu_baseline": base,
